@@ -1,0 +1,179 @@
+/*
+ * lig_b200 — C ABI of the B200-native gsplat2d hot path.
+ *
+ * Plain pointers, sizes and a CUDA stream (passed as void*); no torch types.
+ * Every buffer is allocated by the caller.  Every entry point is asynchronous
+ * on `stream`, returns LIG_OK or a LIG_ERR_* code, and never synchronises the
+ * host.  Device pointers typed `void*` hold float (dtype LIG_F32) or double
+ * (dtype LIG_F64) arrays; the FP64 instantiation exists for checking against
+ * an FP64 oracle.
+ *
+ * Each declaration names the reference interface it replaces (paths relative
+ * to the reference project root; csrc/ = gsplat2d/gsplat2d/cuda/csrc/).  The
+ * reference bound these through pybind11 (csrc/ext.cpp:4-17); here they are
+ * bound through ctypes by lig_b200/_lib.py.
+ */
+#ifndef LIG_B200_H
+#define LIG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LIG_OK 0
+#define LIG_ERR_INVALID 1     /* bad argument (size, dtype, block width, null) */
+#define LIG_ERR_CAPACITY 2    /* intersection count exceeds the given capacity */
+#define LIG_ERR_LAUNCH 3      /* a kernel launch failed (cudaGetLastError) */
+#define LIG_ERR_WORKSPACE 4   /* workspace smaller than the *_workspace_bytes query */
+
+#define LIG_F32 0
+#define LIG_F64 1
+
+/* Device status word bits written by lig_bin (int32 at `status`). */
+#define LIG_STATUS_OVERFLOW 1 /* num_intersects > capacity: outputs incomplete */
+#define LIG_STATUS_BADBOX 2   /* a tile bbox disagreed with num_tiles_hit */
+
+/* ABI version (bumped on any signature change). */
+int lig_abi_version(void);
+
+/* ------------------------------------------------------------ projection */
+
+/* Projection forward: conic, SnugBox extent, tile bbox and tile-hit count per
+ * Gaussian.  cholesky=0: in3 = cov2d [N,3] (upper triangle a,b,c);
+ * cholesky=1: in3 = [l11, l21, l22].  opacities may be NULL (1.0).
+ * Every output element is written (zeros where the reference leaves its
+ * torch::zeros initialisation).
+ * Replaces project_gaussians_forward_tensor (csrc/bindings.cu:68-117) and
+ * project_gaussians_forward_cholesky_tensor (csrc/bindings.cu:153-202). */
+int lig_project_fwd(int dtype, int num_points, int cholesky, const void *in3,
+                    const void *means2d, const void *opacities, int img_h, int img_w,
+                    int block_width, void *xys, void *extents, void *conics,
+                    int32_t *num_tiles_hit, void *stream);
+
+/* Projection backward that recomputes conic and extent from the inputs
+ * instead of reading saved ones.  v_xy / v_conic rows may be strided
+ * (row stride in elements, unit inner stride).
+ * Replaces the saved-tensor path of project_gaussians.py:77-104 and
+ * project_gaussians_cholesky.py:84-112. */
+int lig_project_bwd(int dtype, int num_points, int cholesky, const void *in3,
+                    const void *means2d, const void *opacities, int img_h, int img_w,
+                    int block_width, const void *v_xy, int64_t v_xy_stride,
+                    const void *v_conic, int64_t v_conic_stride, void *v_in3,
+                    void *v_mean2d, void *stream);
+
+/* Projection backward from saved extents and conics (reference-shaped).
+ * in3 is only read when cholesky=1.
+ * Replaces project_gaussians_backward_tensor (csrc/bindings.cu:119-151) and
+ * project_gaussians_backward_cholesky_tensor (csrc/bindings.cu:204-237). */
+int lig_project_bwd_saved(int dtype, int num_points, int cholesky, const void *extents,
+                          const void *in3, const void *conics, const void *v_xy,
+                          const void *v_conic, void *v_in3, void *v_mean2d, void *stream);
+
+/* Conic and extent only.  Where det == 0 the outputs are zeros.
+ * Replaces compute_cov2d_bounds_tensor (csrc/bindings.cu:41-66). */
+int lig_cov2d_bounds(int dtype, int num_points, const void *cov2d, const void *opacities,
+                     void *conics, void *extents, void *stream);
+
+/* --------------------------------------------------------------- binning */
+
+/* Workspace bytes needed by lig_cumsum_tiles. */
+size_t lig_cumsum_workspace_bytes(int num_points);
+
+/* Inclusive int32 prefix sum of num_tiles_hit; the total (num_intersects) is
+ * written to the device word *num_intersects, with no host synchronisation.
+ * Replaces compute_cumulative_intersects (gsplat2d/gsplat2d/utils.py:61-67). */
+int lig_cumsum_tiles(int num_points, const int32_t *num_tiles_hit, int32_t *cum_tiles_hit,
+                     int32_t *num_intersects, void *workspace, size_t workspace_bytes,
+                     void *stream);
+
+/* Workspace bytes needed by lig_bin for `capacity` intersections. */
+size_t lig_bin_workspace_bytes(int num_points, int capacity, int num_tiles);
+
+/* Key emission + stable LSD radix sort by tile + tile ranges, in one call.
+ * Reads the intersection count from the device word *num_intersects and
+ * handles at most `capacity` of them; if more exist it sets
+ * LIG_STATUS_OVERFLOW in *status (device int32, zeroed by the call) and the
+ * outputs are incomplete.  Outputs: gaussian_ids_sorted [capacity],
+ * tile_bins [T,2] ((0,0) for empty tiles); optional (may be NULL):
+ * isect_ids / gaussian_ids (unsorted, int64 keys tile<<32) and
+ * isect_ids_sorted.
+ * Replaces bin_and_sort_gaussians (gsplat2d/gsplat2d/utils.py:70-100):
+ * map_gaussian_to_intersects (csrc/bindings.cu:239-281), torch.sort +
+ * torch.gather (utils.py:97-98) and get_tile_bin_edges (csrc/bindings.cu:283-301). */
+int lig_bin(int dtype, int num_points, const void *xys, const void *extents,
+            const int32_t *cum_tiles_hit, const int32_t *num_intersects, int img_h, int img_w,
+            int block_width, int capacity, void *workspace, size_t workspace_bytes,
+            int32_t *gaussian_ids_sorted, int32_t *tile_bins, int64_t *isect_ids,
+            int32_t *gaussian_ids, int64_t *isect_ids_sorted, int32_t *status, void *stream);
+
+/* Key emission only, reference-shaped (num_intersects given by the host).
+ * Replaces map_gaussian_to_intersects_tensor (csrc/bindings.cu:239-281). */
+int lig_map_intersects(int dtype, int num_points, int num_intersects, const void *xys,
+                       const void *extents, const int32_t *cum_tiles_hit, int tiles_x,
+                       int tiles_y, int block_width, int64_t *isect_ids, int32_t *gaussian_ids,
+                       void *stream);
+
+/* Tile ranges from sorted int64 keys; empty tiles get (0,0).
+ * Replaces get_tile_bin_edges_tensor (csrc/bindings.cu:283-301). */
+int lig_tile_bin_edges(int num_intersects, const int64_t *isect_ids_sorted, int num_tiles,
+                       int32_t *tile_bins, void *stream);
+
+/* ---------------------------------------------------------- rasterization */
+
+/* Workspace bytes for lig_raster_fwd / lig_raster_bwd (packed records). */
+size_t lig_raster_workspace_bytes(int dtype, int num_points);
+
+/* Weighted-sum rasterizer forward.  out_dx/out_dy/out_dxy == NULL selects the
+ * plain sum; non-NULL selects the gradient-aware variant.  colors are [N,3].
+ * When *num_intersects == 0 the image is all ones and the other outputs zero
+ * (the reference's empty-list branch, rasterize.py:80-90).
+ * Replaces rasterize_forward_tensor (csrc/bindings.cu:303-401). */
+int lig_raster_fwd(int dtype, int img_h, int img_w, int block_width, int num_points,
+                   const int32_t *gaussian_ids_sorted, const int32_t *tile_bins,
+                   const int32_t *num_intersects, const void *xys, const void *conics,
+                   const void *colors, const void *opacities, void *workspace,
+                   size_t workspace_bytes, void *out_img, void *out_wsum, void *out_dx,
+                   void *out_dy, void *out_dxy, int32_t *final_idx, void *stream);
+
+/* Rasterizer backward.  v_dx == NULL selects the sum variant (reference alpha
+ * clamp 0.99), non-NULL the gradient-aware one (reference clamp 0.999);
+ * alpha_clamp overrides the clamp when > 0.  v_opacity may be NULL.
+ * All outputs are fully written.
+ * Replaces rasterize_backward_tensor (csrc/bindings.cu:403-506). */
+int lig_raster_bwd(int dtype, int img_h, int img_w, int block_width, int num_points,
+                   const int32_t *gaussian_ids_sorted, const int32_t *tile_bins,
+                   const int32_t *num_intersects, const void *xys, const void *conics,
+                   const void *colors, const void *opacities, const int32_t *final_idx,
+                   const void *v_img, const void *v_wsum, const void *v_dx, const void *v_dy,
+                   const void *v_dxy, double alpha_clamp, void *workspace,
+                   size_t workspace_bytes, void *v_xy, void *v_xy_abs, void *v_conic,
+                   void *v_rgb, void *v_opacity, void *stream);
+
+/* ---------------------------------------------------------------- upscale */
+
+/* Gradient-aware Hermite-bicubic upscale of [src_h,src_w,3] value/dx/dy/dxy
+ * planes to [dst_h,dst_w,3].  mode 0: half-pixel mapping over the ROI
+ * (x1,y1,x2,y2), ROI extent truncated to int — replaces
+ * gradient_aware_upscale_forward_tensor (csrc/bindings.cu:508-559);
+ * mode 1: align-corners mapping (ROI ignored) — replaces
+ * torch_gradient_aware_upscale (upscaler_torch.py:168-183). */
+int lig_upscale_fwd(int dtype, int mode, int src_h, int src_w, int dst_h, int dst_w,
+                    double roi_x1, double roi_y1, double roi_x2, double roi_y2,
+                    const void *render, const void *dx, const void *dy, const void *dxy,
+                    void *out, void *stream);
+
+/* Upscale backward as a gather (each source texel written once, no atomics).
+ * Replaces gradient_aware_upscale_backward_tensor (csrc/bindings.cu:561-605)
+ * and the autograd of upscaler_torch.py. */
+int lig_upscale_bwd(int dtype, int mode, int src_h, int src_w, int dst_h, int dst_w,
+                    double roi_x1, double roi_y1, double roi_x2, double roi_y2,
+                    const void *grad_out, void *grad_render, void *grad_dx, void *grad_dy,
+                    void *grad_dxy, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LIG_B200_H */

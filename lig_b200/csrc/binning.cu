@@ -1,0 +1,583 @@
+// Tile binning: prefix sum of tile counts, key emission, stable LSD radix
+// sort by tile, tile ranges.
+//
+// Layout in HBM (workspace of lig_bin): keys0/vals0/keys1 [capacity] u32/i32,
+// radix histogram [bins x blocks] u32, scan partials.  The intersection count
+// lives in a device word written by lig_cumsum_tiles; every kernel here reads
+// it and bounds its work by the caller's capacity, so the whole chain runs
+// without a host round trip (the reference reads it back with .item(),
+// gsplat2d/gsplat2d/utils.py:66).
+//
+// Keys are 32-bit tile ids (the reference's int64 (tile << 32) | depth keys
+// carry depth 0, so only ceil(log2 T) bits hold information).  The sort is a
+// stable LSD radix sort over exactly those bits with <= 10-bit digits, so the
+// order inside a tile is emission order (ascending Gaussian id), which is the
+// order of the reference's stable torch.sort.
+#include "common.cuh"
+
+namespace lig {
+
+// ------------------------------------------------------------------ scan
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 16;
+constexpr int kScanTile = kScanThreads * kScanItems;  // 4096
+
+// Block-wide inclusive scan of one value per thread; returns the block total.
+__device__ __forceinline__ uint32_t block_incl_scan(uint32_t v, uint32_t &total,
+                                                    uint32_t *s_warp) {
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    if (lane == 31) s_warp[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        int nw = blockDim.x >> 5;
+        uint32_t w = lane < nw ? s_warp[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += t;
+        }
+        if (lane < nw) s_warp[lane] = w;
+    }
+    __syncthreads();
+    total = s_warp[(blockDim.x >> 5) - 1];
+    uint32_t add = warp > 0 ? s_warp[warp - 1] : 0;
+    __syncthreads();
+    return v + add;
+}
+
+// Each thread owns kScanItems consecutive elements (loaded warp-striped and
+// transposed through registers via shuffles would save little here: the scan
+// runs on <= a few MB).  Phase 1: per-block sums.
+__global__ void scan_reduce_kernel(const uint32_t *__restrict__ in, int n,
+                                   uint32_t *__restrict__ partials) {
+    __shared__ uint32_t s_warp[32];
+    int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    uint32_t acc = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        int64_t i = base + k;
+        if (i < n) acc += in[i];
+    }
+    uint32_t total;
+    block_incl_scan(acc, total, s_warp);
+    if (threadIdx.x == 0) partials[blockIdx.x] = total;
+}
+
+// Phase 2: exclusive scan of the partials by one block (any count).
+__global__ void scan_partials_kernel(uint32_t *__restrict__ partials, int nparts) {
+    __shared__ uint32_t s_warp[32];
+    uint32_t carry = 0;
+    for (int base = 0; base < nparts; base += blockDim.x) {
+        int i = base + threadIdx.x;
+        uint32_t v = i < nparts ? partials[i] : 0;
+        uint32_t total;
+        uint32_t incl = block_incl_scan(v, total, s_warp);
+        if (i < nparts) partials[i] = carry + incl - v;
+        carry += total;
+    }
+}
+
+// Phase 3: rescan each block with its carry-in; inclusive or exclusive output.
+// The last element's inclusive value (the grand total) goes to *total_out.
+__global__ void scan_final_kernel(const uint32_t *__restrict__ in, int n,
+                                  const uint32_t *__restrict__ partials, bool inclusive,
+                                  uint32_t *__restrict__ out, int32_t *__restrict__ total_out) {
+    __shared__ uint32_t s_warp[32];
+    int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    uint32_t acc = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        int64_t i = base + k;
+        v[k] = i < n ? in[i] : 0;
+        acc += v[k];
+    }
+    uint32_t total;
+    uint32_t incl = block_incl_scan(acc, total, s_warp);
+    uint32_t run = partials[blockIdx.x] + incl - acc;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        int64_t i = base + k;
+        uint32_t nxt = run + v[k];
+        if (i < n) out[i] = inclusive ? nxt : run;
+        if (total_out && i == n - 1) *total_out = (int32_t)nxt;
+        run = nxt;
+    }
+}
+
+inline int scan_blocks(int n) { return (n + kScanTile - 1) / kScanTile; }
+
+// Device-wide scan of n u32 values (in may alias out).  partials needs
+// scan_blocks(n) words.
+inline int device_scan(const uint32_t *in, uint32_t *out, int n, bool inclusive,
+                       uint32_t *partials, int32_t *total_out, cudaStream_t s) {
+    if (n <= 0) {
+        if (total_out) cudaMemsetAsync(total_out, 0, sizeof(int32_t), s);
+        return LIG_OK;
+    }
+    int nb = scan_blocks(n);
+    scan_reduce_kernel<<<nb, kScanThreads, 0, s>>>(in, n, partials);
+    scan_partials_kernel<<<1, 1024, 0, s>>>(partials, nb);
+    scan_final_kernel<<<nb, kScanThreads, 0, s>>>(in, n, partials, inclusive, out, total_out);
+    LIG_LAUNCH_CHECK();
+    return LIG_OK;
+}
+
+// -------------------------------------------------------------- emission
+// One warp per 32 consecutive Gaussians.  The warp flattens their tile slots
+// (counts from the inclusive prefix sum) and writes them lane-per-slot, so the
+// stores are coalesced and lanes stay busy whatever the per-Gaussian counts.
+// Slot j of Gaussian g maps to tile (y0 + j / w, x0 + j % w): row-major over
+// the bbox, the emission order of csrc/forward.cu:134-142.  Gaussians whose
+// extent is <= 0 but whose count is non-zero get key 0 / id 0 slots — the
+// values the reference leaves in its zero-initialised buffers.
+template <typename T>
+__global__ void emit_kernel(int n, const T *__restrict__ xys, const T *__restrict__ extents,
+                            const int32_t *__restrict__ cum, unsigned tbx, unsigned tby,
+                            unsigned block, int capacity, uint32_t *__restrict__ keys,
+                            int32_t *__restrict__ vals, int64_t *__restrict__ keys64,
+                            int32_t *__restrict__ vals_extra, int32_t *__restrict__ status) {
+    const unsigned FULL = 0xffffffffu;
+    int lane = threadIdx.x & 31;
+    int64_t warp_id = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int64_t g0 = warp_id * 32;
+    if (g0 >= n) return;
+    int g = (int)(g0 + lane);
+    int cnt = 0, start = 0, x0 = 0, y0 = 0, bw = 1, bh = 0;
+    bool valid = false;
+    if (g < n) {
+        int prev = g > 0 ? cum[g - 1] : 0;
+        start = prev;
+        cnt = cum[g] - prev;
+        T ex = extents[2 * g], ey = extents[2 * g + 1];
+        valid = !(ex <= (T)0 || ey <= (T)0);
+        if (valid && cnt > 0) {
+            int x1, y1;
+            tile_bbox(xys[2 * g], xys[2 * g + 1], ex, ey, tbx, tby, block, x0, y0, x1, y1);
+            bw = x1 - x0;
+            bh = y1 - y0;
+            if (bw <= 0 || bw * bh != cnt) {
+                // inconsistent inputs: keep emission in range and flag it
+                if (status) atomicOr(status, LIG_STATUS_BADBOX);
+                valid = false;
+                bw = 1;
+            }
+        }
+    }
+    // inclusive warp prefix of counts
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += t;
+    }
+    int total = __shfl_sync(FULL, incl, 31);
+    bool overflow = false;
+    for (int s0 = 0; s0 < total; s0 += 32) {
+        int s = s0 + lane;
+        // owner = first lane whose inclusive count exceeds s
+        int lo = 0;
+#pragma unroll
+        for (int step = 16; step >= 1; step >>= 1) {
+            int probe = lo + step - 1;
+            int v = __shfl_sync(FULL, incl, probe);
+            if (v <= s) lo += step;
+        }
+        int owner = lo;
+        int o_incl = __shfl_sync(FULL, incl, owner);
+        int o_cnt = __shfl_sync(FULL, cnt, owner);
+        int o_start = __shfl_sync(FULL, start, owner);
+        int o_x0 = __shfl_sync(FULL, x0, owner);
+        int o_y0 = __shfl_sync(FULL, y0, owner);
+        int o_bw = __shfl_sync(FULL, bw, owner);
+        int o_valid = __shfl_sync(FULL, (int)valid, owner);
+        if (s >= total) continue;
+        int j = s - (o_incl - o_cnt);
+        int slot = o_start + j;
+        if (slot >= capacity) {
+            overflow = true;
+            continue;
+        }
+        uint32_t key = 0;
+        int32_t gid = 0;
+        if (o_valid) {
+            int q = j / o_bw;
+            int r = j - q * o_bw;
+            key = (uint32_t)(o_y0 + q) * tbx + (uint32_t)(o_x0 + r);
+            gid = (int32_t)(g0 + owner);
+        }
+        if (keys) keys[slot] = key;
+        vals[slot] = gid;
+        if (keys64) keys64[slot] = (int64_t)key << 32;
+        if (vals_extra) vals_extra[slot] = gid;
+    }
+    if (overflow && status) atomicOr(status, LIG_STATUS_OVERFLOW);
+}
+
+// ----------------------------------------------------------------- radix
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortRounds = 16;                         // keys per lane
+constexpr int kSortTile = kSortThreads * kSortRounds;   // 4096 keys per block
+constexpr int kWarpSeg = 32 * kSortRounds;              // 512 keys per warp
+
+__device__ __forceinline__ int bounded_count(const int32_t *d_total, int capacity) {
+    int m = *d_total;
+    return m < capacity ? m : capacity;
+}
+
+// Per-block digit histogram -> hist[d * nblk + blk].
+__global__ void radix_upsweep_kernel(const uint32_t *__restrict__ keys, const int32_t *d_total,
+                                     int capacity, int shift, int bins,
+                                     uint32_t *__restrict__ hist, int nblk) {
+    extern __shared__ uint32_t s_hist[];
+    for (int i = threadIdx.x; i < bins; i += blockDim.x) s_hist[i] = 0;
+    __syncthreads();
+    int m = bounded_count(d_total, capacity);
+    int64_t base = (int64_t)blockIdx.x * kSortTile;
+    if (base < m) {
+#pragma unroll 4
+        for (int r = 0; r < kSortRounds; ++r) {
+            int64_t i = base + r * kSortThreads + threadIdx.x;
+            if (i < m) atomicAdd(&s_hist[(keys[i] >> shift) & (bins - 1)], 1u);
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < bins; i += blockDim.x)
+        hist[(int64_t)i * nblk + blockIdx.x] = s_hist[i];
+}
+
+// Stable scatter.  Each warp ranks its 512 consecutive keys in 16 rounds of
+// 32 with __match_any_sync and per-warp digit counters, so ranks follow input
+// order; counters are then prefixed across warps and digits, the block's keys
+// are placed in shared memory in sorted order, and written out in runs
+// (consecutive threads -> consecutive output positions of one digit).
+// Shared layout: wcnt[kSortWarps][bins] | bofs[bins] | gbase[bins] |
+//                skeys[4096] | svals[4096].
+__global__ void __launch_bounds__(kSortThreads)
+radix_downsweep_kernel(const uint32_t *__restrict__ keys_in, const int32_t *__restrict__ vals_in,
+                       uint32_t *__restrict__ keys_out, int32_t *__restrict__ vals_out,
+                       const int32_t *d_total, int capacity, int shift, int bins,
+                       const uint32_t *__restrict__ hist_scan, int nblk) {
+    extern __shared__ uint32_t smem[];
+    uint32_t *wcnt = smem;
+    uint32_t *bofs = wcnt + kSortWarps * bins;
+    uint32_t *gbase = bofs + bins;
+    uint32_t *skeys = gbase + bins;
+    int32_t *svals = (int32_t *)(skeys + kSortTile);
+
+    const unsigned FULL = 0xffffffffu;
+    int m = bounded_count(d_total, capacity);
+    int64_t base = (int64_t)blockIdx.x * kSortTile;
+    if (base >= m) return;  // uniform across the block
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < kSortWarps * bins; i += blockDim.x) wcnt[i] = 0;
+    for (int i = threadIdx.x; i < bins; i += blockDim.x)
+        gbase[i] = hist_scan[(int64_t)i * nblk + blockIdx.x];
+    __syncthreads();
+
+    uint32_t k[kSortRounds];
+    int32_t v[kSortRounds];
+    uint32_t rk[kSortRounds];
+    int64_t wbase = base + warp * kWarpSeg;
+#pragma unroll
+    for (int r = 0; r < kSortRounds; ++r) {
+        int64_t i = wbase + r * 32 + lane;
+        bool ok = i < m;
+        k[r] = ok ? keys_in[i] : 0u;
+        v[r] = ok ? vals_in[i] : 0;
+    }
+    uint32_t lt_mask = (1u << lane) - 1u;
+    uint32_t *my = wcnt + warp * bins;
+#pragma unroll
+    for (int r = 0; r < kSortRounds; ++r) {
+        int64_t i = wbase + r * 32 + lane;
+        bool ok = i < m;
+        uint32_t d = (k[r] >> shift) & (uint32_t)(bins - 1);
+        uint32_t peers = __match_any_sync(FULL, ok ? d : 0xffffffffu);
+        uint32_t before = __popc(peers & lt_mask);
+        uint32_t old = ok ? my[d] : 0u;
+        __syncwarp();
+        if (ok && before == 0) my[d] = old + __popc(peers);
+        __syncwarp();
+        rk[r] = old + before;
+    }
+    __syncthreads();
+    // exclusive prefix over warps per digit; block digit totals into bofs
+    for (int d = threadIdx.x; d < bins; d += blockDim.x) {
+        uint32_t run = 0;
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w) {
+            uint32_t t = wcnt[w * bins + d];
+            wcnt[w * bins + d] = run;
+            run += t;
+        }
+        bofs[d] = run;
+    }
+    __syncthreads();
+    // exclusive scan of bofs over digits (bins <= 1024 = 4 per thread)
+    {
+        __shared__ uint32_t s_warp[32];
+        int per = (bins + kSortThreads - 1) / kSortThreads;
+        int d0 = threadIdx.x * per;
+        uint32_t loc[4] = {0, 0, 0, 0};
+        uint32_t acc = 0;
+        for (int q = 0; q < per; ++q) {
+            int d = d0 + q;
+            loc[q] = d < bins ? bofs[d] : 0;
+            acc += loc[q];
+        }
+        uint32_t total;
+        uint32_t incl = block_incl_scan(acc, total, s_warp);
+        uint32_t run = incl - acc;
+        for (int q = 0; q < per; ++q) {
+            int d = d0 + q;
+            if (d < bins) bofs[d] = run;
+            run += loc[q];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kSortRounds; ++r) {
+        int64_t i = wbase + r * 32 + lane;
+        if (i < m) {
+            uint32_t d = (k[r] >> shift) & (uint32_t)(bins - 1);
+            uint32_t pos = bofs[d] + wcnt[warp * bins + d] + rk[r];
+            skeys[pos] = k[r];
+            svals[pos] = v[r];
+        }
+    }
+    __syncthreads();
+    int nvalid = (int)min((int64_t)kSortTile, (int64_t)m - base);
+    for (int i = threadIdx.x; i < nvalid; i += blockDim.x) {
+        uint32_t key = skeys[i];
+        uint32_t d = (key >> shift) & (uint32_t)(bins - 1);
+        uint32_t gpos = gbase[d] + (uint32_t)i - bofs[d];
+        keys_out[gpos] = key;
+        vals_out[gpos] = svals[i];
+    }
+}
+
+inline size_t downsweep_smem(int bins) {
+    return sizeof(uint32_t) * ((size_t)(kSortWarps + 2) * bins + 2 * kSortTile);
+}
+
+// ----------------------------------------------------------- tile ranges
+// Boundary detection on sorted keys (csrc/forward.cu:148-170); tile_bins must
+// be zeroed first so empty tiles read (0,0).
+template <typename K>
+__device__ __forceinline__ int32_t key_tile(K k);
+template <> __device__ __forceinline__ int32_t key_tile<uint32_t>(uint32_t k) { return (int32_t)k; }
+template <> __device__ __forceinline__ int32_t key_tile<int64_t>(int64_t k) { return (int32_t)(k >> 32); }
+
+template <typename K>
+__global__ void tile_ranges_kernel(const K *__restrict__ keys, const int32_t *d_total,
+                                   int capacity, int m_host, int2 *__restrict__ bins) {
+    int m = d_total ? bounded_count(d_total, capacity) : m_host;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    int32_t cur = key_tile<K>(keys[i]);
+    if (i == 0) bins[cur].x = 0;
+    if (i == m - 1) bins[cur].y = m;
+    if (i == 0) return;
+    int32_t prev = key_tile<K>(keys[i - 1]);
+    if (prev != cur) {
+        bins[prev].y = (int)i;
+        bins[cur].x = (int)i;
+    }
+}
+
+// Widen sorted 32-bit tile keys to the reference's int64 layout (tile << 32).
+__global__ void widen_keys_kernel(const uint32_t *__restrict__ keys, const int32_t *d_total,
+                                  int capacity, int64_t *__restrict__ out) {
+    int m = bounded_count(d_total, capacity);
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) out[i] = (int64_t)keys[i] << 32;
+}
+
+__global__ void flag_overflow_kernel(const int32_t *d_total, int capacity, int32_t *status) {
+    if (*d_total > capacity) atomicOr(status, LIG_STATUS_OVERFLOW);
+}
+
+// ------------------------------------------------------- workspace plan
+struct BinPlan {
+    int bits, passes, dbits, bins, nblk;
+    size_t off_k0, off_v0, off_k1, off_hist, off_part, total;
+};
+
+inline size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
+
+inline BinPlan make_plan(int capacity, int num_tiles) {
+    BinPlan p{};
+    int bits = 0;
+    while (bits < 31 && (1ll << bits) < (long long)num_tiles) ++bits;
+    p.bits = bits;
+    p.passes = (bits + 9) / 10;
+    p.dbits = p.passes ? (bits + p.passes - 1) / p.passes : 0;
+    p.bins = 1 << p.dbits;
+    p.nblk = (capacity + kSortTile - 1) / kSortTile;
+    if (p.nblk < 1) p.nblk = 1;
+    size_t cap = (size_t)(capacity > 0 ? capacity : 1);
+    size_t off = 0;
+    p.off_k0 = off; off = align_up(off + 4 * cap);
+    p.off_v0 = off; off = align_up(off + 4 * cap);
+    p.off_k1 = off; off = align_up(off + 4 * cap);
+    size_t hist_n = (size_t)p.bins * p.nblk;
+    p.off_hist = off; off = align_up(off + 4 * hist_n);
+    size_t nparts = (hist_n + kScanTile - 1) / kScanTile + 1;
+    p.off_part = off; off = align_up(off + 4 * nparts);
+    p.total = off;
+    return p;
+}
+
+template <typename T>
+int run_bin(int n, const void *xys, const void *ext, const int32_t *cum, const int32_t *d_total,
+            int h, int w, int b, int capacity, void *ws, size_t ws_bytes, int32_t *gid_sorted,
+            int32_t *tile_bins, int64_t *isect, int32_t *gids, int64_t *isect_sorted,
+            int32_t *status, cudaStream_t s) {
+    unsigned tbx = (w + b - 1) / b, tby = (h + b - 1) / b;
+    int T_ = (int)(tbx * tby);
+    BinPlan p = make_plan(capacity, T_);
+    if (ws_bytes < p.total) return LIG_ERR_WORKSPACE;
+    char *base = (char *)ws;
+    uint32_t *k0 = (uint32_t *)(base + p.off_k0);
+    int32_t *v0 = (int32_t *)(base + p.off_v0);
+    uint32_t *k1 = (uint32_t *)(base + p.off_k1);
+    uint32_t *hist = (uint32_t *)(base + p.off_hist);
+    uint32_t *part = (uint32_t *)(base + p.off_part);
+
+    cudaMemsetAsync(status, 0, sizeof(int32_t), s);
+    cudaMemsetAsync(tile_bins, 0, sizeof(int32_t) * 2 * (size_t)T_, s);
+    if (n == 0 || capacity == 0) {
+        flag_overflow_kernel<<<1, 1, 0, s>>>(d_total, capacity, status);
+        LIG_LAUNCH_CHECK();
+        return LIG_OK;
+    }
+    // Ping-pong so that the last pass lands in (k1, gid_sorted).
+    uint32_t *ka = (p.passes % 2 == 1) ? k0 : k1;
+    int32_t *va = (p.passes % 2 == 1) ? v0 : gid_sorted;
+    uint32_t *kb = (p.passes % 2 == 1) ? k1 : k0;
+    int32_t *vb = (p.passes % 2 == 1) ? gid_sorted : v0;
+
+    int warps = (n + 31) / 32;
+    int eblocks = (warps * 32 + 255) / 256;
+    emit_kernel<T><<<eblocks, 256, 0, s>>>(n, (const T *)xys, (const T *)ext, cum, tbx, tby, b,
+                                           capacity, ka, va, isect, gids, status);
+    flag_overflow_kernel<<<1, 1, 0, s>>>(d_total, capacity, status);
+    LIG_LAUNCH_CHECK();
+
+    size_t dsm = downsweep_smem(p.bins);
+    if (dsm > 48 * 1024)
+        cudaFuncSetAttribute(radix_downsweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)dsm);
+    int hist_n = p.bins * p.nblk;
+    for (int pass = 0; pass < p.passes; ++pass) {
+        int shift = pass * p.dbits;
+        radix_upsweep_kernel<<<p.nblk, kSortThreads, sizeof(uint32_t) * p.bins, s>>>(
+            ka, d_total, capacity, shift, p.bins, hist, p.nblk);
+        int rc = device_scan(hist, hist, hist_n, false, part, nullptr, s);
+        if (rc) return rc;
+        radix_downsweep_kernel<<<p.nblk, kSortThreads, dsm, s>>>(
+            ka, va, kb, vb, d_total, capacity, shift, p.bins, hist, p.nblk);
+        LIG_LAUNCH_CHECK();
+        uint32_t *tk = ka; ka = kb; kb = tk;
+        int32_t *tv = va; va = vb; vb = tv;
+    }
+    // (ka, va) now hold the sorted keys / ids; va == gid_sorted.
+    // with zero passes (a single tile) emission already wrote (k1, gid_sorted)
+    tile_ranges_kernel<uint32_t><<<(capacity + 255) / 256, 256, 0, s>>>(ka, d_total, capacity, 0,
+                                                                      (int2 *)tile_bins);
+    if (isect_sorted)
+        widen_keys_kernel<<<(capacity + 255) / 256, 256, 0, s>>>(ka, d_total, capacity,
+                                                                 isect_sorted);
+    LIG_LAUNCH_CHECK();
+    return LIG_OK;
+}
+
+}  // namespace lig
+
+using namespace lig;
+
+extern "C" size_t lig_cumsum_workspace_bytes(int n) {
+    return sizeof(uint32_t) * ((size_t)scan_blocks(n > 0 ? n : 1) + 1);
+}
+
+extern "C" int lig_cumsum_tiles(int n, const int32_t *counts, int32_t *cum, int32_t *total,
+                                void *workspace, size_t workspace_bytes, void *stream) {
+    if (n < 0 || !total || (n > 0 && (!counts || !cum || !workspace))) return LIG_ERR_INVALID;
+    if (workspace_bytes < lig_cumsum_workspace_bytes(n)) return LIG_ERR_WORKSPACE;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (n == 0) {
+        cudaMemsetAsync(total, 0, sizeof(int32_t), s);
+        LIG_LAUNCH_CHECK();
+        return LIG_OK;
+    }
+    return device_scan((const uint32_t *)counts, (uint32_t *)cum, n, true, (uint32_t *)workspace,
+                       total, s);
+}
+
+extern "C" size_t lig_bin_workspace_bytes(int n, int capacity, int num_tiles) {
+    (void)n;
+    return make_plan(capacity, num_tiles).total;
+}
+
+extern "C" int lig_bin(int dtype, int n, const void *xys, const void *ext, const int32_t *cum,
+                       const int32_t *d_total, int h, int w, int b, int capacity, void *ws,
+                       size_t ws_bytes, int32_t *gid_sorted, int32_t *tile_bins, int64_t *isect,
+                       int32_t *gids, int64_t *isect_sorted, int32_t *status, void *stream) {
+    if (n < 0 || h <= 0 || w <= 0 || b < 1 || capacity < 0 || !d_total || !tile_bins || !status ||
+        (n > 0 && (!xys || !ext || !cum)) || (capacity > 0 && (!gid_sorted || !ws)))
+        return LIG_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (dtype == LIG_F32)
+        return run_bin<float>(n, xys, ext, cum, d_total, h, w, b, capacity, ws, ws_bytes,
+                              gid_sorted, tile_bins, isect, gids, isect_sorted, status, s);
+    if (dtype == LIG_F64)
+        return run_bin<double>(n, xys, ext, cum, d_total, h, w, b, capacity, ws, ws_bytes,
+                               gid_sorted, tile_bins, isect, gids, isect_sorted, status, s);
+    return LIG_ERR_INVALID;
+}
+
+extern "C" int lig_map_intersects(int dtype, int n, int m, const void *xys, const void *ext,
+                                  const int32_t *cum, int tbx, int tby, int b, int64_t *isect,
+                                  int32_t *gids, void *stream) {
+    if (n < 0 || m < 0 || tbx <= 0 || tby <= 0 || b < 1 || (m > 0 && (!isect || !gids)) ||
+        (n > 0 && (!xys || !ext || !cum)))
+        return LIG_ERR_INVALID;
+    if (n == 0 || m == 0) return LIG_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    // reference semantics: slots not written by any Gaussian stay zero
+    cudaMemsetAsync(isect, 0, sizeof(int64_t) * (size_t)m, s);
+    cudaMemsetAsync(gids, 0, sizeof(int32_t) * (size_t)m, s);
+    int warps = (n + 31) / 32;
+    int eblocks = (warps * 32 + 255) / 256;
+    if (dtype == LIG_F32)
+        emit_kernel<float><<<eblocks, 256, 0, s>>>(n, (const float *)xys, (const float *)ext, cum,
+                                                   tbx, tby, b, m, nullptr, gids, isect, nullptr,
+                                                   nullptr);
+    else if (dtype == LIG_F64)
+        emit_kernel<double><<<eblocks, 256, 0, s>>>(n, (const double *)xys, (const double *)ext,
+                                                    cum, tbx, tby, b, m, nullptr, gids, isect,
+                                                    nullptr, nullptr);
+    else
+        return LIG_ERR_INVALID;
+    LIG_LAUNCH_CHECK();
+    return LIG_OK;
+}
+
+extern "C" int lig_tile_bin_edges(int m, const int64_t *isect_sorted, int num_tiles,
+                                  int32_t *tile_bins, void *stream) {
+    if (m < 0 || num_tiles <= 0 || !tile_bins || (m > 0 && !isect_sorted)) return LIG_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaMemsetAsync(tile_bins, 0, sizeof(int32_t) * 2 * (size_t)num_tiles, s);
+    if (m > 0)
+        tile_ranges_kernel<int64_t><<<(m + 255) / 256, 256, 0, s>>>(isect_sorted, nullptr, m, m,
+                                                                    (int2 *)tile_bins);
+    LIG_LAUNCH_CHECK();
+    return LIG_OK;
+}

@@ -1,0 +1,163 @@
+"""The drop-in gsplat2d API on the GPU: end-to-end equality with the reference
+pipeline, empty-list branch, error behaviour, absgrad, the `_C` table,
+align-corners upscaler, and a LIG-style training step."""
+import numpy as np
+import pytest
+import torch
+
+import lig_b200
+from lig_b200 import gsplat2d, ops, upscaler_torch
+from lig_b200.gsplat2d import cuda as C
+from oracle import oracle as O
+from oracle import ref
+from tests._scene import chol_to_cov, np_, rel_err, scene
+
+pytestmark = pytest.mark.gpu
+
+
+def test_install_gsplat2d_aliases():
+    lig_b200.install_gsplat2d()
+    import gsplat2d as g2
+    from gsplat2d.project_gaussians import project_gaussians
+    from gsplat2d.rasterize import rasterize_gaussians
+    from upscaler_torch import torch_gradient_aware_upscale
+    assert g2.project_gaussians_2d is project_gaussians
+    assert g2.rasterize_gaussians_sum is rasterize_gaussians
+    assert torch_gradient_aware_upscale is upscaler_torch.torch_gradient_aware_upscale
+
+
+def test_gaussianlig_style_forward_backward_matches_reference():
+    """gaussianlig.Gaussian2D.forward + L2 backward, raw cov2d ~ U[0,1)^3
+    (non-PD allowed), no opacities, B=16."""
+    H, W, B, n = 120, 136, 16, 1500
+    g = torch.Generator().manual_seed(2)
+    means = (torch.rand(n, 2, generator=g) * torch.tensor([W, H])).cuda()
+    cov = torch.rand(n, 3, generator=g).cuda()
+    rgbs = torch.rand(n, 3, generator=g).cuda()
+    gt = torch.rand(1, 3, H, W, generator=g).cuda()
+
+    def step(project, raster):
+        p = [means.clone().requires_grad_(), cov.clone().requires_grad_(),
+             rgbs.clone().requires_grad_()]
+        xys, ext, con, cnt = project(p[1], p[0], H, W, B)
+        img = raster(xys, ext, con, cnt, p[2], None, H, W, B)[0][..., :3]
+        img = torch.clamp(img, 0, 1).view(-1, H, W, 3).permute(0, 3, 1, 2).contiguous()
+        loss = torch.nn.functional.mse_loss(img, gt)
+        loss.backward()
+        return img.detach(), [q.grad for q in p]
+
+    img, grads = step(gsplat2d.project_gaussians, gsplat2d.rasterize_gaussians)
+    # reference pipeline with the reference kernels; gradients via the same chain rule
+    r = ref.render(cov, means, rgbs, None, H, W, B, chol=False)
+    rimg = torch.clamp(r["img"], 0, 1).permute(2, 0, 1).unsqueeze(0)
+    assert (img - rimg).abs().max().item() <= 1e-5
+    v_img = (2.0 / img.numel()) * (rimg - gt) * ((r["img"].permute(2, 0, 1).unsqueeze(0) >= 0) &
+                                                  (r["img"].permute(2, 0, 1).unsqueeze(0) <= 1))
+    v_img = v_img.squeeze(0).permute(1, 2, 0).contiguous()
+    rg = ref.raster_bwd(H, W, B, r["binning"], r["xys"], r["conics"], rgbs, None, r["final_idx"],
+                        v_img, torch.zeros(H, W, device="cuda"))
+    v_cov, v_mean = ref.project_bwd(r["extents"], cov, r["conics"], rg["v_xy"], rg["v_conic"],
+                                    chol=False)
+    assert rel_err(np_(grads[0]), np_(v_mean)) <= 1e-4
+    assert rel_err(np_(grads[1]), np_(v_cov)) <= 1e-4
+    assert rel_err(np_(grads[2]), np_(rg["v_rgb"])) <= 1e-4
+
+
+def test_empty_list_white_image_and_zero_grads():
+    H, W, B = 32, 48, 16
+    means = torch.tensor([[-500.0, -500.0], [900.0, 10.0]], device="cuda", requires_grad=True)
+    chol = torch.tensor([[1.0, 0.0, 1.0], [1.0, 0.0, 1.0]], device="cuda", requires_grad=True)
+    cols = torch.rand(2, 3, device="cuda", requires_grad=True)
+    xys, ext, con, cnt = gsplat2d.project_gaussians_cholesky(chol, means, H, W, B)
+    assert int(cnt.sum()) == 0
+    img, wsum, dx, dy, dxy = gsplat2d.rasterize_gaussians(xys, ext, con, cnt, cols, None, H, W, B,
+                                                          compute_upscale_gradients=True)
+    assert torch.all(img == 1) and torch.all(wsum == 0) and torch.all(dx == 0)
+    (img.sum() + wsum.sum()).backward()
+    assert torch.all(cols.grad == 0) and torch.all(means.grad == 0)
+
+
+def test_errors_and_uint8_and_absgrad():
+    H, W, B = 64, 64, 16
+    means, L, colors, op = scene(200, H, W)
+    xys, ext, con, cnt = gsplat2d.project_gaussians_cholesky(L, means, H, W, B, op)
+    with pytest.raises(AssertionError):
+        gsplat2d.rasterize_gaussians(xys, ext, con, cnt, colors, op, H, W, 32)
+    with pytest.raises(ValueError):
+        gsplat2d.rasterize_gaussians(xys[:, :1], ext, con, cnt, colors, op, H, W, B)
+    with pytest.raises(ValueError):
+        gsplat2d.rasterize_gaussians(xys, ext, con, cnt, colors[:, 0], op, H, W, B)
+    with pytest.raises(ValueError):
+        gsplat2d.project_gaussians_cholesky(L[:, :2], means, H, W, B)
+    c8 = (colors * 255).to(torch.uint8)
+    a = gsplat2d.rasterize_gaussians(xys, ext, con, cnt, c8, op, H, W, B)[0]
+    b = gsplat2d.rasterize_gaussians(xys, ext, con, cnt, c8.float() / 255, op, H, W, B)[0]
+    assert torch.equal(a, b)
+    x = xys.detach().clone().requires_grad_()
+    img = gsplat2d.rasterize_gaussians(x, ext, con, cnt, colors, op, H, W, B)[0]
+    img.sum().backward()
+    assert hasattr(x, "absgrad") and x.absgrad.shape == x.shape
+    assert torch.all(x.absgrad >= x.grad.abs() - 1e-6)
+
+
+def test_c_table_matches_reference():
+    H, W, B = 90, 100, 16
+    means, L, colors, op = scene(700, H, W, opac=(0.05, 1.0))
+    cov = chol_to_cov(L)
+    n = cov.shape[0]
+    for a, b in zip(C.project_gaussians_forward(n, cov, means, op, H, W, B),
+                    ref.project_fwd(cov, means, op, H, W, B, False)):
+        assert torch.equal(a, b)
+    xys, ext, con, cnt = C.project_gaussians_forward_cholesky(n, L, means, op, H, W, B)
+    m, cum = gsplat2d.compute_cumulative_intersects(cnt)
+    tb = ((W + B - 1) // B, (H + B - 1) // B, 1)
+    depths = torch.zeros(n, device="cuda")
+    out = gsplat2d.bin_and_sort_gaussians(n, m, xys, depths, ext, cum, tb, B)
+    rb = ref.bin_and_sort(xys, ext, cnt, H, W, B)
+    for a, b in zip(out, (rb.isect_ids, rb.gaussian_ids, rb.isect_ids_sorted,
+                          rb.gaussian_ids_sorted, rb.tile_bins)):
+        assert torch.equal(a, b)
+    fwd = C.rasterize_forward(tb, (B, B, 1), (W, H, 1), out[3], out[4], xys, con, colors, op, True)
+    rf = ref.raster_fwd(H, W, B, rb, xys, con, colors, op, True)
+    assert torch.equal(fwd[5], rf["final_idx"])
+    assert (fwd[0] - rf["img"]).abs().max().item() <= 1e-5
+    c2, e2 = C.compute_cov2d_bounds(n, cov, op)
+    rc, re_ = ref.cov2d_bounds(cov, op)
+    assert torch.equal(c2, rc) and torch.equal(e2, re_)
+
+
+def test_align_corners_upscaler_matches_oracle():
+    h, w, nh, nw = 40, 52, 101, 157
+    g = torch.Generator().manual_seed(8)
+    planes = [torch.randn(h, w, 3, generator=g, dtype=torch.float64) for _ in range(4)]
+    got = upscaler_torch.torch_gradient_aware_upscale(*[p.cuda() for p in planes], nh, nw)
+    exp = O.upscale_fwd(*[p.numpy() for p in planes], nh, nw, mode=1, dtype=np.float64)
+    assert np.abs(np_(got) - exp).max() <= 1e-12
+    gout = torch.randn(nh, nw, 3, generator=g, dtype=torch.float64)
+    x = [p.cuda().requires_grad_() for p in planes]
+    upscaler_torch.torch_gradient_aware_upscale(*x, nh, nw).backward(gout.cuda())
+    eg = O.upscale_bwd(gout.numpy(), h, w, mode=1, dtype=np.float64)
+    for a, b in zip(x, eg):
+        assert rel_err(np_(a.grad), b) <= 1e-12
+
+
+def test_lig_training_step_decreases_loss():
+    H, W, B, n = 96, 96, 16, 2000
+    means, L, colors, _ = scene(n, H, W, diag=(0.5, 3.0), seed=2)
+    gt_means, gt_L, gt_col, _ = scene(1500, H, W, diag=(0.5, 3.0), seed=0)
+    with torch.no_grad():
+        x, e, c, k = gsplat2d.project_gaussians_cholesky(gt_L, gt_means, H, W, B)
+        gt = torch.clamp(gsplat2d.rasterize_gaussians(x, e, c, k, gt_col, None, H, W, B)[0], 0, 1)
+    params = [means.requires_grad_(), L.requires_grad_(), colors.requires_grad_()]
+    opt = torch.optim.Adam(params, lr=1e-2)
+    losses = []
+    for _ in range(30):
+        x, e, c, k = gsplat2d.project_gaussians_cholesky(params[1], params[0], H, W, B)
+        img = torch.clamp(gsplat2d.rasterize_gaussians(x, e, c, k, params[2], None, H, W, B)[0],
+                          0, 1)
+        loss = torch.nn.functional.mse_loss(img, gt)
+        opt.zero_grad()
+        loss.backward()
+        opt.step()
+        losses.append(loss.item())
+    assert losses[-1] < 0.7 * losses[0]

@@ -1,0 +1,195 @@
+"""Parity of the sm_100a kernels against the reference's own CUDA kernels
+(oracle/_ref, compiled from the reference sources) on identical seeded inputs.
+
+Bars: tile counts, keys, sorted ids and tile ranges bit-exact; images within
+1e-5 max-abs (float32); gradients within 1e-4 relative to the largest
+component (float32, atomics make the reference's own order arbitrary)."""
+import numpy as np
+import pytest
+import torch
+
+from lig_b200 import ops
+from oracle import ref
+from tests._scene import chol_to_cov, np_, rel_err, scene
+
+pytestmark = pytest.mark.gpu
+
+IMG_TOL = 1e-5
+GRAD_TOL = 1e-4
+
+CASES = [
+    # n, H, W, B, diag, opac
+    (600, 128, 160, 16, (0.5, 4.0), None),
+    (900, 77, 91, 16, (0.5, 6.0), (0.05, 1.0)),
+    (500, 96, 96, 8, (0.5, 4.0), None),
+    (400, 70, 50, 12, (0.5, 3.0), (0.2, 0.95)),
+    (300, 40, 33, 5, (0.3, 2.0), None),
+    (2500, 256, 256, 16, (0.5, 8.0), (0.0, 1.0)),  # includes opacity < 1/255: phantom slots
+]
+
+
+def _ids(c):
+    n, H, W, B, d, o = c
+    return f"n{n}_{H}x{W}_B{B}_{'op' if o else 'noop'}"
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _need_ref():
+    assert ref.available(), "reference kernels missing: run `make -C oracle ref`"
+
+
+@pytest.mark.parametrize("case", CASES, ids=_ids)
+@pytest.mark.parametrize("chol", [True, False])
+def test_projection_bit_exact(case, chol):
+    n, H, W, B, diag, opac = case
+    means, L, colors, op = scene(n, H, W, diag=diag, opac=opac)
+    in3 = L if chol else chol_to_cov(L)
+    r = ref.project_fwd(in3, means, op, H, W, B, chol)
+    m = ops.project_fwd(in3, means, op, H, W, B, chol)
+    for a, b, name in zip(m, r, ["xys", "extents", "conics", "num_tiles_hit"]):
+        assert torch.equal(a, b), f"{name} differs from the reference kernel"
+
+
+def test_projection_degenerate_inputs():
+    H, W, B = 64, 64, 16
+    cov = torch.tensor([[1.0, 1.0, 1.0],      # det == 0
+                        [0.3, 0.5, 0.2],      # det < 0 (non-PD)
+                        [-1.0, 0.0, 2.0],     # negative variance -> NaN extent
+                        [4.0, 0.0, 4.0],
+                        [1e-8, 0.0, 1e-8],
+                        [float("nan"), 0.0, 1.0],
+                        [1e6, 0.0, 1e6]], device="cuda")
+    means = torch.tensor([[10.0, 10.0], [30.5, 20.0], [5.0, 60.0], [-3.0, 2.0], [63.9, 63.9],
+                          [1.0, 1.0], [32.0, 32.0]], device="cuda")
+    for op in (None, torch.tensor([1.0, 0.5, 0.003, 0.9, 1.0, 1.0, 1.0], device="cuda")):
+        r = ref.project_fwd(cov, means, op, H, W, B, False)
+        m = ops.project_fwd(cov, means, op, H, W, B, False)
+        for a, b in zip(m, r):
+            assert torch.equal(torch.nan_to_num(a, nan=-7.0), torch.nan_to_num(b, nan=-7.0))
+
+
+@pytest.mark.parametrize("case", CASES, ids=_ids)
+def test_binning_bit_exact(case):
+    n, H, W, B, diag, opac = case
+    means, L, colors, op = scene(n, H, W, diag=diag, opac=opac)
+    xys, ext, con, cnt = ref.project_fwd(L, means, op, H, W, B, True)
+    rb = ref.bin_and_sort(xys, ext, cnt, H, W, B)
+    mb = ops.bin_gaussians(xys, ext, cnt, H, W, B, want_keys=True)
+    M = rb.num_intersects
+    assert mb.num_intersects == M
+    assert torch.equal(mb.cum_tiles_hit, rb.cum_tiles_hit)
+    assert torch.equal(mb.isect_ids[:M], rb.isect_ids)
+    assert torch.equal(mb.gaussian_ids[:M], rb.gaussian_ids)
+    assert torch.equal(mb.isect_ids_sorted[:M], rb.isect_ids_sorted)
+    assert torch.equal(mb.gaussian_ids_sorted[:M], rb.gaussian_ids_sorted)
+    assert torch.equal(mb.tile_bins, rb.tile_bins)
+
+
+def test_binning_speculative_capacity_retry():
+    """A capacity guess below the true count is detected and redone."""
+    H, W, B = 128, 128, 16
+    means, L, colors, op = scene(800, H, W, diag=(0.5, 4.0))
+    xys, ext, con, cnt = ops.project_fwd(L, means, op, H, W, B, True)
+    key = (xys.shape[0], H, W, B, xys.device.index)
+    ops._CAP_HINT[key] = 10  # far too small
+    mb = ops.bin_gaussians(xys, ext, cnt, H, W, B)
+    rb = ref.bin_and_sort(xys, ext, cnt, H, W, B)
+    assert mb.num_intersects == rb.num_intersects
+    assert mb.capacity >= rb.num_intersects
+    assert torch.equal(mb.gaussian_ids_sorted[:rb.num_intersects], rb.gaussian_ids_sorted)
+    assert torch.equal(mb.tile_bins, rb.tile_bins)
+
+
+def _my_render(L, means, colors, op, H, W, B, ga):
+    xys, ext, con, cnt = ops.project_fwd(L, means, op, H, W, B, True)
+    mb = ops.bin_gaussians(xys, ext, cnt, H, W, B)
+    out = ops.raster_fwd(H, W, B, mb.gaussian_ids_sorted, mb.tile_bins, mb.total, xys, con,
+                         colors, op, ga)
+    return (xys, ext, con, cnt), mb, out
+
+
+@pytest.mark.parametrize("case", CASES, ids=_ids)
+@pytest.mark.parametrize("ga", [False, True], ids=["sum", "gradaware"])
+def test_raster_forward(case, ga):
+    n, H, W, B, diag, opac = case
+    means, L, colors, op = scene(n, H, W, diag=diag, opac=opac)
+    r = ref.render(L, means, colors, op, H, W, B, True, ga)
+    _, mb, (img, wsum, dx, dy, dxy, fin) = _my_render(L, means, colors, op, H, W, B, ga)
+    assert torch.equal(fin, r["final_idx"])
+    assert (img - r["img"]).abs().max().item() <= IMG_TOL
+    assert (wsum - r["wsum"]).abs().max().item() <= IMG_TOL
+    if ga:
+        for a, k in zip((dx, dy, dxy), ("dx", "dy", "dxy")):
+            assert (a - r[k]).abs().max().item() <= IMG_TOL, k
+
+
+@pytest.mark.parametrize("case", CASES, ids=_ids)
+@pytest.mark.parametrize("ga", [False, True], ids=["sum", "gradaware"])
+def test_raster_backward(case, ga):
+    n, H, W, B, diag, opac = case
+    means, L, colors, op = scene(n, H, W, diag=diag, opac=opac)
+    r = ref.render(L, means, colors, op, H, W, B, True, ga)
+    (xys, ext, con, cnt), mb, (img, wsum, dx, dy, dxy, fin) = _my_render(L, means, colors, op, H,
+                                                                        W, B, ga)
+    g = torch.Generator().manual_seed(3)
+    cot = [torch.randn(s, generator=g).cuda() for s in [(H, W, 3), (H, W), (H, W, 3), (H, W, 3),
+                                                        (H, W, 3)]]
+    vd = cot[2:] if ga else [None, None, None]
+    rg = ref.raster_bwd(H, W, B, r["binning"], r["xys"], r["conics"], colors, op,
+                        r["final_idx"], cot[0], cot[1], *vd)
+    v_xy, v_abs, v_con, v_rgb, v_op = ops.raster_bwd(H, W, B, mb.gaussian_ids_sorted,
+                                                     mb.tile_bins, mb.total, xys, con, colors,
+                                                     op, fin, cot[0], cot[1], *vd)
+    for a, k in [(v_xy, "v_xy"), (v_abs, "v_xy_abs"), (v_con, "v_conic"), (v_rgb, "v_rgb"),
+                 (v_op, "v_opacity")]:
+        if rg[k] is None:
+            assert a is None
+            continue
+        assert rel_err(np_(a), np_(rg[k])) <= GRAD_TOL, k
+
+
+@pytest.mark.parametrize("chol", [True, False])
+def test_projection_backward(chol):
+    n, H, W, B = 2000, 200, 180, 16
+    means, L, colors, op = scene(n, H, W, diag=(0.5, 5.0), opac=(0.01, 1.0))
+    in3 = L if chol else chol_to_cov(L)
+    xys, ext, con, cnt = ref.project_fwd(in3, means, op, H, W, B, chol)
+    g = torch.Generator().manual_seed(3)
+    v_xy = torch.randn(n, 2, generator=g).cuda()
+    v_con = torch.randn(n, 3, generator=g).cuda()
+    r_in3, r_mean = ref.project_bwd(ext, in3, con, v_xy, v_con, chol)
+    s_in3, s_mean = ops.project_bwd_saved(ext, in3, con, v_xy, v_con, chol)
+    m_in3, m_mean = ops.project_bwd(in3, means, op, H, W, B, chol, v_xy, v_con)
+    assert torch.equal(s_mean, r_mean) and torch.equal(m_mean, r_mean)
+    assert rel_err(np_(s_in3), np_(r_in3)) <= 1e-6
+    assert torch.equal(m_in3, s_in3)
+
+
+@pytest.mark.parametrize("shape", [(64, 80, 256, 320), (50, 37, 200, 148), (128, 128, 512, 512),
+                                   (40, 60, 97, 131), (64, 64, 48, 40)])
+def test_upscale_half_pixel(shape):
+    h, w, dh, dw = shape
+    g = torch.Generator().manual_seed(5)
+    planes = [torch.randn(h, w, 3, generator=g).cuda() for _ in range(4)]
+    r = ref.upscale_fwd(*planes, dh, dw)
+    m = ops.upscale_fwd(*planes, dh, dw, mode=0)
+    assert (m - r).abs().max().item() <= IMG_TOL
+    go = torch.randn(dh, dw, 3, generator=g).cuda()
+    rg = ref.upscale_bwd(go, h, w)
+    mg = ops.upscale_bwd(go, h, w, mode=0)
+    for a, b in zip(mg, rg):
+        assert rel_err(np_(a), np_(b)) <= GRAD_TOL
+
+
+def test_upscale_roi():
+    h, w = 96, 128
+    g = torch.Generator().manual_seed(6)
+    planes = [torch.randn(h, w, 3, generator=g).cuda() for _ in range(4)]
+    for roi, dh, dw in [((10.0, 20.0, 74.5, 60.0), 160, 256), ((0.0, 0.0, 64.0, 48.0), 96, 128),
+                        ((31.0, 7.0, 95.0, 71.0), 64, 64)]:
+        r = ref.upscale_fwd(*planes, dh, dw, roi)
+        m = ops.upscale_fwd(*planes, dh, dw, roi, mode=0)
+        assert (m - r).abs().max().item() <= IMG_TOL
+        go = torch.randn(dh, dw, 3, generator=g).cuda()
+        for a, b in zip(ops.upscale_bwd(go, h, w, roi, mode=0), ref.upscale_bwd(go, h, w, roi)):
+            assert rel_err(np_(a), np_(b)) <= GRAD_TOL
