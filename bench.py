@@ -1,0 +1,342 @@
+"""Benchmark: LIG fit iterations/s at 8192^2 (level 2 of the two-level fit).
+
+Workload (one "step"): one fit iteration of LIG's full-resolution level —
+2M Cholesky Gaussians (means U[0,8192)^2, diagonals U[0.5,6], off-diagonal
+N(0,0.5), colours U(0,1)) on an 8192x8192 RGB fp32 target (a render of 2M
+seeded teacher Gaussians plus 1/f^2 noise of std 0.03, clipped): project ->
+bin -> raster forward -> clamp -> L2 -> raster backward -> projection
+backward -> Adam, through the drop-in gsplat2d API.  Synthetic data stands
+in for the DIV2K/STimage images (not available offline).
+
+  value  device-timed iterations/s, target resident in HBM (inputs > L2).
+  e2e    same loop through the public API with the step's input (the target
+         image) copied host->device from pinned memory and the loss read
+         back every step.
+  roofline  the dominant kernel's algorithmic rate (reference-defined
+         Gaussian-pixel evaluations x FLOP per evaluation) / measured FP32
+         FMA peak of this device.
+  cpu_baseline  the C restatement of the reference algorithm (oracle/) on
+         this host's cores, on a horizontal band of the same workload.
+
+`--impl reference` times that CPU implementation (the reference has no CPU
+path of its own; its GPU kernels are compared in tests/) and prints the
+same metric.  Multi-GPU: independent replicas (no data-path collective),
+value = total iterations of all ranks / max rank time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+import torch
+import torch.distributed as dist
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "LIG fit iters/s (fwd+bwd) at 8192^2, PSNR-matched; render p50/p99 ms"
+H = W = 8192
+N_FIT = 2_000_000
+N_TEACHER = 2_000_000
+DIAG = (0.5, 6.0)
+BLOCK = 16
+FLOP_PER_EVAL = {"lig_raster_fwd": 20.0, "lig_raster_bwd": 40.0}
+CLOCK_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["lig", "reference"], default="lig")
+    ap.add_argument("--size", type=int, default=H, help="image side (default 8192)")
+    ap.add_argument("--points", type=int, default=None,
+                    help="fitted Gaussians (default 2M scaled by (size/8192)^2)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0,
+                    help="approximate CPU work per baseline sample")
+    return ap.parse_args()
+
+
+def points_for(args) -> int:
+    if args.points is not None:
+        return args.points
+    return max(1, int(N_FIT * (args.size / H) ** 2))
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={CLOCK_FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        return False
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                    rows.append(parts)
+        finally:
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v == "Active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]),
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+
+
+# ------------------------------------------------------------------ setup
+def make_workload(size: int, n: int, device):
+    from lig_b200 import synthetic
+    from lig_b200.fit import LevelFit, make_target
+    n_teacher = max(1, int(N_TEACHER * (size / H) ** 2))
+    target = make_target(size, size, n_teacher, DIAG, noise="spectral", noise_std=0.03,
+                         device=device, block=BLOCK)
+    fit = LevelFit(n, size, size, device=device, lr=1e-3, block=BLOCK, diag=DIAG,
+                   seed=synthetic.SEED_INIT)
+    return target, fit
+
+
+def evaluations(fit) -> tuple[int, int]:
+    """(M, E): intersections and reference-defined Gaussian-pixel evaluations
+    (sum over tiles of list length x pixels of the tile inside the image)."""
+    from lig_b200 import ops
+    with torch.no_grad():
+        xys, ext, con, cnt = ops.project_fwd(fit.chol, fit.means, None, fit.H, fit.W, fit.block,
+                                             True)
+        b = ops.bin_gaussians(xys, ext, cnt, fit.H, fit.W, fit.block)
+        tbx, tby = ops.tile_bounds(fit.H, fit.W, fit.block)
+        lens = (b.tile_bins[:, 1] - b.tile_bins[:, 0]).to(torch.int64)
+        tx = torch.arange(tbx * tby, device=lens.device) % tbx
+        ty = torch.arange(tbx * tby, device=lens.device) // tbx
+        pw = torch.clamp(fit.W - tx * fit.block, max=fit.block)
+        ph = torch.clamp(fit.H - ty * fit.block, max=fit.block)
+        e = int((lens * pw * ph).sum().item())
+    return b.num_intersects, e
+
+
+# -------------------------------------------------------------- CPU side
+def cpu_band_sample(size, n, target_secs, steps):
+    """Time the oracle (C restatement, OpenMP) on horizontal bands of the
+    workload; returns (iters/s for the full image, cores, description)."""
+    from lig_b200 import synthetic
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    means, chol, colors = synthetic.gaussians(n, size, size, diag=DIAG, seed=synthetic.SEED_INIT)
+    means, chol, colors = means.numpy(), chol.numpy(), colors.numpy()
+    rng = np.random.default_rng(0)
+
+    def band_step(rows):
+        sel = (means[:, 1] >= -32) & (means[:, 1] < rows + 32)
+        m, L, c = means[sel], chol[sel], colors[sel]
+        tgt = rng.uniform(0, 1, (rows, size, 3)).astype(np.float32)
+        t0 = time.perf_counter()
+        xys, ext, con, cnt = O.project_fwd(L, m, None, rows, size, BLOCK, chol=True)
+        bn = O.bin_and_sort(xys, ext, cnt, rows, size, BLOCK)
+        out = O.raster_fwd(rows, size, BLOCK, bn, xys, con, c, None)
+        img = out["img"]
+        v_img = (2.0 / img.size) * (np.clip(img, 0, 1) - tgt) * ((img >= 0) & (img <= 1))
+        g = O.raster_bwd(rows, size, BLOCK, bn, xys, con, c, None, out["final_idx"],
+                         v_img.astype(np.float32), np.zeros((rows, size), np.float32))
+        O.project_bwd(ext, L, con, g["v_xy"], g["v_conic"], chol=True)
+        return time.perf_counter() - t0
+
+    probe_rows = max(BLOCK, (size // 64) // BLOCK * BLOCK)
+    t_probe = band_step(probe_rows)
+    rows = int(min(size, max(BLOCK, probe_rows * target_secs / max(t_probe, 1e-3))))
+    rows = max(BLOCK, rows // BLOCK * BLOCK)
+    times = [band_step(rows) for _ in range(steps)]
+    t = statistics.median(times)
+    full_secs = t * size / rows
+    desc = (f"{rows}x{size} band of the {size}^2 level-2 fit step (Gaussians with centres in "
+            f"the band +-32 px), project+bin+raster fwd+L2 grad+raster bwd+proj bwd, "
+            f"fp32, scaled by {size / rows:.2f} to the full image; median of {steps}")
+    return 1.0 / full_secs, cores, desc, times, rows
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    size = args.size
+    n = points_for(args)
+    per_step = max(1.0, 120.0 / max(args.steps + args.warmup, 1))
+    _, cores, desc, times, rows = cpu_band_sample(size, n, per_step, args.warmup + args.steps)
+    timed = times[args.warmup:] or times
+    secs = statistics.median(timed) * size / rows
+    val = 1.0 / secs
+    line = {"metric": METRIC, "value": val, "unit": "iters/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"LIG level-2 fit step, {size}x{size} RGB, {n} Gaussians, "
+                                   f"16x16 tiles (CPU: band sample)",
+                       "global_batch": 1, "parallelism": "replicas"},
+            "cpu_baseline": {"value": val, "unit": "iters/s", "cores": cores, "kind": "port",
+                             "sample": desc},
+            "e2e": {"value": val, "unit": "iters/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# -------------------------------------------------------------- GPU side
+def run_lig(args, rank, world, local_rank):
+    from lig_b200 import _lib, ops
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    size = args.size
+    n = points_for(args)
+    target, fit = make_workload(size, n, dev)
+    for _ in range(args.warmup):
+        fit.step(target)
+    torch.cuda.synchronize()
+    m_isect, evals = evaluations(fit)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---- device-timed loop (value)
+    l0 = _lib.lib.lig_kernel_launches()
+    barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index) as clocks, ops.KernelTimer() as kt:
+        start.record()
+        for _ in range(args.steps):
+            fit.step(target)
+        end.record()
+        torch.cuda.synchronize()
+    barrier()
+    launches = (_lib.lib.lig_kernel_launches() - l0) / args.steps
+    ms = start.elapsed_time(end)
+    ms_t = torch.tensor([ms], device=dev)
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = world * args.steps / (ms_max / 1e3)
+    per = kt.summary()
+    clk = clocks.summary()
+
+    # ---- end-to-end loop through the public API with host buffers
+    host_target = target.cpu().pin_memory()
+    dev_target = torch.empty_like(target)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        dev_target.copy_(host_target, non_blocking=True)
+        loss = fit.step(dev_target)
+        _ = loss.item()
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = torch.tensor([e0.elapsed_time(e1)], device=dev)
+    if world > 1:
+        dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
+    e2e = world * args.steps / (float(e2e_ms.item()) / 1e3)
+
+    if rank != 0:
+        return
+    # ---- roofline of the dominant kernel
+    fp32_peak = ops.probe_fp32(dev)
+    kernels = {}
+    for name, (calls, tot) in per.items():
+        k = {"calls_per_step": calls / args.steps, "ms_per_step": tot / args.steps,
+             "ms_per_call": tot / calls}
+        if name in FLOP_PER_EVAL:
+            rate = FLOP_PER_EVAL[name] * evals / (k["ms_per_call"] / 1e3)
+            k.update(algorithmic_tflops=rate / 1e12, frac_of_fp32=rate / fp32_peak)
+        kernels[name] = k
+    dom = max(kernels, key=lambda k: kernels[k]["ms_per_step"])
+    dk = kernels[dom]
+    if dom in FLOP_PER_EVAL:
+        achieved = FLOP_PER_EVAL[dom] * evals / (dk["ms_per_call"] / 1e3) / 1e12
+        roof = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak / 1e12,
+                "unit": "TFLOP/s", "frac": achieved * 1e12 / fp32_peak, "traffic": None,
+                "kernel": dom, "per_launch_units": evals,
+                "note": "algorithmic = reference Gaussian-pixel evaluations x FLOP/eval "
+                        f"({FLOP_PER_EVAL[dom]:.0f}); peak = FP32 FMA probe measured on this "
+                        "device (a SIMT-bound kernel: neither HBM nor tensor cores bound it)"}
+    else:
+        roof = {"bound": "hbm", "achieved": None, "peak": None, "unit": "GB/s", "frac": None,
+                "traffic": None, "kernel": dom}
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        v, cores, desc, _, _ = cpu_band_sample(size, n, args.cpu_seconds, 1)
+        cpu = {"value": v, "unit": "iters/s", "cores": cores, "kind": "port", "sample": desc}
+    line = {"metric": METRIC, "value": value, "unit": "iters/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"LIG level-2 fit step, {size}x{size} RGB fp32, {n} "
+                                   f"Gaussians (diag U[0.5,6]), 16x16 tiles, L2 + Adam",
+                       "global_batch": world, "seq_len": None,
+                       "parallelism": f"replicas{world}",
+                       "l2": "inputs > L2 (805 MB image per step)",
+                       "intersections": m_isect, "evaluations": evals},
+            "e2e": {"value": e2e, "unit": "iters/s",
+                    "h2d_bytes_per_step": int(target.numel() * 4), "d2h_bytes_per_step": 4},
+            "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+            "kernels": kernels}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        from datetime import timedelta
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    try:
+        run_lig(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -39,6 +39,10 @@ extern "C" {
 /* ABI version (bumped on any signature change). */
 int lig_abi_version(void);
 
+/* Number of CUDA kernels this library has launched in this process (all
+ * devices, all threads) — for launch accounting by benchmarks. */
+int64_t lig_kernel_launches(void);
+
 /* ------------------------------------------------------------ projection */
 
 /* Projection forward: conic, SnugBox extent, tile bbox and tile-hit count per
@@ -172,6 +176,13 @@ int lig_upscale_bwd(int dtype, int mode, int src_h, int src_w, int dst_h, int ds
                     double roi_x1, double roi_y1, double roi_x2, double roi_y2,
                     const void *grad_out, void *grad_render, void *grad_dx, void *grad_dy,
                     void *grad_dxy, void *stream);
+
+/* ----------------------------------------------------------------- probes */
+
+/* FP32 FMA throughput probe: blocks x 256 threads, each `iters` x 8
+ * independent FMAs (2 FLOP each).  Used to measure the FP32 roofline
+ * denominator on the device.  No reference counterpart (measurement aid). */
+int lig_probe_fp32(int blocks, int iters, float *out, void *stream);
 
 #ifdef __cplusplus
 }

@@ -6,6 +6,7 @@ include/lig_b200.h), loaded at import; there is no CPU fallback.
     import lig_b200
     lig_b200.install_gsplat2d()      # `import gsplat2d` / `upscaler_torch` now resolve here
 """
+import importlib
 import sys
 
 from . import _lib  # noqa: F401  (loads liblig_b200.so; raises if missing)
@@ -20,17 +21,10 @@ def install_gsplat2d() -> None:
     """Register this package under the reference's module names so that LIG's
     own code (gaussianlig.py, train.py, minimal_trainer_upscale.py) imports it
     unchanged: gsplat2d, gsplat2d.<submodule>, gsplat2d.cuda, upscaler_torch."""
-    from .gsplat2d import (cuda, project_gaussians, project_gaussians_cholesky, rasterize,
-                           upscale, utils, version)
-    mods = {
-        "gsplat2d": gsplat2d,
-        "gsplat2d.cuda": cuda,
-        "gsplat2d.project_gaussians": project_gaussians,
-        "gsplat2d.project_gaussians_cholesky": project_gaussians_cholesky,
-        "gsplat2d.rasterize": rasterize,
-        "gsplat2d.upscale": upscale,
-        "gsplat2d.utils": utils,
-        "gsplat2d.version": version,
-        "upscaler_torch": upscaler_torch,
-    }
+    # submodules by module path: the package attributes `project_gaussians` etc.
+    # are the functions (as in the reference's __init__), not the modules
+    mods = {"gsplat2d": gsplat2d, "upscaler_torch": upscaler_torch}
+    for sub in ("cuda", "project_gaussians", "project_gaussians_cholesky", "rasterize",
+                "upscale", "utils", "version"):
+        mods["gsplat2d." + sub] = importlib.import_module(f"{__name__}.gsplat2d.{sub}")
     sys.modules.update(mods)

@@ -37,6 +37,7 @@ SZ = ctypes.c_size_t
 # name -> (restype, argtypes), mirroring include/lig_b200.h
 SIGNATURES = {
     "lig_abi_version": (I, []),
+    "lig_kernel_launches": (I64, []),
     "lig_project_fwd": (I, [I, I, I, P, P, P, I, I, I, P, P, P, P, P]),
     "lig_project_bwd": (I, [I, I, I, P, P, P, I, I, I, P, I64, P, I64, P, P, P]),
     "lig_project_bwd_saved": (I, [I, I, I, P, P, P, P, P, P, P, P]),
@@ -53,6 +54,7 @@ SIGNATURES = {
                            P, P, P, P, P, P]),
     "lig_upscale_fwd": (I, [I, I, I, I, I, I, D, D, D, D, P, P, P, P, P, P]),
     "lig_upscale_bwd": (I, [I, I, I, I, I, I, D, D, D, D, P, P, P, P, P, P]),
+    "lig_probe_fp32": (I, [I, I, P, P]),
 }
 
 

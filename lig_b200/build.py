@@ -3,6 +3,8 @@
 Compiles every ``lig_b200/csrc/*.cu`` with nvcc for ``sm_100a`` into
 ``lig_b200/_build/*.o`` (in parallel, skipping up-to-date objects) and links
 ``lig_b200/liblig_b200.so``, which ``lig_b200._lib`` loads through ctypes.
+Run it as a script (``python lig_b200/build.py``): importing the package
+loads the library, which must exist first.
 
 Flags: ``-O3 --use_fast_math`` matches the reference's setup.py
 (gsplat2d/setup.py:65-77), which the bit-exact tile counts and alpha-threshold

@@ -124,6 +124,7 @@ inline int device_scan(const uint32_t *in, uint32_t *out, int n, bool inclusive,
     scan_reduce_kernel<<<nb, kScanThreads, 0, s>>>(in, n, partials);
     scan_partials_kernel<<<1, 1024, 0, s>>>(partials, nb);
     scan_final_kernel<<<nb, kScanThreads, 0, s>>>(in, n, partials, inclusive, out, total_out);
+    note_launches(3);
     LIG_LAUNCH_CHECK();
     return LIG_OK;
 }
@@ -455,6 +456,7 @@ int run_bin(int n, const void *xys, const void *ext, const int32_t *cum, const i
     cudaMemsetAsync(tile_bins, 0, sizeof(int32_t) * 2 * (size_t)T_, s);
     if (n == 0 || capacity == 0) {
         flag_overflow_kernel<<<1, 1, 0, s>>>(d_total, capacity, status);
+        note_launches(1);
         LIG_LAUNCH_CHECK();
         return LIG_OK;
     }
@@ -469,6 +471,7 @@ int run_bin(int n, const void *xys, const void *ext, const int32_t *cum, const i
     emit_kernel<T><<<eblocks, 256, 0, s>>>(n, (const T *)xys, (const T *)ext, cum, tbx, tby, b,
                                            capacity, ka, va, isect, gids, status);
     flag_overflow_kernel<<<1, 1, 0, s>>>(d_total, capacity, status);
+    note_launches(2);
     LIG_LAUNCH_CHECK();
 
     size_t dsm = downsweep_smem(p.bins);
@@ -484,6 +487,7 @@ int run_bin(int n, const void *xys, const void *ext, const int32_t *cum, const i
         if (rc) return rc;
         radix_downsweep_kernel<<<p.nblk, kSortThreads, dsm, s>>>(
             ka, va, kb, vb, d_total, capacity, shift, p.bins, hist, p.nblk);
+        note_launches(2);
         LIG_LAUNCH_CHECK();
         uint32_t *tk = ka; ka = kb; kb = tk;
         int32_t *tv = va; va = vb; vb = tv;
@@ -495,6 +499,7 @@ int run_bin(int n, const void *xys, const void *ext, const int32_t *cum, const i
     if (isect_sorted)
         widen_keys_kernel<<<(capacity + 255) / 256, 256, 0, s>>>(ka, d_total, capacity,
                                                                  isect_sorted);
+    note_launches(isect_sorted ? 2 : 1);
     LIG_LAUNCH_CHECK();
     return LIG_OK;
 }
@@ -566,6 +571,7 @@ extern "C" int lig_map_intersects(int dtype, int n, int m, const void *xys, cons
                                                     nullptr, nullptr);
     else
         return LIG_ERR_INVALID;
+    note_launches(1);
     LIG_LAUNCH_CHECK();
     return LIG_OK;
 }
@@ -578,6 +584,7 @@ extern "C" int lig_tile_bin_edges(int m, const int64_t *isect_sorted, int num_ti
     if (m > 0)
         tile_ranges_kernel<int64_t><<<(m + 255) / 256, 256, 0, s>>>(isect_sorted, nullptr, m, m,
                                                                     (int2 *)tile_bins);
+    note_launches(m > 0 ? 1 : 0);
     LIG_LAUNCH_CHECK();
     return LIG_OK;
 }

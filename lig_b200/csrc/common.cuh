@@ -81,6 +81,9 @@ __device__ __forceinline__ bool cov2d_bounds(T cx, T cy, T cz, T opacity, T &ca,
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31; }
 
+// Process-wide count of kernel launches issued by this library.
+void note_launches(int n);
+
 }  // namespace lig
 
 // Host-side launch check: every entry point returns a LIG_* status.

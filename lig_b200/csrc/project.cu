@@ -4,6 +4,8 @@
 // One thread per Gaussian; the kernels are HBM-bound (52 B/Gaussian forward).
 // Every output element is written, so callers need no zero-fill (the reference
 // pre-zeroes with torch::zeros, csrc/bindings.cu:89-97).
+#include <atomic>
+
 #include "common.cuh"
 
 namespace lig {
@@ -203,6 +205,7 @@ int project_fwd(int n, int chol, const void *in3, const void *means, const void 
     project_fwd_kernel<T><<<proj_blocks(n), kProjThreads, 0, s>>>(
         n, chol != 0, (const T *)in3, (const T *)means, (const T *)opac, tbx, tby, b, (T *)xys,
         (T *)ext, (T *)con, cnt);
+    note_launches(1);
     LIG_LAUNCH_CHECK();
     return LIG_OK;
 }
@@ -216,6 +219,7 @@ int project_bwd(int n, int chol, const void *in3, const void *means, const void 
     project_bwd_kernel<T><<<proj_blocks(n), kProjThreads, 0, s>>>(
         n, chol != 0, (const T *)in3, (const T *)means, (const T *)opac, tbx, tby, b,
         (const T *)v_xy, sxy, (const T *)v_con, sco, (T *)v_in3, (T *)v_mean);
+    note_launches(1);
     LIG_LAUNCH_CHECK();
     return LIG_OK;
 }
@@ -224,7 +228,14 @@ int project_bwd(int n, int chol, const void *in3, const void *means, const void 
 
 using namespace lig;
 
+namespace lig {
+static std::atomic<long long> g_launches{0};
+void note_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+}  // namespace lig
+
 extern "C" int lig_abi_version(void) { return 1; }
+
+extern "C" int64_t lig_kernel_launches(void) { return (int64_t)lig::g_launches.load(); }
 
 extern "C" int lig_project_fwd(int dtype, int n, int chol, const void *in3, const void *means,
                                const void *opac, int h, int w, int b, void *xys, void *ext,
@@ -271,6 +282,7 @@ extern "C" int lig_project_bwd_saved(int dtype, int n, int chol, const void *ext
             (const double *)v_xy, (const double *)v_con, (double *)v_in3, (double *)v_mean);
     else
         return LIG_ERR_INVALID;
+    note_launches(1);
     LIG_LAUNCH_CHECK();
     return LIG_OK;
 }
@@ -288,6 +300,7 @@ extern "C" int lig_cov2d_bounds(int dtype, int n, const void *cov, const void *o
             n, (const double *)cov, (const double *)opac, (double *)con, (double *)ext);
     else
         return LIG_ERR_INVALID;
+    note_launches(1);
     LIG_LAUNCH_CHECK();
     return LIG_OK;
 }

@@ -570,6 +570,7 @@ int pack(int n, const void *xys, const void *con, const void *col, const void *o
     if (n > 0)
         pack_kernel<T><<<(n + 255) / 256, 256, 0, s>>>(n, (const T *)xys, (const T *)con,
                                                       (const T *)col, (const T *)op, (Rec<T> *)ws);
+    note_launches(n > 0 ? 1 : 0);
     LIG_LAUNCH_CHECK();
     return LIG_OK;
 }
@@ -595,6 +596,7 @@ int raster_fwd(int H, int W, int B, int n, const int32_t *ids, const int32_t *bi
         raster_fwd_kernel<T, false, Cfg<T>::kFwd><<<grid, 32 * kWarpsPerCta, 0, s>>>(
             H, W, B, tbx, nbands, nwork, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws,
             (T *)img, (T *)wsum, nullptr, nullptr, nullptr, fin);
+    note_launches(1);
     LIG_LAUNCH_CHECK();
     return LIG_OK;
 }
@@ -630,6 +632,7 @@ int raster_bwd(int H, int W, int B, int n, const int32_t *ids, const int32_t *bi
         raster_bwd_kernel<T, false, Cfg<T>::kBwd><<<grid, 32 * kWarpsPerCta, 0, s>>>(
             H, W, B, tbx, nbands, nwork, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws,
             fin, (const T *)v_img, (const T *)v_wsum, nullptr, nullptr, nullptr, cl, g);
+    note_launches(1);
     LIG_LAUNCH_CHECK();
     return LIG_OK;
 }

@@ -379,6 +379,7 @@ int upscale_fwd(int mode, int src_h, int src_w, int dst_h, int dst_w, double x1,
     dim3 grid((dst_w + kFwdCols - 1) / kFwdCols, (dst_h + kFwdRows - 1) / kFwdRows);
     upscale_fwd_kernel<T><<<grid, kFwdThreads, sm, s>>>(mx, my, src_w, (const T *)f, (const T *)fx,
                                                        (const T *)fy, (const T *)fxy, (T *)out);
+    note_launches(1);
     LIG_LAUNCH_CHECK();
     return LIG_OK;
 }
@@ -394,6 +395,7 @@ int upscale_bwd(int mode, int src_h, int src_w, int dst_h, int dst_w, double x1,
     dim3 grid((src_w + kBwdTexW - 1) / kBwdTexW, (src_h + kBwdTexH - 1) / kBwdTexH);
     upscale_bwd_kernel<T><<<grid, kBwdThreads, sm, s>>>(mx, my, src_w, src_h, (const T *)g,
                                                        (T *)gf, (T *)gfx, (T *)gfy, (T *)gfxy);
+    note_launches(1);
     LIG_LAUNCH_CHECK();
     return LIG_OK;
 }

@@ -23,7 +23,7 @@ from typing import Optional
 import torch
 
 from . import _lib
-from ._lib import call
+from ._lib import call as _raw_call
 
 _VP = ctypes.c_void_p
 
@@ -60,6 +60,68 @@ def _c(t: Optional[torch.Tensor], dtype=None) -> Optional[torch.Tensor]:
 
 def tile_bounds(img_h: int, img_w: int, block: int):
     return (img_w + block - 1) // block, (img_h + block - 1) // block
+
+
+# Optional per-entry-point timing with CUDA events on the launching stream
+# (used by bench.py inside its timed region).
+_TIMER = None
+
+
+def call(name, *args):
+    t = _TIMER
+    if t is None:
+        return _raw_call(name, *args)
+    s = torch.cuda.Event(enable_timing=True)
+    e = torch.cuda.Event(enable_timing=True)
+    s.record()
+    _raw_call(name, *args)
+    e.record()
+    t.append((name, s, e))
+
+
+class KernelTimer:
+    """Context manager: records (entry point, start, end) events for every
+    lig_* call made inside it; summary() -> {name: (calls, total_ms)}."""
+
+    def __enter__(self):
+        global _TIMER
+        self.events = []
+        _TIMER = self.events
+        return self
+
+    def __exit__(self, *exc):
+        global _TIMER
+        _TIMER = None
+        return False
+
+    def summary(self):
+        torch.cuda.synchronize()
+        out = {}
+        for name, s, e in self.events:
+            n, ms = out.get(name, (0, 0.0))
+            out[name] = (n + 1, ms + s.elapsed_time(e))
+        return out
+
+
+def probe_fp32(device=None, blocks=None, iters=4096):
+    """Measured FP32 FMA throughput of this device (FLOP/s)."""
+    dev = torch.device(device or "cuda")
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    blocks = blocks or sms * 8
+    out = torch.empty((blocks,), dtype=torch.float32, device=dev)
+    st = _stream(dev)
+    for _ in range(2):
+        _raw_call("lig_probe_fp32", blocks, iters, _p(out), st)
+    s = torch.cuda.Event(enable_timing=True)
+    e = torch.cuda.Event(enable_timing=True)
+    s.record()
+    reps = 5
+    for _ in range(reps):
+        _raw_call("lig_probe_fp32", blocks, iters, _p(out), st)
+    e.record()
+    torch.cuda.synchronize()
+    secs = s.elapsed_time(e) / 1e3
+    return reps * blocks * 256.0 * iters * 8 * 2 / secs
 
 
 # ------------------------------------------------------------------ projection

@@ -21,11 +21,11 @@ from tests._scene import scene  # noqa: E402
 
 CASES = {
     # name: (n, H, W, B, diag, opacity range)
-    "b16_op": (300, 70, 90, 16, (0.5, 4.0), (0.0, 1.0)),
-    "b16_noop": (350, 64, 64, 16, (0.5, 6.0), None),
-    "b12_op": (250, 50, 61, 12, (0.3, 3.0), (0.1, 0.95)),
-    "b8_noop": (200, 40, 48, 8, (0.5, 3.0), None),
+    "b16_op": (170, 40, 52, 16, (0.5, 4.0), (0.0, 1.0)),
+    "b12_op": (120, 36, 45, 12, (0.3, 3.0), (0.1, 0.95)),
+    "b8_noop": (100, 32, 32, 8, (0.5, 3.0), None),
 }
+UP_H, UP_W = 14, 18  # source planes of the upscale cases
 
 
 def np_(t):
@@ -65,14 +65,14 @@ def case(name, n, H, W, B, diag, opac, out_dir):
     v_in3, v_mean = ref.project_bwd(ext, L, con, v_xy, v_con, True)
     d.update(pb_v_xy=np_(v_xy), pb_v_conic=np_(v_con), pb_v_chol=np_(v_in3), pb_v_mean=np_(v_mean))
     # upscale: render planes -> 3x and a ROI crop
-    planes = [torch.randn(H, W, 3, generator=g).cuda() for _ in range(4)]
+    planes = [torch.randn(UP_H, UP_W, 3, generator=g).cuda() for _ in range(4)]
     d.update(up_f=np_(planes[0]), up_fx=np_(planes[1]), up_fy=np_(planes[2]), up_fxy=np_(planes[3]))
-    roi = (3.0, 5.0, float(W) - 7.5, float(H) - 2.0)
-    for tag, r_, dh, dw in (("full", None, 3 * H, 3 * W), ("roi", roi, 2 * H, 2 * W)):
+    roi = (3.0, 2.0, float(UP_W) - 4.5, float(UP_H) - 1.0)
+    for tag, r_, dh, dw in (("full", None, 3 * UP_H, 3 * UP_W), ("roi", roi, 2 * UP_H, 2 * UP_W)):
         d[f"up_{tag}_out"] = np_(ref.upscale_fwd(*planes, dh, dw, r_))
         go = torch.randn(dh, dw, 3, generator=g).cuda()
         d[f"up_{tag}_g"] = np_(go)
-        for k, v in zip(("gf", "gfx", "gfy", "gfxy"), ref.upscale_bwd(go, H, W, r_)):
+        for k, v in zip(("gf", "gfx", "gfy", "gfxy"), ref.upscale_bwd(go, UP_H, UP_W, r_)):
             d[f"up_{tag}_{k}"] = np_(v)
     d["up_roi"] = np.array(roi)
     path = os.path.join(out_dir, f"ref_{name}.npz")
