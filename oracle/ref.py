@@ -24,8 +24,17 @@ from typing import Optional
 import torch
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
+# Tests synchronise around every reference launch (clear error attribution);
+# timing runs set this False so the reference runs with only its own
+# host synchronisations (the .item() of utils.py:66).
+STRICT_SYNC = True
 LIB_PATH = os.path.join(_HERE, "_ref", "libgsplat2d_ref.so")
 _lib = None
+
+
+def _sync():
+    if STRICT_SYNC:
+        torch.cuda.synchronize()
 
 
 def available() -> bool:
@@ -61,10 +70,10 @@ def project_fwd(in3, means, opac, H, W, B, chol=True):
     ext = torch.empty(n, 2, device=dev)
     con = torch.empty(n, 3, device=dev)
     cnt = torch.empty(n, dtype=torch.int32, device=dev)
-    torch.cuda.synchronize()
+    _sync()
     _chk(lib().ref_project_fwd(n, int(chol), _p(_f(in3)), _p(_f(means)), _p(_f(opac)), H, W, B,
                                _p(xys), _p(ext), _p(con), _p(cnt)), "ref_project_fwd")
-    torch.cuda.synchronize()
+    _sync()
     return xys, ext, con, cnt
 
 
@@ -73,11 +82,11 @@ def project_bwd(extents, in3, conics, v_xy, v_conic, chol=True):
     dev = extents.device
     v_in3 = torch.empty(n, 3, device=dev)
     v_mean = torch.empty(n, 2, device=dev)
-    torch.cuda.synchronize()
+    _sync()
     _chk(lib().ref_project_bwd(n, int(chol), _p(_f(extents)), _p(_f(in3)), _p(_f(conics)),
                                _p(_f(v_xy)), _p(_f(v_conic)), _p(v_in3), _p(v_mean)),
          "ref_project_bwd")
-    torch.cuda.synchronize()
+    _sync()
     return v_in3, v_mean
 
 
@@ -85,9 +94,9 @@ def cov2d_bounds(cov, opac=None):
     n = cov.shape[0]
     con = torch.empty(n, 3, device=cov.device)
     ext = torch.empty(n, 2, device=cov.device)
-    torch.cuda.synchronize()
+    _sync()
     _chk(lib().ref_cov2d_bounds(n, _p(_f(cov)), _p(_f(opac)), _p(con), _p(ext)), "ref_cov2d_bounds")
-    torch.cuda.synchronize()
+    _sync()
     return con, ext
 
 
@@ -112,16 +121,16 @@ def bin_and_sort(xys, extents, counts, H, W, B) -> RefBinning:
     depths = torch.zeros(n, device=dev)
     isect = torch.empty(m, dtype=torch.int64, device=dev)
     gids = torch.empty(m, dtype=torch.int32, device=dev)
-    torch.cuda.synchronize()
+    _sync()
     _chk(lib().ref_map_intersects(n, m, _p(_f(xys)), _p(depths), _p(_f(extents)), _p(cum), tbx,
                                   tby, B, _p(isect), _p(gids)), "ref_map_intersects")
-    torch.cuda.synchronize()
+    _sync()
     isect_sorted, order = torch.sort(isect, stable=True)
     gid_sorted = torch.gather(gids, 0, order)
     bins = torch.empty(tbx * tby, 2, dtype=torch.int32, device=dev)
-    torch.cuda.synchronize()
+    _sync()
     _chk(lib().ref_tile_bin_edges(m, _p(isect_sorted), tbx * tby, _p(bins)), "ref_tile_bin_edges")
-    torch.cuda.synchronize()
+    _sync()
     return RefBinning(m, cum, isect, gids, isect_sorted, gid_sorted, bins)
 
 
@@ -138,12 +147,12 @@ def raster_fwd(H, W, B, bn: RefBinning, xys, conics, colors, opac, grad_aware=Fa
     dx = torch.empty(H, W, 3, device=dev) if grad_aware else None
     dy = torch.empty(H, W, 3, device=dev) if grad_aware else None
     dxy = torch.empty(H, W, 3, device=dev) if grad_aware else None
-    torch.cuda.synchronize()
+    _sync()
     _chk(lib().ref_raster_fwd(H, W, B, _p(bn.gaussian_ids_sorted), _p(bn.tile_bins), _p(_f(xys)),
                               _p(_f(conics)), _p(_f(colors)), _p(_f(opac)), int(grad_aware),
                               _p(fin), _p(img), _p(wsum), _p(dx), _p(dy), _p(dxy)),
          "ref_raster_fwd")
-    torch.cuda.synchronize()
+    _sync()
     return dict(img=img, wsum=wsum, dx=dx, dy=dy, dxy=dxy, final_idx=fin)
 
 
@@ -157,13 +166,13 @@ def raster_bwd(H, W, B, bn: RefBinning, xys, conics, colors, opac, final_idx, v_
     v_rgb = torch.zeros(n, 3, device=dev)
     v_op = torch.zeros(n, device=dev) if opac is not None else None
     if bn.num_intersects >= 1:
-        torch.cuda.synchronize()
+        _sync()
         _chk(lib().ref_raster_bwd(H, W, B, n, _p(bn.gaussian_ids_sorted), _p(bn.tile_bins),
                                   _p(_f(xys)), _p(_f(conics)), _p(_f(colors)), _p(_f(opac)),
                                   _p(final_idx.contiguous()), _p(_f(v_img)), _p(_f(v_wsum)),
                                   _p(_f(v_dx)), _p(_f(v_dy)), _p(_f(v_dxy)), _p(v_xy), _p(v_abs),
                                   _p(v_con), _p(v_rgb), _p(v_op)), "ref_raster_bwd")
-        torch.cuda.synchronize()
+        _sync()
     return dict(v_xy=v_xy, v_xy_abs=v_abs, v_conic=v_con, v_rgb=v_rgb, v_opacity=v_op)
 
 
@@ -172,12 +181,12 @@ def upscale_fwd(f, fx, fy, fxy, dst_h, dst_w, roi=None):
     if roi is None:
         roi = (0.0, 0.0, float(w), float(h))
     out = torch.empty(dst_h, dst_w, 3, device=f.device)
-    torch.cuda.synchronize()
+    _sync()
     cf = ctypes.c_float
     _chk(lib().ref_upscale_fwd(h, w, dst_h, dst_w, cf(roi[0]), cf(roi[1]), cf(roi[2]), cf(roi[3]),
                                _p(_f(f)), _p(_f(fx)), _p(_f(fy)), _p(_f(fxy)), _p(out)),
          "ref_upscale_fwd")
-    torch.cuda.synchronize()
+    _sync()
     return out
 
 
@@ -186,11 +195,11 @@ def upscale_bwd(g, src_h, src_w, roi=None):
     if roi is None:
         roi = (0.0, 0.0, float(src_w), float(src_h))
     outs = [torch.empty(src_h, src_w, 3, device=g.device) for _ in range(4)]
-    torch.cuda.synchronize()
+    _sync()
     cf = ctypes.c_float
     _chk(lib().ref_upscale_bwd(src_h, src_w, dh, dw, cf(roi[0]), cf(roi[1]), cf(roi[2]),
                                cf(roi[3]), _p(_f(g)), *[_p(o) for o in outs]), "ref_upscale_bwd")
-    torch.cuda.synchronize()
+    _sync()
     return tuple(outs)
 
 

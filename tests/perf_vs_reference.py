@@ -1,0 +1,116 @@
+"""Fit speed and PSNR: this library vs the reference's own CUDA kernels.
+
+Both sides run the same LIG level fit (same seeded init, target and Adam
+settings): render -> clamp -> L2 -> backward -> Adam.  The reference side is
+its kernels (oracle/_ref, compiled from the reference sources) with its torch
+glue restated in oracle/ref.py — cumsum + .item(), torch.sort + gather — and
+the L2/clamp gradient computed as autograd would; only the reference's own
+host synchronisation remains.  Prints one JSON line per configuration.
+
+    python tests/perf_vs_reference.py [--configs c0,c1l2] [--iters N]
+"""
+import argparse
+import json
+import os
+import sys
+
+import torch
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+from lig_b200 import synthetic  # noqa: E402
+from lig_b200.fit import LevelFit, make_target, psnr  # noqa: E402
+from oracle import ref  # noqa: E402
+
+CONFIGS = {
+    # name: (H=W, fit N, teacher N, diag, noise, noise std, timed iters, psnr iters)
+    "c0": (512, 50_000, 20_000, (0.5, 4.0), "white", 0.02, 200, 1000),
+    "c1l2": (8192, 2_000_000, 2_000_000, (0.5, 6.0), "spectral", 0.03, 20, 100),
+    "c3": (4096, 1_000_000, 1_000_000, (0.5, 8.0), "white", 0.02, 20, 0),
+}
+
+
+class RefFit:
+    """The same fit driven by the reference kernels."""
+
+    def __init__(self, n, H, W, diag, lr=1e-3, B=16):
+        means, chol, colors = synthetic.gaussians(n, H, W, diag=diag, seed=synthetic.SEED_INIT)
+        self.means = means.cuda().requires_grad_()
+        self.chol = chol.cuda().requires_grad_()
+        self.rgbs = colors.cuda().requires_grad_()
+        self.H, self.W, self.B = H, W, B
+        self.opt = torch.optim.Adam([self.rgbs, self.means, self.chol], lr=lr, fused=True)
+
+    def render(self):
+        with torch.no_grad():
+            return ref.render(self.chol, self.means, self.rgbs, None, self.H, self.W, self.B)
+
+    def step(self, target):
+        H, W, B = self.H, self.W, self.B
+        with torch.no_grad():
+            r = ref.render(self.chol, self.means, self.rgbs, None, H, W, B)
+            img = r["img"]
+            c = torch.clamp(img, 0, 1)
+            diff = c - target
+            loss = (diff * diff).mean()
+            v_img = (2.0 / img.numel()) * diff * ((img >= 0) & (img <= 1))
+            v_w = torch.zeros(H, W, device=img.device)
+            g = ref.raster_bwd(H, W, B, r["binning"], r["xys"], r["conics"], self.rgbs, None,
+                               r["final_idx"], v_img, v_w)
+            v_chol, v_mean = ref.project_bwd(r["extents"], self.chol, r["conics"], g["v_xy"],
+                                             g["v_conic"], chol=True)
+        self.means.grad, self.chol.grad, self.rgbs.grad = v_mean, v_chol, g["v_rgb"]
+        self.opt.step()
+        self.opt.zero_grad(set_to_none=True)
+        return loss
+
+
+def timed(fit, target, iters):
+    for _ in range(3):
+        fit.step(target)
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(iters):
+        fit.step(target)
+    e.record()
+    torch.cuda.synchronize()
+    return iters / (s.elapsed_time(e) / 1e3)
+
+
+def run(name):
+    size, n, nt, diag, noise, std, iters, piters = CONFIGS[name]
+    target = make_target(size, size, nt, diag, noise=noise, noise_std=std)
+    ref.STRICT_SYNC = False
+    out = {"config": name, "size": size, "points": n}
+    mine = LevelFit(n, size, size, lr=1e-3, diag=diag)
+    out["lig_iters_per_s"] = timed(mine, target, iters)
+    del mine
+    theirs = RefFit(n, size, size, diag)
+    out["ref_iters_per_s"] = timed(theirs, target, iters)
+    del theirs
+    out["speedup"] = out["lig_iters_per_s"] / out["ref_iters_per_s"]
+    if piters:
+        mine, theirs = LevelFit(n, size, size, lr=1e-3, diag=diag), RefFit(n, size, size, diag)
+        for _ in range(piters):
+            mine.step(target)
+            theirs.step(target)
+        with torch.no_grad():
+            pm = psnr(torch.clamp(mine.render()[0], 0, 1), target)
+            pr = psnr(torch.clamp(theirs.render()["img"], 0, 1), target)
+        out.update(psnr_iters=piters, lig_psnr=pm, ref_psnr=pr, psnr_delta_db=pm - pr)
+    print(json.dumps(out), flush=True)
+    torch.cuda.empty_cache()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--configs", default="c0,c1l2")
+    a = ap.parse_args()
+    for c in a.configs.split(","):
+        run(c)
+
+
+if __name__ == "__main__":
+    main()
