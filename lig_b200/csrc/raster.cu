@@ -1,33 +1,29 @@
 // Weighted-sum rasterizer, forward and backward, plain and gradient-aware.
 //
-// Work decomposition (B200): one warp owns one (tile, band) work item.  A band
-// is up to PPL "pixel blocks" of the tile; a pixel block is 32 pixels, one per
-// lane, so a lane holds PPL pixels and keeps their accumulators (forward) or
-// cotangents (backward) in registers for the whole tile list.  There is no
-// __syncthreads: warps of a CTA work on different tiles.
+// Work decomposition (B200): one CTA per tile; the tile is split into <= 32
+// regions of 32 pixels and warp w owns region w (8x4 pixels in the forward,
+// 8x8 with two pixels per lane in the sum backward, the reference's warp in
+// the gradient-aware backward, whose v_xy_abs is |sum over that warp| per
+// Gaussian, csrc/gradient_aware_rasterizer.cu:317-341).
 //
-// Pixel blocks are 8x4 pixel rectangles, except in the gradient-aware backward,
-// where block b is the reference's warp b (thread ranks 32b..32b+31 of the
-// B x B tile, rank = ty*B + tx): its v_xy_abs is |sum over that warp| per
-// Gaussian (csrc/gradient_aware_rasterizer.cu:317-341), so the grouping is
-// part of the result.
+// Gaussian data: a pack kernel writes one 16-byte-aligned 48-byte record per
+// Gaussian (mean, conic, opacity, colour, cull half-widths).  The tile's
+// sorted id list is consumed in batches of blockDim Gaussians: each thread
+// parks one record in shared memory (fetched into registers while the
+// previous batch was processed) together with that Gaussian's region mask.
 //
-// Gaussian data: a pack kernel writes one 16-byte-aligned record per Gaussian
-// (mean, conic, opacity, colour, cull half-widths).  A warp streams its tile's
-// sorted id list in chunks of 32: lane l fetches record (chunk + l) into
-// registers two chunks ahead of use (ids three chunks ahead), then parks it in
-// a per-warp shared-memory slot from which all lanes read it by broadcast.
-//
-// Culling: for each (Gaussian, pixel block) the warp tests the block's pixel
-// centres against a conservative box around the Gaussian's alpha >= 1/255
-// ellipse and skips the block when it misses.  The box is built with margin
-// (see pack_kernel), so every skipped pixel would have failed the reference's
-// own `alpha < 1/255` test (csrc/forward.cu:258): results are unchanged.
+// Culling: a warp runs only the Gaussians whose mask has its region bit
+// (one ballot per 32 Gaussians, then the set bits in ascending order, i.e.
+// list order).  The mask comes from a conservative box around the
+// Gaussian's alpha >= 1/255 ellipse, built with margin (see pack_kernel), so
+// every skipped pixel would have failed the reference's own `alpha < 1/255`
+// test (csrc/forward.cu:258): results are unchanged.
 //
 // Per-pixel arithmetic is written exactly as the reference writes it
 // (csrc/forward.cu:250-269, csrc/backward.cu:102-150,
 // csrc/gradient_aware_rasterizer.cu:201-315, :434-482) so that the float
-// roundings, and with them the alpha-threshold decisions, are the same.
+// roundings, and with them the alpha-threshold decisions, are the same, and
+// each pixel adds its terms in list order.
 #include "common.cuh"
 
 namespace lig {
@@ -85,226 +81,217 @@ __global__ void pack_kernel(int n, const T *__restrict__ xys, const T *__restric
     recs[i] = r;
 }
 
-// ------------------------------------------------------------ pixel maps
-// mode 0: 8x4 blocks; mode 1: reference warps (32 consecutive thread ranks).
-struct TileMap {
-    int B, nbx, nblk;
-    __device__ __forceinline__ void pixel(int mode, int bi, int lane, int &lx, int &ly) const {
-        if (mode == 0) {
-            int bx = bi % nbx, by = bi / nbx;
-            lx = bx * 8 + (lane & 7);
-            ly = by * 4 + (lane >> 3);
+// ---------------------------------------------------------------- regions
+// A tile is split into R <= 32 regions of 32 pixels; warp w of the CTA owns
+// region w and each lane owns PPL pixels of it.
+//   kind 0: 8x4 blocks, PPL 1                          (forward)
+//   kind 1: 8x8 blocks, lane owns (x, y) and (x, y+4)  (sum backward)
+//   kind 2: the reference's warps, thread ranks 32w..32w+31 with
+//           rank = ty*B + tx, PPL 1                    (gradient-aware backward)
+struct Regions {
+    int kind, B, nbx, nby, count;
+    __host__ __device__ static Regions make(int kind, int B) {
+        Regions r{kind, B, 1, 1, 1};
+        if (kind == 0) { r.nbx = (B + 7) / 8; r.nby = (B + 3) / 4; }
+        else if (kind == 1) { r.nbx = (B + 7) / 8; r.nby = (B + 7) / 8; }
+        else { r.nbx = 1; r.nby = (B * B + 31) / 32; }
+        r.count = r.nbx * r.nby;
+        return r;
+    }
+    __device__ __forceinline__ void pixel(int w, int lane, int p, int &lx, int &ly) const {
+        if (kind == 0) {
+            lx = (w % nbx) * 8 + (lane & 7);
+            ly = (w / nbx) * 4 + (lane >> 3);
+        } else if (kind == 1) {
+            lx = (w % nbx) * 8 + (lane & 7);
+            ly = (w / nbx) * 8 + (lane >> 3) + 4 * p;
         } else {
-            int r = bi * 32 + lane;
+            int r = w * 32 + lane;
             lx = r % B;
-            ly = r / B;
-            if (r >= B * B) ly = B;  // mark invalid
+            ly = r < B * B ? r / B : B;  // B marks "no pixel"
         }
     }
-    // conservative tile-local pixel-index rectangle of block bi
-    __device__ __forceinline__ void rect(int mode, int bi, int &x0, int &x1, int &y0,
-                                         int &y1) const {
-        if (mode == 0) {
-            int bx = bi % nbx, by = bi / nbx;
-            x0 = bx * 8; x1 = x0 + 7;
-            y0 = by * 4; y1 = y0 + 3;
-        } else {
-            int r0 = bi * 32, r1 = min(r0 + 31, B * B - 1);
-            y0 = r0 / B; y1 = r1 / B;
-            if (y0 == y1) { x0 = r0 % B; x1 = r1 % B; }
-            else { x0 = 0; x1 = B - 1; }
+    __device__ __forceinline__ uint32_t all() const {
+        return count >= 32 ? 0xffffffffu : ((1u << count) - 1u);
+    }
+    // Regions whose pixel centres (tile-local, pixel i at i + 0.5) can lie in
+    // the box [x0, x1] x [y0, y1].  Conservative.
+    template <typename T>
+    __device__ __forceinline__ uint32_t bits(T x0, T x1, T y0, T y1) const {
+        if (kind == 2) {
+            // rows j with centre in [y0, y1]; a region spans rows r0/B .. r1/B
+            T fy0 = Math<T>::ceil_(y0 - (T)0.5), fy1 = Math<T>::floor_(y1 - (T)0.5);
+            if (!(fy0 <= fy1) || fy1 < (T)0 || fy0 > (T)(B - 1)) return 0u;
+            int j0 = (int)max(fy0, (T)0), j1 = (int)min(fy1, (T)(B - 1));
+            uint32_t m = 0;
+            for (int w = 0; w < count; ++w) {
+                int r0 = (w * 32) / B, r1 = min(w * 32 + 31, B * B - 1) / B;
+                if (r0 <= j1 && r1 >= j0) m |= 1u << w;
+            }
+            return m;
         }
+        const int hb = kind == 0 ? 4 : 8;
+        T c0 = Math<T>::ceil_((x0 - (T)7.5) / (T)8), c1 = Math<T>::floor_((x1 - (T)0.5) / (T)8);
+        T r0 = Math<T>::ceil_((y0 - ((T)hb - (T)0.5)) / (T)hb);
+        T r1 = Math<T>::floor_((y1 - (T)0.5) / (T)hb);
+        c0 = max(c0, (T)0); r0 = max(r0, (T)0);
+        c1 = min(c1, (T)(nbx - 1)); r1 = min(r1, (T)(nby - 1));
+        if (!(c0 <= c1) || !(r0 <= r1)) return 0u;
+        int ic0 = (int)c0, ic1 = (int)c1, ir0 = (int)r0, ir1 = (int)r1;
+        uint32_t cols = ((1u << (ic1 - ic0 + 1)) - 1u) << ic0;
+        uint32_t m = 0;
+        for (int r = ir0; r <= ir1; ++r) m |= cols << (r * nbx);
+        return m;
     }
 };
 
-// True when the Gaussian's cull box misses the block's pixel centres.  Written
-// as "strictly outside" so NaN / infinite values never cause a skip.
+// Region mask of one Gaussian for the tile at pixel origin (tx0, ty0).  The
+// cull box (see pack_kernel) has margin, so every pixel outside it fails the
+// reference's own alpha >= 1/255 test; records without a box (wx < 0) touch
+// every region.
 template <typename T>
-__device__ __forceinline__ bool box_misses(const Rec<T> &g, T bx0, T bx1, T by0, T by1) {
-    if (!(g.wx >= (T)0)) return false;
-    return (g.x + g.wx < bx0) || (g.x - g.wx > bx1) || (g.y + g.wy < by0) || (g.y - g.wy > by1);
+__device__ __forceinline__ uint32_t region_bits(const Rec<T> &g, const Regions &R, int tx0,
+                                                int ty0) {
+    if (!(g.wx >= (T)0)) return R.all();
+    T cx = g.x - (T)tx0, cy = g.y - (T)ty0;
+    return R.bits<T>(cx - g.wx, cx + g.wx, cy - g.wy, cy + g.wy);
 }
 
-// Record streaming state for one warp.
+// --------------------------------------------------------------- forward
+// One CTA per tile, warp w = region w (8x4 pixels), one pixel per lane.
+// Batches of blockDim Gaussians (list order) are staged in shared memory, one
+// record per thread, with the next batch's record fetched into registers
+// while the current batch is processed.  Each thread also stores its
+// Gaussian's region mask; a warp then walks only the Gaussians whose mask has
+// its bit (ballot over the batch, set bits in ascending order = list order),
+// two per iteration so the two sigma/alpha chains overlap, accumulating in
+// list order — per pixel exactly the reference's sequence of additions.
 template <typename T>
-struct Stream {
-    Rec<T> *slots;   // 32 per-warp shared slots
-    Rec<T> nxt;      // record of the next chunk (this lane's entry)
-    int id_nxt2;     // id of the chunk after next (this lane's entry)
-    const Rec<T> *recs;
-    const int32_t *ids;
-    int end;
-
-    __device__ __forceinline__ void fetch_id(int e, int &id) const {
-        id = e < end ? __ldg(ids + e) : -1;
-    }
-    __device__ __forceinline__ void fetch_rec(int id, Rec<T> &r) const {
-        if (id >= 0) r = recs[id];
-    }
-    // Begin at entry e0: park chunk e0 in smem, prefetch chunk e0+32, ids of e0+64.
-    __device__ __forceinline__ void start(int e0, int lane) {
-        int id0, id1;
-        fetch_id(e0 + lane, id0);
-        fetch_id(e0 + 32 + lane, id1);
-        fetch_id(e0 + 64 + lane, id_nxt2);
-        Rec<T> cur;
-        fetch_rec(id0, cur);
-        fetch_rec(id1, nxt);
-        slots[lane] = cur;
-        __syncwarp();
-    }
-    // After chunk `e` is consumed: park chunk e+32, prefetch e+64, ids of e+96.
-    __device__ __forceinline__ void advance(int e, int lane) {
-        __syncwarp();
-        slots[lane] = nxt;
-        int id = id_nxt2;
-        fetch_id(e + 96 + lane, id_nxt2);
-        fetch_rec(id, nxt);
-        __syncwarp();
+struct PixelEval {
+    // csrc/forward.cu:250-259 (sum) / csrc/gradient_aware_rasterizer.cu:436-445
+    // (gradient-aware: d = p - mu); returns false when the term is skipped.
+    template <bool GA>
+    static __device__ __forceinline__ bool alpha(const Rec<T> &g, T px, T py, T &dx, T &dy,
+                                                 T &a) {
+        using M = Math<T>;
+        if (!GA) { dx = g.x - px; dy = g.y - py; }
+        else { dx = px - g.x; dy = py - g.y; }
+        const T sigma = (T)0.5 * (g.a * dx * dx + g.c * dy * dy) + g.b * dx * dy;
+        a = M::min_((T)0.999, g.o * M::exp_(-sigma));
+        return !(sigma < (T)0 || a < (T)1 / (T)255);
     }
 };
 
-// --------------------------------------------------------------- forward
-template <typename T, bool GA, int PPL>
-__global__ void __launch_bounds__(128)
-raster_fwd_kernel(int H, int W, int B, int tbx, int nbands, int nwork,
-                  const int32_t *__restrict__ ids, const int2 *__restrict__ tile_bins,
-                  const int32_t *__restrict__ d_total, const Rec<T> *__restrict__ recs,
-                  T *__restrict__ img, T *__restrict__ wsum, T *__restrict__ odx,
-                  T *__restrict__ ody, T *__restrict__ odxy, int32_t *__restrict__ final_idx) {
-    using M = Math<T>;
-    __shared__ Rec<T> s_rec[4][32];
-    int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    int work = blockIdx.x * 4 + wib;
-    if (work >= nwork) return;
-    int tile = work / nbands, band = work % nbands;
-    int tx0 = (tile % tbx) * B, ty0 = (tile / tbx) * B;
-    TileMap map{B, (B + 7) / 8, ((B + 7) / 8) * ((B + 3) / 4)};
-
-    T px[PPL], py[PPL];
-    bool in[PPL];
-    int pix[PPL];
-#pragma unroll
-    for (int i = 0; i < PPL; ++i) {
-        int bi = band * PPL + i, lx = B, ly = B;
-        if (bi < map.nblk) map.pixel(0, bi, lane, lx, ly);
-        int gx = tx0 + lx, gy = ty0 + ly;
-        in[i] = lx < B && ly < B && gx < W && gy < H;
-        px[i] = (T)gx + (T)0.5;
-        py[i] = (T)gy + (T)0.5;
-        pix[i] = gy * W + gx;
+template <typename T, bool GA>
+struct FwdAcc {
+    T r = 0, g = 0, b = 0, w = 0;
+    T dx[GA ? 3 : 1] = {}, dy[GA ? 3 : 1] = {}, dxy[GA ? 3 : 1] = {};
+    int cur = 0;
+    __device__ __forceinline__ void add(const Rec<T> &q, T dxp, T dyp, T a, int idx) {
+        // csrc/forward.cu:264-269, csrc/gradient_aware_rasterizer.cu:451-482
+        r += q.r * a;
+        g += q.g * a;
+        b += q.bl * a;
+        if (GA) {
+            const T sdx = q.a * dxp + q.b * dyp;
+            const T sdy = q.b * dxp + q.c * dyp;
+            const T s2 = q.b;
+            const T adx = -a * sdx;
+            const T ady = -a * sdy;
+            const T adxy = -a * (s2 - sdx * sdy);
+            dx[0] += q.r * adx; dx[1] += q.g * adx; dx[2] += q.bl * adx;
+            dy[0] += q.r * ady; dy[1] += q.g * ady; dy[2] += q.bl * ady;
+            dxy[0] += q.r * adxy; dxy[1] += q.g * adxy; dxy[2] += q.bl * adxy;
+        }
+        w += a;
+        cur = idx;
     }
+};
 
-    if (*d_total == 0) {  // reference: white image, zero weights (rasterize.py:80-90)
-#pragma unroll
-        for (int i = 0; i < PPL; ++i) {
-            if (!in[i]) continue;
-            int p = pix[i];
-            img[3 * p] = (T)1; img[3 * p + 1] = (T)1; img[3 * p + 2] = (T)1;
-            wsum[p] = 0;
-            final_idx[p] = 0;
+template <typename T, bool GA>
+__global__ void __launch_bounds__(1024)
+raster_fwd_kernel(int H, int W, int B, int tbx, const int32_t *__restrict__ ids,
+                  const int2 *__restrict__ tile_bins, const int32_t *__restrict__ d_total,
+                  const Rec<T> *__restrict__ recs, T *__restrict__ img, T *__restrict__ wsum,
+                  T *__restrict__ odx, T *__restrict__ ody, T *__restrict__ odxy,
+                  int32_t *__restrict__ final_idx) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int nt = blockDim.x;
+    Rec<T> *s_rec = reinterpret_cast<Rec<T> *>(smem_raw);
+    uint32_t *s_bits = reinterpret_cast<uint32_t *>(s_rec + nt);
+    const unsigned FULL = 0xffffffffu;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int tile = blockIdx.x;
+    const int tx0 = (tile % tbx) * B, ty0 = (tile / tbx) * B;
+    const Regions R = Regions::make(0, B);
+    int lx, ly;
+    R.pixel(w, lane, 0, lx, ly);
+    const int gx = tx0 + lx, gy = ty0 + ly;
+    const bool inside = lx < B && ly < B && gx < W && gy < H;
+    const int pix = gy * W + gx;
+    const T px = (T)gx + (T)0.5, py = (T)gy + (T)0.5;
+
+    if (*d_total == 0) {  // the reference's empty-list branch (rasterize.py:80-90)
+        if (inside) {
+            img[3 * pix] = (T)1; img[3 * pix + 1] = (T)1; img[3 * pix + 2] = (T)1;
+            wsum[pix] = 0;
+            final_idx[pix] = 0;
             if (GA) {
 #pragma unroll
-                for (int ch = 0; ch < 3; ++ch) { odx[3 * p + ch] = 0; ody[3 * p + ch] = 0; odxy[3 * p + ch] = 0; }
+                for (int ch = 0; ch < 3; ++ch) { odx[3 * pix + ch] = 0; ody[3 * pix + ch] = 0; odxy[3 * pix + ch] = 0; }
             }
         }
         return;
     }
 
-    T acc[PPL][3], ws[PPL];
-    T adx[GA ? PPL : 1][3], ady[GA ? PPL : 1][3], adxy[GA ? PPL : 1][3];
-    int cur[PPL];
-#pragma unroll
-    for (int i = 0; i < PPL; ++i) {
-        acc[i][0] = acc[i][1] = acc[i][2] = 0;
-        ws[i] = 0;
-        cur[i] = 0;
-        if (GA) {
-#pragma unroll
-            for (int ch = 0; ch < 3; ++ch) adx[i][ch] = ady[i][ch] = adxy[i][ch] = 0;
+    const int2 range = tile_bins[tile];
+    FwdAcc<T, GA> acc;
+    Rec<T> pre;
+    if (range.x + tid < range.y) pre = recs[__ldg(ids + range.x + tid)];
+    for (int base = range.x; base < range.y; base += nt) {
+        const int cnt = min(nt, range.y - base);
+        __syncthreads();
+        if (tid < cnt) {
+            s_rec[tid] = pre;
+            s_bits[tid] = region_bits(pre, R, tx0, ty0);
         }
-    }
-    // block pixel-centre rectangles (image coordinates), per i
-    T bx0[PPL], bx1[PPL], by0[PPL], by1[PPL];
-    bool bvalid[PPL];
-#pragma unroll
-    for (int i = 0; i < PPL; ++i) {
-        int bi = band * PPL + i;
-        int x0 = 0, x1 = -1, y0 = 0, y1 = -1;
-        bvalid[i] = bi < map.nblk;
-        if (bvalid[i]) map.rect(0, bi, x0, x1, y0, y1);
-        bx0[i] = (T)(tx0 + x0) + (T)0.5; bx1[i] = (T)(tx0 + x1) + (T)0.5;
-        by0[i] = (T)(ty0 + y0) + (T)0.5; by1[i] = (T)(ty0 + y1) + (T)0.5;
-    }
-
-    int2 range = tile_bins[tile];
-    Stream<T> st;
-    st.slots = s_rec[wib];
-    st.recs = recs;
-    st.ids = ids;
-    st.end = range.y;
-    if (range.x < range.y) st.start(range.x, lane);
-    for (int e = range.x; e < range.y; e += 32) {
-        int cnt = min(32, range.y - e);
-        for (int t = 0; t < cnt; ++t) {
-            const Rec<T> g = st.slots[t];
-#pragma unroll
-            for (int i = 0; i < PPL; ++i) {
-                if (!bvalid[i] || box_misses(g, bx0[i], bx1[i], by0[i], by1[i])) continue;
-                if (!in[i]) continue;
-                if (!GA) {
-                    // csrc/forward.cu:250-269
-                    const T dx = g.x - px[i];
-                    const T dy = g.y - py[i];
-                    const T sigma = (T)0.5 * (g.a * dx * dx + g.c * dy * dy) + g.b * dx * dy;
-                    const T alpha = M::min_((T)0.999, g.o * M::exp_(-sigma));
-                    if (sigma < (T)0 || alpha < (T)1 / (T)255) continue;
-                    acc[i][0] += g.r * alpha;
-                    acc[i][1] += g.g * alpha;
-                    acc[i][2] += g.bl * alpha;
-                    ws[i] += alpha;
-                    cur[i] = e + t;
-                } else {
-                    // csrc/gradient_aware_rasterizer.cu:434-482
-                    const T dx = px[i] - g.x;
-                    const T dy = py[i] - g.y;
-                    const T sigma = (T)0.5 * (g.a * dx * dx + g.c * dy * dy) + g.b * dx * dy;
-                    const T alpha = M::min_((T)0.999, g.o * M::exp_(-sigma));
-                    if (sigma < (T)0 || alpha < (T)1 / (T)255) continue;
-                    const T sdx = g.a * dx + g.b * dy;
-                    const T sdy = g.b * dx + g.c * dy;
-                    const T s2 = g.b;
-                    const T adx_ = -alpha * sdx;
-                    const T ady_ = -alpha * sdy;
-                    const T adxy_ = -alpha * (s2 - sdx * sdy);
-                    acc[i][0] += g.r * alpha;
-                    acc[i][1] += g.g * alpha;
-                    acc[i][2] += g.bl * alpha;
-                    adx[i][0] += g.r * adx_; adx[i][1] += g.g * adx_; adx[i][2] += g.bl * adx_;
-                    ady[i][0] += g.r * ady_; ady[i][1] += g.g * ady_; ady[i][2] += g.bl * ady_;
-                    adxy[i][0] += g.r * adxy_; adxy[i][1] += g.g * adxy_; adxy[i][2] += g.bl * adxy_;
-                    ws[i] += alpha;
-                    cur[i] = e + t;
+        __syncthreads();
+        if (base + nt + tid < range.y) pre = recs[__ldg(ids + base + nt + tid)];
+        for (int m = 0; m * 32 < cnt; ++m) {
+            const int t = m * 32 + lane;
+            uint32_t mask = __ballot_sync(FULL, t < cnt && ((s_bits[t] >> w) & 1u));
+            while (mask) {
+                const int b1 = __ffs(mask) - 1;
+                mask &= mask - 1;
+                const Rec<T> g1 = s_rec[m * 32 + b1];
+                T dx1, dy1, a1;
+                const bool ok1 = PixelEval<T>::template alpha<GA>(g1, px, py, dx1, dy1, a1);
+                if (mask) {
+                    const int b2 = __ffs(mask) - 1;
+                    mask &= mask - 1;
+                    const Rec<T> g2 = s_rec[m * 32 + b2];
+                    T dx2, dy2, a2;
+                    const bool ok2 = PixelEval<T>::template alpha<GA>(g2, px, py, dx2, dy2, a2);
+                    if (ok1) acc.add(g1, dx1, dy1, a1, base + m * 32 + b1);
+                    if (ok2) acc.add(g2, dx2, dy2, a2, base + m * 32 + b2);
+                } else if (ok1) {
+                    acc.add(g1, dx1, dy1, a1, base + m * 32 + b1);
                 }
             }
         }
-        if (e + 32 < range.y) st.advance(e, lane);
     }
-#pragma unroll
-    for (int i = 0; i < PPL; ++i) {
-        if (!in[i]) continue;
-        int p = pix[i];
-        final_idx[p] = cur[i];
-        img[3 * p] = acc[i][0];
-        img[3 * p + 1] = acc[i][1];
-        img[3 * p + 2] = acc[i][2];
-        wsum[p] = ws[i];
+    if (inside) {
+        final_idx[pix] = acc.cur;
+        img[3 * pix] = acc.r;
+        img[3 * pix + 1] = acc.g;
+        img[3 * pix + 2] = acc.b;
+        wsum[pix] = acc.w;
         if (GA) {
 #pragma unroll
             for (int ch = 0; ch < 3; ++ch) {
-                odx[3 * p + ch] = adx[i][ch];
-                ody[3 * p + ch] = ady[i][ch];
-                odxy[3 * p + ch] = adxy[i][ch];
+                odx[3 * pix + ch] = acc.dx[ch];
+                ody[3 * pix + ch] = acc.dy[ch];
+                odxy[3 * pix + ch] = acc.dxy[ch];
             }
         }
     }
@@ -361,208 +348,193 @@ struct Grads {
     }
 };
 
-template <typename T, bool GA, int PPL>
-__global__ void __launch_bounds__(128)
-raster_bwd_kernel(int H, int W, int B, int tbx, int nbands, int nwork,
-                  const int32_t *__restrict__ ids, const int2 *__restrict__ tile_bins,
-                  const int32_t *__restrict__ d_total, const Rec<T> *__restrict__ recs,
-                  const int32_t *__restrict__ final_idx, const T *__restrict__ v_img,
-                  const T *__restrict__ v_wsum, const T *__restrict__ v_dx,
-                  const T *__restrict__ v_dy, const T *__restrict__ v_dxy, T clamp,
-                  Grads<T> out) {
+// One CTA per tile.  Sum variant: warp = 8x8 region, lane owns 2 pixels;
+// gradient-aware: warp = reference warp (its v_xy_abs is |sum over the warp|,
+// csrc/gradient_aware_rasterizer.cu:317-341), lane owns 1 pixel.  Batches and
+// region masks as in the forward, over the list prefix that can contribute
+// (entries past every pixel's final index are skipped).  Per Gaussian a lane
+// accumulates its 11 gradient terms over its pixels, the warp reduces them
+// with one 16-shuffle transpose-reduce and 11 lanes issue the atomics.
+template <typename T, bool GA>
+__global__ void __launch_bounds__(1024)
+raster_bwd_kernel(int H, int W, int B, int tbx, const int32_t *__restrict__ ids,
+                  const int2 *__restrict__ tile_bins, const int32_t *__restrict__ d_total,
+                  const Rec<T> *__restrict__ recs, const int32_t *__restrict__ final_idx,
+                  const T *__restrict__ v_img, const T *__restrict__ v_wsum,
+                  const T *__restrict__ v_dx, const T *__restrict__ v_dy,
+                  const T *__restrict__ v_dxy, T clamp, Grads<T> out) {
     using M = Math<T>;
-    constexpr int MODE = GA ? 1 : 0;
-    __shared__ Rec<T> s_rec[4][32];
+    constexpr int PPL = GA ? 1 : 2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int nt = blockDim.x;
+    Rec<T> *s_rec = reinterpret_cast<Rec<T> *>(smem_raw);
+    uint32_t *s_bits = reinterpret_cast<uint32_t *>(s_rec + nt);
+    int32_t *s_ids = reinterpret_cast<int32_t *>(s_bits + nt);
+    __shared__ int s_end;
     const unsigned FULL = 0xffffffffu;
-    int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    int work = blockIdx.x * 4 + wib;
-    if (work >= nwork) return;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     if (*d_total == 0) return;  // gradients stay zero (rasterize.py:156-161)
-    int tile = work / nbands, band = work % nbands;
-    int tx0 = (tile % tbx) * B, ty0 = (tile / tbx) * B;
-    int nblk = GA ? (B * B + 31) / 32 : ((B + 7) / 8) * ((B + 3) / 4);
-    TileMap map{B, (B + 7) / 8, nblk};
+    const int tile = blockIdx.x;
+    const int tx0 = (tile % tbx) * B, ty0 = (tile / tbx) * B;
+    const Regions R = Regions::make(GA ? 2 : 1, B);
 
-    T px[PPL], py[PPL];
+    T px[PPL], py[PPL], vo[PPL][3], vw[PPL];
+    T vdx[GA ? 1 : 1][3], vdy[GA ? 1 : 1][3], vdxy[GA ? 1 : 1][3];
     int fin[PPL];
-    T vo[PPL][3], vw[PPL];
-    T vdx[GA ? PPL : 1][3], vdy[GA ? PPL : 1][3], vdxy[GA ? PPL : 1][3];
-    T bx0[PPL], bx1[PPL], by0[PPL], by1[PPL];
-    bool bvalid[PPL];
-    int band_fin = -1;
+    int my_fin = -1;
 #pragma unroll
-    for (int i = 0; i < PPL; ++i) {
-        int bi = band * PPL + i, lx = B, ly = B;
-        bvalid[i] = bi < map.nblk;
-        int x0 = 0, x1 = -1, y0 = 0, y1 = -1;
-        if (bvalid[i]) {
-            map.pixel(MODE, bi, lane, lx, ly);
-            map.rect(MODE, bi, x0, x1, y0, y1);
-        }
-        bx0[i] = (T)(tx0 + x0) + (T)0.5; bx1[i] = (T)(tx0 + x1) + (T)0.5;
-        by0[i] = (T)(ty0 + y0) + (T)0.5; by1[i] = (T)(ty0 + y1) + (T)0.5;
-        int gx = tx0 + lx, gy = ty0 + ly;
-        bool inside = lx < B && ly < B && gx < W && gy < H;
-        px[i] = (T)gx + (T)0.5;
-        py[i] = (T)gy + (T)0.5;
-        int p = inside ? gy * W + gx : 0;
-        fin[i] = inside ? final_idx[p] : -1;  // -1: never valid
-        vo[i][0] = inside ? v_img[3 * p] : (T)0;
-        vo[i][1] = inside ? v_img[3 * p + 1] : (T)0;
-        vo[i][2] = inside ? v_img[3 * p + 2] : (T)0;
-        vw[i] = inside ? v_wsum[p] : (T)0;
+    for (int p = 0; p < PPL; ++p) {
+        int lx, ly;
+        R.pixel(w, lane, p, lx, ly);
+        const int gx = tx0 + lx, gy = ty0 + ly;
+        const bool inside = lx < B && ly < B && gx < W && gy < H;
+        const int q = inside ? gy * W + gx : 0;
+        px[p] = (T)gx + (T)0.5;
+        py[p] = (T)gy + (T)0.5;
+        fin[p] = inside ? final_idx[q] : -1;  // -1: never valid
+        vo[p][0] = inside ? v_img[3 * q] : (T)0;
+        vo[p][1] = inside ? v_img[3 * q + 1] : (T)0;
+        vo[p][2] = inside ? v_img[3 * q + 2] : (T)0;
+        vw[p] = inside ? v_wsum[q] : (T)0;
         if (GA) {
 #pragma unroll
             for (int ch = 0; ch < 3; ++ch) {
-                vdx[i][ch] = inside ? v_dx[3 * p + ch] : (T)0;
-                vdy[i][ch] = inside ? v_dy[3 * p + ch] : (T)0;
-                vdxy[i][ch] = inside ? v_dxy[3 * p + ch] : (T)0;
+                vdx[0][ch] = inside ? v_dx[3 * q + ch] : (T)0;
+                vdy[0][ch] = inside ? v_dy[3 * q + ch] : (T)0;
+                vdxy[0][ch] = inside ? v_dxy[3 * q + ch] : (T)0;
             }
         }
-        band_fin = max(band_fin, fin[i]);
+        my_fin = max(my_fin, fin[p]);
     }
+    if (tid == 0) s_end = -1;
+    __syncthreads();
 #pragma unroll
-    for (int o = 16; o >= 1; o >>= 1) band_fin = max(band_fin, __shfl_xor_sync(FULL, band_fin, o));
+    for (int o = 16; o >= 1; o >>= 1) my_fin = max(my_fin, __shfl_xor_sync(FULL, my_fin, o));
+    if (lane == 0) atomicMax(&s_end, my_fin);
+    __syncthreads();
+    const int2 range = tile_bins[tile];
+    const int end = min(range.y, s_end + 1);
 
-    int2 range = tile_bins[tile];
-    int end = min(range.y, band_fin + 1);  // entries past every pixel's final index: no work
-    Stream<T> st;
-    st.slots = s_rec[wib];
-    st.recs = recs;
-    st.ids = ids;
-    st.end = end;
-    if (range.x < end) st.start(range.x, lane);
-    for (int e = range.x; e < end; e += 32) {
-        int cnt = min(32, end - e);
-        for (int t = 0; t < cnt; ++t) {
-            const Rec<T> g = st.slots[t];
-            const int k = e + t;
-            T v[16];
+    Rec<T> pre;
+    int pre_id = -1;
+    if (range.x + tid < end) {
+        pre_id = __ldg(ids + range.x + tid);
+        pre = recs[pre_id];
+    }
+    for (int base = range.x; base < end; base += nt) {
+        const int cnt = min(nt, end - base);
+        __syncthreads();
+        if (tid < cnt) {
+            s_rec[tid] = pre;
+            s_bits[tid] = region_bits(pre, R, tx0, ty0);
+            s_ids[tid] = pre_id;
+        }
+        __syncthreads();
+        if (base + nt + tid < end) {
+            pre_id = __ldg(ids + base + nt + tid);
+            pre = recs[pre_id];
+        }
+        for (int m = 0; m * 32 < cnt; ++m) {
+            const int t = m * 32 + lane;
+            uint32_t mask = __ballot_sync(FULL, t < cnt && ((s_bits[t] >> w) & 1u));
+            while (mask) {
+                const int bsel = __ffs(mask) - 1;
+                mask &= mask - 1;
+                const int slot = m * 32 + bsel;
+                const Rec<T> g = s_rec[slot];
+                const int k = base + slot;
+                T v[16];
 #pragma unroll
-            for (int q = 0; q < 16; ++q) v[q] = 0;
-            bool any = false;
+                for (int q = 0; q < 16; ++q) v[q] = 0;
+                bool any = false;
 #pragma unroll
-            for (int i = 0; i < PPL; ++i) {
-                if (!bvalid[i] || box_misses(g, bx0[i], bx1[i], by0[i], by1[i])) continue;
-                bool valid = k <= fin[i];
-                if (!GA) {
-                    if (!__any_sync(FULL, valid)) continue;
-                    if (!valid) continue;
-                    // csrc/backward.cu:102-150
-                    const T dx = g.x - px[i];
-                    const T dy = g.y - py[i];
-                    const T sigma = (T)0.5 * (g.a * dx * dx + g.c * dy * dy) + g.b * dx * dy;
-                    const T vis = M::exp_(-sigma);
-                    const T alpha = M::min_(clamp, g.o * vis);
-                    if (sigma < (T)0 || alpha < (T)1 / (T)255) continue;
-                    any = true;
-                    T v_alpha = 0;
-                    v[7] += alpha * vo[i][0];
-                    v[8] += alpha * vo[i][1];
-                    v[9] += alpha * vo[i][2];
-                    v_alpha += g.r * vo[i][0];
-                    v_alpha += g.g * vo[i][1];
-                    v_alpha += g.bl * vo[i][2];
-                    v_alpha += vw[i];
-                    v[10] += vis * v_alpha;
-                    const T v_sigma = -alpha * v_alpha;
-                    v[4] += (T)0.5 * v_sigma * dx * dx;
-                    v[5] += v_sigma * dx * dy;
-                    v[6] += (T)0.5 * v_sigma * dy * dy;
-                    const T gx = v_sigma * (g.a * dx + g.b * dy);
-                    const T gy = v_sigma * (g.b * dx + g.c * dy);
-                    v[0] += gx;
-                    v[1] += gy;
-                    v[2] += M::abs_(gx);
-                    v[3] += M::abs_(gy);
-                } else {
-                    // csrc/gradient_aware_rasterizer.cu:191-315
-                    T gx = 0, gy = 0;
-                    bool ok = false;
-                    if (valid) {
-                        const T dx = px[i] - g.x;
-                        const T dy = py[i] - g.y;
+                for (int p = 0; p < PPL; ++p) {
+                    if (k > fin[p]) continue;
+                    if (!GA) {
+                        // csrc/backward.cu:102-150
+                        const T dx = g.x - px[p];
+                        const T dy = g.y - py[p];
                         const T sigma = (T)0.5 * (g.a * dx * dx + g.c * dy * dy) + g.b * dx * dy;
                         const T vis = M::exp_(-sigma);
                         const T alpha = M::min_(clamp, g.o * vis);
-                        ok = !(sigma < (T)0 || alpha < (T)1 / (T)255);
-                        if (ok) {
-                            const T sx = g.a * dx + g.b * dy;
-                            const T sy = g.b * dx + g.c * dy;
-                            const T a = g.a, b = g.b, cc = g.c;
-                            const T ax = -alpha * sx;
-                            const T ay = -alpha * sy;
-                            const T axy = alpha * (sx * sy - b);
-                            v[7] += vo[i][0] * alpha + vdx[i][0] * ax + vdy[i][0] * ay + vdxy[i][0] * axy;
-                            v[8] += vo[i][1] * alpha + vdx[i][1] * ax + vdy[i][1] * ay + vdxy[i][1] * axy;
-                            v[9] += vo[i][2] * alpha + vdx[i][2] * ax + vdy[i][2] * ay + vdxy[i][2] * axy;
-                            const T va = (vo[i][0] * g.r + vo[i][1] * g.g + vo[i][2] * g.bl) + vw[i];
-                            const T vax = vdx[i][0] * g.r + vdx[i][1] * g.g + vdx[i][2] * g.bl;
-                            const T vay = vdy[i][0] * g.r + vdy[i][1] * g.g + vdy[i][2] * g.bl;
-                            const T vaxy = vdxy[i][0] * g.r + vdxy[i][1] * g.g + vdxy[i][2] * g.bl;
-                            const T sx2 = sx * sx, sy2 = sy * sy, sxsy = sx * sy;
-                            gx = alpha * (va * sx + vax * (a - sx2) + vay * (b - sxsy) +
-                                          vaxy * (sx2 * sy - (T)2 * b * sx - a * sy));
-                            gy = alpha * (va * sy + vax * (b - sxsy) + vay * (cc - sy2) +
-                                          vaxy * (sx * sy2 - (T)2 * b * sy - cc * sx));
-                            const T dx2 = dx * dx, dy2 = dy * dy, dxdy = dx * dy;
-                            const T P = sxsy - b;
-                            v[4] += alpha * (va * (-(T)0.5 * dx2) + vax * ((T)0.5 * dx2 * sx - dx) +
-                                             vay * ((T)0.5 * dx2 * sy) +
-                                             vaxy * (-(T)0.5 * dx2 * P + dx * sy));
-                            v[5] += alpha * (va * (-dxdy) + vax * (dxdy * sx - dy) +
-                                             vay * (dxdy * sy - dx) +
-                                             vaxy * (-dxdy * P + dy * sy + dx * sx - (T)1));
-                            v[6] += alpha * (va * (-(T)0.5 * dy2) + vax * ((T)0.5 * dy2 * sx) +
-                                             vay * ((T)0.5 * dy2 * sy - dy) +
-                                             vaxy * (-(T)0.5 * dy2 * P + dy * sx));
-                            v[10] += vis * va;
-                            v[0] += gx;
-                            v[1] += gy;
-                        }
-                    }
-                    if (!__any_sync(FULL, ok)) continue;
-                    any = true;
-                    // v_xy_abs: |sum over this reference warp| (all lanes get the sum)
-                    T sx_ = gx, sy_ = gy;
-#pragma unroll
-                    for (int o = 16; o >= 1; o >>= 1) {
-                        sx_ += __shfl_xor_sync(FULL, sx_, o);
-                        sy_ += __shfl_xor_sync(FULL, sy_, o);
-                    }
-                    if (lane == 0) {
-                        v[2] += M::abs_(sx_);
-                        v[3] += M::abs_(sy_);
+                        if (sigma < (T)0 || alpha < (T)1 / (T)255) continue;
+                        any = true;
+                        T v_alpha = 0;
+                        v[7] += alpha * vo[p][0];
+                        v[8] += alpha * vo[p][1];
+                        v[9] += alpha * vo[p][2];
+                        v_alpha += g.r * vo[p][0];
+                        v_alpha += g.g * vo[p][1];
+                        v_alpha += g.bl * vo[p][2];
+                        v_alpha += vw[p];
+                        v[10] += vis * v_alpha;
+                        const T v_sigma = -alpha * v_alpha;
+                        v[4] += (T)0.5 * v_sigma * dx * dx;
+                        v[5] += v_sigma * dx * dy;
+                        v[6] += (T)0.5 * v_sigma * dy * dy;
+                        const T gx = v_sigma * (g.a * dx + g.b * dy);
+                        const T gy = v_sigma * (g.b * dx + g.c * dy);
+                        v[0] += gx;
+                        v[1] += gy;
+                        v[2] += M::abs_(gx);
+                        v[3] += M::abs_(gy);
+                    } else {
+                        // csrc/gradient_aware_rasterizer.cu:201-315
+                        const T dx = px[p] - g.x;
+                        const T dy = py[p] - g.y;
+                        const T sigma = (T)0.5 * (g.a * dx * dx + g.c * dy * dy) + g.b * dx * dy;
+                        const T vis = M::exp_(-sigma);
+                        const T alpha = M::min_(clamp, g.o * vis);
+                        if (sigma < (T)0 || alpha < (T)1 / (T)255) continue;
+                        any = true;
+                        const T sx = g.a * dx + g.b * dy;
+                        const T sy = g.b * dx + g.c * dy;
+                        const T a = g.a, b = g.b, cc = g.c;
+                        const T ax = -alpha * sx;
+                        const T ay = -alpha * sy;
+                        const T axy = alpha * (sx * sy - b);
+                        v[7] += vo[p][0] * alpha + vdx[0][0] * ax + vdy[0][0] * ay + vdxy[0][0] * axy;
+                        v[8] += vo[p][1] * alpha + vdx[0][1] * ax + vdy[0][1] * ay + vdxy[0][1] * axy;
+                        v[9] += vo[p][2] * alpha + vdx[0][2] * ax + vdy[0][2] * ay + vdxy[0][2] * axy;
+                        const T va = (vo[p][0] * g.r + vo[p][1] * g.g + vo[p][2] * g.bl) + vw[p];
+                        const T vax = vdx[0][0] * g.r + vdx[0][1] * g.g + vdx[0][2] * g.bl;
+                        const T vay = vdy[0][0] * g.r + vdy[0][1] * g.g + vdy[0][2] * g.bl;
+                        const T vaxy = vdxy[0][0] * g.r + vdxy[0][1] * g.g + vdxy[0][2] * g.bl;
+                        const T sx2 = sx * sx, sy2 = sy * sy, sxsy = sx * sy;
+                        v[0] += alpha * (va * sx + vax * (a - sx2) + vay * (b - sxsy) +
+                                         vaxy * (sx2 * sy - (T)2 * b * sx - a * sy));
+                        v[1] += alpha * (va * sy + vax * (b - sxsy) + vay * (cc - sy2) +
+                                         vaxy * (sx * sy2 - (T)2 * b * sy - cc * sx));
+                        const T dx2 = dx * dx, dy2 = dy * dy, dxdy = dx * dy;
+                        const T P = sxsy - b;
+                        v[4] += alpha * (va * (-(T)0.5 * dx2) + vax * ((T)0.5 * dx2 * sx - dx) +
+                                         vay * ((T)0.5 * dx2 * sy) +
+                                         vaxy * (-(T)0.5 * dx2 * P + dx * sy));
+                        v[5] += alpha * (va * (-dxdy) + vax * (dxdy * sx - dy) +
+                                         vay * (dxdy * sy - dx) +
+                                         vaxy * (-dxdy * P + dy * sy + dx * sx - (T)1));
+                        v[6] += alpha * (va * (-(T)0.5 * dy2) + vax * ((T)0.5 * dy2 * sx) +
+                                         vay * ((T)0.5 * dy2 * sy - dy) +
+                                         vaxy * (-(T)0.5 * dy2 * P + dy * sx));
+                        v[10] += vis * va;
                     }
                 }
-            }
-            if (!__any_sync(FULL, any)) continue;
-            transpose_reduce16(v, lane);
-            int kk = (lane >> 1) & 15;
-            if ((lane & 1) == 0 && kk < 11) {
-                int gid = __ldg(ids + k);
-                out.add(kk, gid, v[0]);
+                if (!__any_sync(FULL, any)) continue;
+                transpose_reduce16(v, lane);
+                const int kk = (lane >> 1) & 15;
+                T val = v[0];
+                if (GA) {
+                    // lanes of values 2/3 take |warp sum of v_xy| from lanes of values 0/1
+                    const T src = __shfl_sync(FULL, v[0], (lane - 4) & 31);
+                    if (kk == 2 || kk == 3) val = M::abs_(src);
+                }
+                if ((lane & 1) == 0 && kk < 11) out.add(kk, s_ids[slot], val);
             }
         }
-        if (e + 32 < end) st.advance(e, lane);
     }
 }
 
 // ------------------------------------------------------------------ host
-constexpr int kWarpsPerCta = 4;
-
-template <typename T> struct Cfg;
-template <> struct Cfg<float> {
-    static constexpr int kFwd = 8, kFwdGA = 4, kBwd = 8, kBwdGA = 4;
-};
-template <> struct Cfg<double> {
-    static constexpr int kFwd = 2, kFwdGA = 2, kBwd = 2, kBwdGA = 2;
-};
-
-inline int nblocks_map(int B, bool rank_map) {
-    return rank_map ? (B * B + 31) / 32 : ((B + 7) / 8) * ((B + 3) / 4);
-}
-
 template <typename T>
 int pack(int n, const void *xys, const void *con, const void *col, const void *op, void *ws,
          size_t ws_bytes, cudaStream_t s) {
@@ -575,6 +547,12 @@ int pack(int n, const void *xys, const void *con, const void *col, const void *o
     return LIG_OK;
 }
 
+inline bool set_dyn_smem(const void *fn, size_t bytes) {
+    if (bytes <= 48 * 1024) return true;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) ==
+           cudaSuccess;
+}
+
 template <typename T>
 int raster_fwd(int H, int W, int B, int n, const int32_t *ids, const int32_t *bins,
                const int32_t *d_total, const void *xys, const void *con, const void *col,
@@ -582,20 +560,21 @@ int raster_fwd(int H, int W, int B, int n, const int32_t *ids, const int32_t *bi
                void *dy, void *dxy, int32_t *fin, cudaStream_t s) {
     int rc = pack<T>(n, xys, con, col, op, ws, ws_bytes, s);
     if (rc) return rc;
-    bool ga = dx != nullptr;
-    int tbx = (W + B - 1) / B, tby = (H + B - 1) / B;
-    int ppl = ga ? Cfg<T>::kFwdGA : Cfg<T>::kFwd;
-    int nbands = (nblocks_map(B, false) + ppl - 1) / ppl;
-    int nwork = tbx * tby * nbands;
-    int grid = (nwork + kWarpsPerCta - 1) / kWarpsPerCta;
+    const bool ga = dx != nullptr;
+    const int tbx = (W + B - 1) / B, tby = (H + B - 1) / B;
+    const int nt = 32 * Regions::make(0, B).count;
+    const size_t sm = (size_t)nt * (sizeof(Rec<T>) + sizeof(uint32_t));
+    const void *fn = ga ? (const void *)raster_fwd_kernel<T, true>
+                        : (const void *)raster_fwd_kernel<T, false>;
+    if (!set_dyn_smem(fn, sm)) return LIG_ERR_LAUNCH;
     if (ga)
-        raster_fwd_kernel<T, true, Cfg<T>::kFwdGA><<<grid, 32 * kWarpsPerCta, 0, s>>>(
-            H, W, B, tbx, nbands, nwork, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws,
-            (T *)img, (T *)wsum, (T *)dx, (T *)dy, (T *)dxy, fin);
+        raster_fwd_kernel<T, true><<<tbx * tby, nt, sm, s>>>(
+            H, W, B, tbx, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws, (T *)img,
+            (T *)wsum, (T *)dx, (T *)dy, (T *)dxy, fin);
     else
-        raster_fwd_kernel<T, false, Cfg<T>::kFwd><<<grid, 32 * kWarpsPerCta, 0, s>>>(
-            H, W, B, tbx, nbands, nwork, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws,
-            (T *)img, (T *)wsum, nullptr, nullptr, nullptr, fin);
+        raster_fwd_kernel<T, false><<<tbx * tby, nt, sm, s>>>(
+            H, W, B, tbx, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws, (T *)img,
+            (T *)wsum, nullptr, nullptr, nullptr, fin);
     note_launches(1);
     LIG_LAUNCH_CHECK();
     return LIG_OK;
@@ -615,23 +594,24 @@ int raster_bwd(int H, int W, int B, int n, const int32_t *ids, const int32_t *bi
     if (v_op) cudaMemsetAsync(v_op, 0, sizeof(T) * (size_t)n, s);
     int rc = pack<T>(n, xys, con, col, op, ws, ws_bytes, s);
     if (rc) return rc;
-    bool ga = v_dx != nullptr;
-    T cl = (T)(clamp > 0 ? clamp : (ga ? 0.999 : 0.99));
-    int tbx = (W + B - 1) / B, tby = (H + B - 1) / B;
-    int ppl = ga ? Cfg<T>::kBwdGA : Cfg<T>::kBwd;
-    int nbands = (nblocks_map(B, ga) + ppl - 1) / ppl;
-    int nwork = tbx * tby * nbands;
-    int grid = (nwork + kWarpsPerCta - 1) / kWarpsPerCta;
+    const bool ga = v_dx != nullptr;
+    const T cl = (T)(clamp > 0 ? clamp : (ga ? 0.999 : 0.99));
+    const int tbx = (W + B - 1) / B, tby = (H + B - 1) / B;
+    const int nt = 32 * Regions::make(ga ? 2 : 1, B).count;
+    const size_t sm = (size_t)nt * (sizeof(Rec<T>) + 2 * sizeof(uint32_t));
+    const void *fn = ga ? (const void *)raster_bwd_kernel<T, true>
+                        : (const void *)raster_bwd_kernel<T, false>;
+    if (!set_dyn_smem(fn, sm)) return LIG_ERR_LAUNCH;
     Grads<T> g{(T *)v_xy, (T *)v_abs, (T *)v_con, (T *)v_rgb, (T *)v_op};
     if (ga)
-        raster_bwd_kernel<T, true, Cfg<T>::kBwdGA><<<grid, 32 * kWarpsPerCta, 0, s>>>(
-            H, W, B, tbx, nbands, nwork, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws,
-            fin, (const T *)v_img, (const T *)v_wsum, (const T *)v_dx, (const T *)v_dy,
+        raster_bwd_kernel<T, true><<<tbx * tby, nt, sm, s>>>(
+            H, W, B, tbx, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws, fin,
+            (const T *)v_img, (const T *)v_wsum, (const T *)v_dx, (const T *)v_dy,
             (const T *)v_dxy, cl, g);
     else
-        raster_bwd_kernel<T, false, Cfg<T>::kBwd><<<grid, 32 * kWarpsPerCta, 0, s>>>(
-            H, W, B, tbx, nbands, nwork, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws,
-            fin, (const T *)v_img, (const T *)v_wsum, nullptr, nullptr, nullptr, cl, g);
+        raster_bwd_kernel<T, false><<<tbx * tby, nt, sm, s>>>(
+            H, W, B, tbx, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws, fin,
+            (const T *)v_img, (const T *)v_wsum, nullptr, nullptr, nullptr, cl, g);
     note_launches(1);
     LIG_LAUNCH_CHECK();
     return LIG_OK;
