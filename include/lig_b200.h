@@ -28,6 +28,7 @@ extern "C" {
 #define LIG_ERR_CAPACITY 2    /* intersection count exceeds the given capacity */
 #define LIG_ERR_LAUNCH 3      /* a kernel launch failed (cudaGetLastError) */
 #define LIG_ERR_WORKSPACE 4   /* workspace smaller than the *_workspace_bytes query */
+#define LIG_ERR_TOO_LARGE 5   /* num_points above LIG_STATIC_MAX_POINTS (allocation-free entry) */
 
 #define LIG_F32 0
 #define LIG_F64 1
@@ -155,6 +156,26 @@ int lig_raster_bwd(int dtype, int img_h, int img_w, int block_width, int num_poi
                    const void *v_dxy, double alpha_clamp, void *workspace,
                    size_t workspace_bytes, void *v_xy, void *v_xy_abs, void *v_conic,
                    void *v_rgb, void *v_opacity, void *stream);
+
+/* Sum rasterizer forward that allocates nothing.  No counterpart in the
+ * reference.  For callers that cannot allocate device memory when they render
+ * (e.g. a plugin running inside a framework that has reserved nearly all GPU
+ * memory for its own pool, or a real-time loop that forbids allocations after
+ * start-up): the scratch lig_raster_fwd takes as `workspace` comes from a
+ * fixed array inside the library (LIG_STATIC_MAX_POINTS records, 6 MiB per
+ * GPU, held until the process exits).  float32 only; otherwise identical to
+ * lig_raster_fwd with out_dx/out_dy/out_dxy = NULL.  Returns
+ * LIG_ERR_TOO_LARGE when num_points > LIG_STATIC_MAX_POINTS.  The first call
+ * on a device looks up the array's device address, so make it before any
+ * stream capture.  All calls on a device share the array (each call rewrites
+ * the records it uses): calls that overlap on that GPU, e.g. on two streams,
+ * race. */
+#define LIG_STATIC_MAX_POINTS 131072
+int lig_raster_fwd_noalloc(int img_h, int img_w, int block_width, int num_points,
+                           const int32_t *gaussian_ids_sorted, const int32_t *tile_bins,
+                           const int32_t *num_intersects, const float *xys, const float *conics,
+                           const float *colors, const float *opacities, float *out_img,
+                           float *out_wsum, int32_t *final_idx, void *stream);
 
 /* ---------------------------------------------------------------- upscale */
 

@@ -16,6 +16,8 @@ LIG_ERR_INVALID = 1
 LIG_ERR_CAPACITY = 2
 LIG_ERR_LAUNCH = 3
 LIG_ERR_WORKSPACE = 4
+LIG_ERR_TOO_LARGE = 5
+LIG_STATIC_MAX_POINTS = 131072
 LIG_F32 = 0
 LIG_F64 = 1
 LIG_STATUS_OVERFLOW = 1
@@ -26,6 +28,8 @@ _ERRORS = {
     LIG_ERR_CAPACITY: "intersection capacity exceeded",
     LIG_ERR_LAUNCH: "CUDA kernel launch failed",
     LIG_ERR_WORKSPACE: "workspace too small",
+    LIG_ERR_TOO_LARGE: f"more Gaussians than the allocation-free entry point's fixed scratch "
+                       f"holds ({LIG_STATIC_MAX_POINTS})",
 }
 
 P = ctypes.c_void_p
@@ -55,6 +59,7 @@ SIGNATURES = {
     "lig_upscale_fwd": (I, [I, I, I, I, I, I, D, D, D, D, P, P, P, P, P, P]),
     "lig_upscale_bwd": (I, [I, I, I, I, I, I, D, D, D, D, P, P, P, P, P, P]),
     "lig_probe_fp32": (I, [I, I, P, P]),
+    "lig_raster_fwd_noalloc": (I, [I, I, I, I, P, P, P, P, P, P, P, P, P, P, P]),
 }
 
 

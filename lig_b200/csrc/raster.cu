@@ -24,6 +24,8 @@
 // csrc/gradient_aware_rasterizer.cu:201-315, :434-482) so that the float
 // roundings, and with them the alpha-threshold decisions, are the same, and
 // each pixel adds its terms in list order.
+#include <mutex>
+
 #include "common.cuh"
 
 namespace lig {
@@ -671,3 +673,59 @@ extern "C" int lig_raster_bwd(int dtype, int H, int W, int B, int n, const int32
                                   v_con, v_rgb, v_op, s);
     return LIG_ERR_INVALID;
 }
+
+// ----------------------------------------------------- allocation-free entry
+// Some callers cannot allocate device memory at the time they render: a
+// plugin inside a framework that has already reserved (nearly) all of the
+// GPU's memory for its own pool, or a real-time loop whose host forbids
+// driver allocations after start-up.  For them, the sum forward below takes
+// its scratch (the packed per-Gaussian records) from a fixed array compiled
+// into this library instead of a caller workspace.  Every GPU that loads the
+// library keeps this array (LIG_STATIC_MAX_POINTS records, 6 MiB) until the
+// process exits.
+namespace lig {
+__device__ __align__(256) unsigned char g_noalloc_scratch[(size_t)LIG_STATIC_MAX_POINTS *
+                                                          sizeof(Rec<float>)];
+
+// Device address of the scratch array, looked up once per device (host code
+// cannot use the symbol itself: on the host it names a stand-in, not device
+// memory).  The first call on a device does the lookup.
+static void *noalloc_scratch_ptr(int &rc) {
+    static std::mutex mu;
+    static void *ptrs[128] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) {
+        rc = LIG_ERR_LAUNCH;
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!ptrs[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+            rc = LIG_ERR_LAUNCH;
+            return nullptr;
+        }
+        ptrs[dev] = p;
+    }
+    rc = LIG_OK;
+    return ptrs[dev];
+}
+}  // namespace lig
+
+extern "C" int lig_raster_fwd_noalloc(int H, int W, int B, int n, const int32_t *ids,
+                                      const int32_t *bins, const int32_t *d_total,
+                                      const float *xys, const float *con, const float *col,
+                                      const float *op, float *img, float *wsum, int32_t *fin,
+                                      void *stream) {
+    if (n > LIG_STATIC_MAX_POINTS) return LIG_ERR_TOO_LARGE;
+    if (!raster_args_ok(H, W, B, n) || !bins || !d_total || !img || !wsum || !fin ||
+        (n > 0 && (!xys || !con || !col)))
+        return LIG_ERR_INVALID;
+    int rc = LIG_OK;
+    void *scratch = noalloc_scratch_ptr(rc);
+    if (rc != LIG_OK) return rc;
+    return raster_fwd<float>(H, W, B, n, ids, bins, d_total, xys, con, col, op, scratch,
+                             sizeof(g_noalloc_scratch), img, wsum, nullptr, nullptr, nullptr, fin,
+                             (cudaStream_t)stream);
+}
+
