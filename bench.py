@@ -47,7 +47,7 @@ N_FIT = 2_000_000
 N_TEACHER = 2_000_000
 DIAG = (0.5, 6.0)
 BLOCK = 16
-FLOP_PER_EVAL = {"lig_raster_fwd": 20.0, "lig_raster_bwd": 40.0}
+FLOP_PER_EVAL = {"lig_raster_fwd": 20.0, "lig_raster_bwd": 40.0, "lig_raster_bwd_l2": 40.0}
 CLOCK_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")

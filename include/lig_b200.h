@@ -145,8 +145,9 @@ int lig_raster_fwd(int dtype, int img_h, int img_w, int block_width, int num_poi
 
 /* Rasterizer backward.  v_dx == NULL selects the sum variant (reference alpha
  * clamp 0.99), non-NULL the gradient-aware one (reference clamp 0.999);
- * alpha_clamp overrides the clamp when > 0.  v_opacity may be NULL.
- * All outputs are fully written.
+ * alpha_clamp overrides the clamp when > 0.  v_wsum and v_opacity may be NULL
+ * (v_wsum NULL = zero cotangent, an unused wsum output).  All outputs are
+ * fully written.
  * Replaces rasterize_backward_tensor (csrc/bindings.cu:403-506). */
 int lig_raster_bwd(int dtype, int img_h, int img_w, int block_width, int num_points,
                    const int32_t *gaussian_ids_sorted, const int32_t *tile_bins,
@@ -156,6 +157,31 @@ int lig_raster_bwd(int dtype, int img_h, int img_w, int block_width, int num_poi
                    const void *v_dxy, double alpha_clamp, void *workspace,
                    size_t workspace_bytes, void *v_xy, void *v_xy_abs, void *v_conic,
                    void *v_rgb, void *v_opacity, void *stream);
+
+/* Sum-rasterizer backward fused with the L2 fit loss: the pixel cotangent is
+ * the gradient of mean((clamp(img, 0, 1) - target)^2) times the device scalar
+ * *grad_loss, computed per pixel from img and target (both [H,W,3]) instead
+ * of read from a materialised dL/dimg; wsum cotangent zero.  Otherwise as
+ * lig_raster_bwd.  Replaces, in the fit loop, the clamp + F.mse_loss backward
+ * of gaussianlig.py:95-103 feeding rasterize_backward_tensor
+ * (csrc/bindings.cu:403-506). */
+int lig_raster_bwd_l2(int dtype, int img_h, int img_w, int block_width, int num_points,
+                      const int32_t *gaussian_ids_sorted, const int32_t *tile_bins,
+                      const int32_t *num_intersects, const void *xys, const void *conics,
+                      const void *colors, const void *opacities, const int32_t *final_idx,
+                      const void *img, const void *target, const void *grad_loss,
+                      double alpha_clamp, void *workspace, size_t workspace_bytes, void *v_xy,
+                      void *v_xy_abs, void *v_conic, void *v_rgb, void *v_opacity,
+                      void *stream);
+
+/* Workspace bytes of lig_l2_clamped_loss. */
+size_t lig_l2_workspace_bytes(void);
+
+/* mean((clamp(img, 0, 1) - target)^2) over n elements into the device scalar
+ * *loss, deterministic.  Replaces torch.clamp + F.mse_loss of the fit loop
+ * (gaussianlig.py:95-102, utils.py:17-21). */
+int lig_l2_clamped_loss(int dtype, int64_t n, const void *img, const void *target, void *loss,
+                        void *workspace, size_t workspace_bytes, void *stream);
 
 /* Sum rasterizer forward that allocates nothing.  No counterpart in the
  * reference.  For callers that cannot allocate device memory when they render

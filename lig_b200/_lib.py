@@ -60,6 +60,10 @@ SIGNATURES = {
     "lig_upscale_bwd": (I, [I, I, I, I, I, I, D, D, D, D, P, P, P, P, P, P]),
     "lig_probe_fp32": (I, [I, I, P, P]),
     "lig_raster_fwd_noalloc": (I, [I, I, I, I, P, P, P, P, P, P, P, P, P, P, P]),
+    "lig_raster_bwd_l2": (I, [I, I, I, I, I, P, P, P, P, P, P, P, P, P, P, P, D, P, SZ, P, P, P,
+                              P, P, P]),
+    "lig_l2_workspace_bytes": (SZ, []),
+    "lig_l2_clamped_loss": (I, [I, I64, P, P, P, P, SZ, P]),
 }
 
 

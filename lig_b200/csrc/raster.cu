@@ -33,16 +33,17 @@ namespace lig {
 template <typename T> struct alignas(16) Rec {
     T x, y, a, b;     // mean, conic (a, b)
     T c, o, wx, wy;   // conic c, opacity, cull half-widths (negative: never cull)
-    T r, g, bl, pad;  // colour
+    T r, g, bl, thr;  // colour, cull threshold on sigma
 };
 
 // ------------------------------------------------------------------ pack
-// Cull half-widths: the alpha >= 1/255 region of a positive-definite conic is
-// the ellipse sigma <= t/2, t = 2 ln(255 o), whose x half-extent is
-// sqrt(t Sxx).  We use t_c = max(t, 0.01) and w = 1.001 sqrt(t_c Sxx) + 2 px:
-// a pixel centre outside the box has sigma above the threshold by at least
-// ~sqrt(t_c/Sxx) + 0.001 t_c, orders of magnitude above float rounding of
-// sigma and __expf.  No culling (w < 0) for non-finite inputs, non-positive
+// Culling data: the alpha >= 1/255 region of a positive-definite conic is the
+// ellipse sigma <= t/2, t = 2 ln(255 o), whose x half-extent is sqrt(t Sxx).
+// With t_c = max(t, 0.01) the record carries the box half-widths
+// w = 1.001 sqrt(t_c Sxx) + 2 px and the sigma threshold
+// thr = 1.001 t_c/2 + 0.02: a pixel with sigma > thr has
+// alpha < exp(-0.02)/255, i.e. 2% below the reference's 1/255 cut, far beyond
+// the rounding of sigma and __expf, so skipping it changes nothing.  No culling (w < 0) for non-finite inputs, non-positive
 // opacity, non-positive-definite or nearly degenerate conics (b^2 > 0.999 ac),
 // where the reference's per-pixel tests must run everywhere in the tile.
 template <typename T>
@@ -61,7 +62,7 @@ __global__ void pack_kernel(int n, const T *__restrict__ xys, const T *__restric
     r.r = colors[3 * i];
     r.g = colors[3 * i + 1];
     r.bl = colors[3 * i + 2];
-    r.pad = 0;
+    r.thr = 0;
     double a = r.a, b = r.b, c = r.c, o = r.o;
     double det = a * c - b * b;
     bool ok = isfinite((double)r.x) && isfinite((double)r.y) && isfinite(a) && isfinite(b) &&
@@ -76,6 +77,7 @@ __global__ void pack_kernel(int n, const T *__restrict__ xys, const T *__restric
         if (hx < 1e7 && hy < 1e7) {
             wx = (T)hx;
             wy = (T)hy;
+            r.thr = (T)(0.5 * tc * 1.001 + 0.02);
         }
     }
     r.wx = wx;
@@ -113,6 +115,23 @@ struct Regions {
             ly = r < B * B ? r / B : B;  // B marks "no pixel"
         }
     }
+    // tile-local pixel-centre rectangle of region w (conservative)
+    template <typename T>
+    __device__ __forceinline__ void rect(int w, T &x0, T &x1, T &y0, T &y1) const {
+        int ix0, ix1, iy0, iy1;
+        if (kind == 2) {
+            const int r0 = w * 32, r1 = min(w * 32 + 31, B * B - 1);
+            iy0 = r0 / B; iy1 = r1 / B;
+            if (iy0 == iy1) { ix0 = r0 % B; ix1 = r1 % B; }
+            else { ix0 = 0; ix1 = B - 1; }
+        } else {
+            const int hb = kind == 0 ? 4 : 8;
+            ix0 = (w % nbx) * 8; ix1 = min(ix0 + 7, B - 1);
+            iy0 = (w / nbx) * hb; iy1 = min(iy0 + hb - 1, B - 1);
+        }
+        x0 = (T)ix0 + (T)0.5; x1 = (T)ix1 + (T)0.5;
+        y0 = (T)iy0 + (T)0.5; y1 = (T)iy1 + (T)0.5;
+    }
     __device__ __forceinline__ uint32_t all() const {
         return count >= 32 ? 0xffffffffu : ((1u << count) - 1u);
     }
@@ -147,16 +166,52 @@ struct Regions {
     }
 };
 
-// Region mask of one Gaussian for the tile at pixel origin (tx0, ty0).  The
-// cull box (see pack_kernel) has margin, so every pixel outside it fails the
-// reference's own alpha >= 1/255 test; records without a box (wx < 0) touch
-// every region.
+// Minimum of sigma(d) = 0.5 (a dx^2 + c dy^2) + b dx dy over the rectangle
+// [dx0, dx1] x [dy0, dy1] (positive-definite conic): zero if the rectangle
+// holds the origin, else the least of the four edge minima (each a clamped
+// 1-D quadratic minimum).
 template <typename T>
+__device__ __forceinline__ T sigma_min_rect(T a, T b, T c, T dx0, T dx1, T dy0, T dy1) {
+    if (dx0 <= (T)0 && dx1 >= (T)0 && dy0 <= (T)0 && dy1 >= (T)0) return (T)0;
+    const T ia = (T)1 / a, ic = (T)1 / c;
+    T best = (T)3.0e38;
+    const T xs[2] = {dx0, dx1}, ys[2] = {dy0, dy1};
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+        T dx = xs[e];
+        T dy = min(max(-b * dx * ic, dy0), dy1);
+        best = min(best, (T)0.5 * (a * dx * dx + c * dy * dy) + b * dx * dy);
+        dy = ys[e];
+        dx = min(max(-b * dy * ia, dx0), dx1);
+        best = min(best, (T)0.5 * (a * dx * dx + c * dy * dy) + b * dx * dy);
+    }
+    return best;
+}
+
+// Region mask of one Gaussian for the tile at pixel origin (tx0, ty0): the
+// regions whose pixel-centre rectangle meets the Gaussian's cull box and, on
+// it, reaches sigma <= thr (see pack_kernel: every pixel with sigma > thr
+// fails the reference's own alpha >= 1/255 test).  Records without culling
+// data (wx < 0) touch every region.
+// ELLIPSE = false stops at the box test: cheaper to build, used where the
+// per-pair work is small (forward).
+template <typename T, bool ELLIPSE = true>
 __device__ __forceinline__ uint32_t region_bits(const Rec<T> &g, const Regions &R, int tx0,
                                                 int ty0) {
     if (!(g.wx >= (T)0)) return R.all();
-    T cx = g.x - (T)tx0, cy = g.y - (T)ty0;
-    return R.bits<T>(cx - g.wx, cx + g.wx, cy - g.wy, cy + g.wy);
+    const T cx = g.x - (T)tx0, cy = g.y - (T)ty0;
+    uint32_t m = R.bits<T>(cx - g.wx, cx + g.wx, cy - g.wy, cy + g.wy);
+    if (!ELLIPSE) return m;
+    uint32_t keep = m;
+    while (m) {
+        const int w = __ffs(m) - 1;
+        m &= m - 1;
+        T x0, x1, y0, y1;
+        R.rect<T>(w, x0, x1, y0, y1);
+        if (sigma_min_rect<T>(g.a, g.b, g.c, x0 - cx, x1 - cx, y0 - cy, y1 - cy) > g.thr)
+            keep &= ~(1u << w);
+    }
+    return keep;
 }
 
 // --------------------------------------------------------------- forward
@@ -255,7 +310,7 @@ raster_fwd_kernel(int H, int W, int B, int tbx, const int32_t *__restrict__ ids,
         __syncthreads();
         if (tid < cnt) {
             s_rec[tid] = pre;
-            s_bits[tid] = region_bits(pre, R, tx0, ty0);
+            s_bits[tid] = region_bits<T, false>(pre, R, tx0, ty0);
         }
         __syncthreads();
         if (base + nt + tid < range.y) pre = recs[__ldg(ids + base + nt + tid)];
@@ -300,41 +355,6 @@ raster_fwd_kernel(int H, int W, int B, int tbx, const int32_t *__restrict__ ids,
 }
 
 // ------------------------------------------------------------- backward
-// Transpose-reduce of 16 per-lane values over the warp in 16 shuffles: after
-// the call lane l holds the warp sum of value ((l >> 1) & 15) in v[0].
-template <typename T>
-__device__ __forceinline__ void transpose_reduce16(T (&v)[16], int lane) {
-    const unsigned FULL = 0xffffffffu;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        bool up = lane & 16;
-        T send = up ? v[k] : v[k + 8];
-        T keep = up ? v[k + 8] : v[k];
-        v[k] = keep + __shfl_xor_sync(FULL, send, 16);
-    }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        bool up = lane & 8;
-        T send = up ? v[k] : v[k + 4];
-        T keep = up ? v[k + 4] : v[k];
-        v[k] = keep + __shfl_xor_sync(FULL, send, 8);
-    }
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-        bool up = lane & 4;
-        T send = up ? v[k] : v[k + 2];
-        T keep = up ? v[k + 2] : v[k];
-        v[k] = keep + __shfl_xor_sync(FULL, send, 4);
-    }
-    {
-        bool up = lane & 2;
-        T send = up ? v[0] : v[1];
-        T keep = up ? v[1] : v[0];
-        v[0] = keep + __shfl_xor_sync(FULL, send, 2);
-    }
-    v[0] += __shfl_xor_sync(FULL, v[0], 1);
-}
-
 template <typename T>
 struct Grads {
     T *v_xy, *v_abs, *v_conic, *v_rgb, *v_opac;
@@ -350,69 +370,108 @@ struct Grads {
     }
 };
 
-// One CTA per tile.  Sum variant: warp = 8x8 region, lane owns 2 pixels;
-// gradient-aware: warp = reference warp (its v_xy_abs is |sum over the warp|,
-// csrc/gradient_aware_rasterizer.cu:317-341), lane owns 1 pixel.  Batches and
-// region masks as in the forward, over the list prefix that can contribute
-// (entries past every pixel's final index are skipped).  Per Gaussian a lane
-// accumulates its 11 gradient terms over its pixels, the warp reduces them
-// with one 16-shuffle transpose-reduce and 11 lanes issue the atomics.
+// Backward, transposed: one CTA per tile, warp w owns region w (an 8x4 block in
+// the sum variant; in the gradient-aware variant the reference's warp w, whose
+// v_xy_abs is |sum over that warp| per Gaussian,
+// csrc/gradient_aware_rasterizer.cu:317-341).  The tile's pixel cotangents,
+// pixel centres and final indices are staged in shared memory once, region
+// by region.  Per batch each warp compacts the batch slots whose region mask
+// has its bit; lanes then take one such Gaussian each and loop over the
+// region's 32 pixels (pixel data read by broadcast), so every lane
+// accumulates its own Gaussian's gradient terms in registers — no cross-lane
+// reduction — and adds them to the packed [N][12] gradient buffer with three
+// 16-byte atomics per (Gaussian, region).  Entries past every pixel's final
+// index are skipped.
+// Pixel cotangent source of the backward: explicit dL/dimg (+ optional
+// dL/dwsum), or — fused L2 — computed on the fly from the render and the target
+// as the gradient of mean((clamp(img, 0, 1) - target)^2): the value torch's
+// mse_loss + clamp backward produce, 2/N (clamp(x) - t) g where 0 <= x <= 1.
+template <typename T>
+struct CotSrc {
+    const T *v_img, *v_wsum;              // explicit (v_wsum may be null: zero)
+    const T *img, *target, *grad_loss;    // fused L2 (v_img == null)
+    T scale;                              // 2 / numel
+    __device__ __forceinline__ void get(int p, T &r, T &g, T &b, T &w) const {
+        w = v_wsum ? v_wsum[p] : (T)0;
+        if (v_img) {
+            r = v_img[3 * p];
+            g = v_img[3 * p + 1];
+            b = v_img[3 * p + 2];
+            return;
+        }
+        const T s = scale * *grad_loss;
+        T v[3];
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch) {
+            const T x = img[3 * p + ch];
+            const T d = min(max(x, (T)0), (T)1) - target[3 * p + ch];
+            v[ch] = (x >= (T)0 && x <= (T)1) ? d * s : (T)0;
+        }
+        r = v[0]; g = v[1]; b = v[2];
+    }
+};
+
+template <typename T, bool GA>
+struct alignas(16) PixRec {
+    T px, py, vw, vo0, vo1, vo2;
+    int fin;
+    T vd[GA ? 9 : 1];  // vdx.rgb, vdy.rgb, vdxy.rgb
+};
+
 template <typename T, bool GA>
 __global__ void __launch_bounds__(1024)
 raster_bwd_kernel(int H, int W, int B, int tbx, const int32_t *__restrict__ ids,
                   const int2 *__restrict__ tile_bins, const int32_t *__restrict__ d_total,
                   const Rec<T> *__restrict__ recs, const int32_t *__restrict__ final_idx,
-                  const T *__restrict__ v_img, const T *__restrict__ v_wsum,
-                  const T *__restrict__ v_dx, const T *__restrict__ v_dy,
-                  const T *__restrict__ v_dxy, T clamp, Grads<T> out) {
+                  CotSrc<T> cot, const T *__restrict__ v_dx, const T *__restrict__ v_dy,
+                  const T *__restrict__ v_dxy, T clamp, T *__restrict__ packed) {
     using M = Math<T>;
-    constexpr int PPL = GA ? 1 : 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int nt = blockDim.x;
-    Rec<T> *s_rec = reinterpret_cast<Rec<T> *>(smem_raw);
+    const int nt = blockDim.x;  // = 32 * regions: region-major pixel slots
+    PixRec<T, GA> *s_pix = reinterpret_cast<PixRec<T, GA> *>(smem_raw);
+    Rec<T> *s_rec = reinterpret_cast<Rec<T> *>(s_pix + nt);
     uint32_t *s_bits = reinterpret_cast<uint32_t *>(s_rec + nt);
     int32_t *s_ids = reinterpret_cast<int32_t *>(s_bits + nt);
+    uint16_t *s_list = reinterpret_cast<uint16_t *>(s_ids + nt);
     __shared__ int s_end;
     const unsigned FULL = 0xffffffffu;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     if (*d_total == 0) return;  // gradients stay zero (rasterize.py:156-161)
     const int tile = blockIdx.x;
     const int tx0 = (tile % tbx) * B, ty0 = (tile / tbx) * B;
-    const Regions R = Regions::make(GA ? 2 : 1, B);
+    const Regions R = Regions::make(GA ? 2 : 0, B);
+    uint16_t *my_list = s_list + w * nt;
+    const PixRec<T, GA> *my_pix = s_pix + w * 32;
 
-    T px[PPL], py[PPL], vo[PPL][3], vw[PPL];
-    T vdx[GA ? 1 : 1][3], vdy[GA ? 1 : 1][3], vdxy[GA ? 1 : 1][3];
-    int fin[PPL];
-    int my_fin = -1;
-#pragma unroll
-    for (int p = 0; p < PPL; ++p) {
+    // stage this thread's pixel (region w, slot lane)
+    if (tid == 0) s_end = -1;
+    {
         int lx, ly;
-        R.pixel(w, lane, p, lx, ly);
+        R.pixel(w, lane, 0, lx, ly);
         const int gx = tx0 + lx, gy = ty0 + ly;
         const bool inside = lx < B && ly < B && gx < W && gy < H;
-        const int q = inside ? gy * W + gx : 0;
-        px[p] = (T)gx + (T)0.5;
-        py[p] = (T)gy + (T)0.5;
-        fin[p] = inside ? final_idx[q] : -1;  // -1: never valid
-        vo[p][0] = inside ? v_img[3 * q] : (T)0;
-        vo[p][1] = inside ? v_img[3 * q + 1] : (T)0;
-        vo[p][2] = inside ? v_img[3 * q + 2] : (T)0;
-        vw[p] = inside ? v_wsum[q] : (T)0;
-        if (GA) {
+        const int p = inside ? gy * W + gx : 0;
+        PixRec<T, GA> c;
+        c.px = (T)gx + (T)0.5;
+        c.py = (T)gy + (T)0.5;
+        c.vo0 = c.vo1 = c.vo2 = c.vw = (T)0;
+        if (inside) cot.get(p, c.vo0, c.vo1, c.vo2, c.vw);
+        c.fin = inside ? final_idx[p] : -1;  // -1: never valid
+        if constexpr (GA) {
 #pragma unroll
             for (int ch = 0; ch < 3; ++ch) {
-                vdx[0][ch] = inside ? v_dx[3 * q + ch] : (T)0;
-                vdy[0][ch] = inside ? v_dy[3 * q + ch] : (T)0;
-                vdxy[0][ch] = inside ? v_dxy[3 * q + ch] : (T)0;
+                c.vd[ch] = inside ? v_dx[3 * p + ch] : (T)0;
+                c.vd[3 + ch] = inside ? v_dy[3 * p + ch] : (T)0;
+                c.vd[6 + ch] = inside ? v_dxy[3 * p + ch] : (T)0;
             }
         }
-        my_fin = max(my_fin, fin[p]);
-    }
-    if (tid == 0) s_end = -1;
-    __syncthreads();
+        s_pix[tid] = c;
+        int my_max = c.fin;
 #pragma unroll
-    for (int o = 16; o >= 1; o >>= 1) my_fin = max(my_fin, __shfl_xor_sync(FULL, my_fin, o));
-    if (lane == 0) atomicMax(&s_end, my_fin);
+        for (int o = 16; o >= 1; o >>= 1) my_max = max(my_max, __shfl_xor_sync(FULL, my_max, o));
+        __syncthreads();
+        if (lane == 0) atomicMax(&s_end, my_max);
+    }
     __syncthreads();
     const int2 range = tile_bins[tile];
     const int end = min(range.y, s_end + 1);
@@ -436,104 +495,136 @@ raster_bwd_kernel(int H, int W, int B, int tbx, const int32_t *__restrict__ ids,
             pre_id = __ldg(ids + base + nt + tid);
             pre = recs[pre_id];
         }
+        // compact the batch slots touching this region (ascending)
+        int nmine = 0;
         for (int m = 0; m * 32 < cnt; ++m) {
             const int t = m * 32 + lane;
-            uint32_t mask = __ballot_sync(FULL, t < cnt && ((s_bits[t] >> w) & 1u));
-            while (mask) {
-                const int bsel = __ffs(mask) - 1;
-                mask &= mask - 1;
-                const int slot = m * 32 + bsel;
-                const Rec<T> g = s_rec[slot];
-                const int k = base + slot;
-                T v[16];
+            const bool hit = t < cnt && ((s_bits[t] >> w) & 1u);
+            const uint32_t mask = __ballot_sync(FULL, hit);
+            if (hit) my_list[nmine + __popc(mask & ((1u << lane) - 1u))] = (uint16_t)t;
+            nmine += __popc(mask);
+        }
+        __syncwarp();
+        for (int g0 = 0; g0 < nmine; g0 += 32) {
+            const int slot = g0 + lane < nmine ? (int)my_list[g0 + lane] : -1;
+            const bool act = slot >= 0;
+            const Rec<T> g = s_rec[act ? slot : 0];
+            const int k = act ? base + slot : 0x7fffffff;
+            T acc[11];
 #pragma unroll
-                for (int q = 0; q < 16; ++q) v[q] = 0;
-                bool any = false;
+            for (int q = 0; q < 11; ++q) acc[q] = 0;
+            bool touched = false;
+            for (int j = 0; j < 32; ++j) {
+                const PixRec<T, GA> &c = my_pix[j];
+                if (k > c.fin) continue;
+                if constexpr (!GA) {
+                    // csrc/backward.cu:102-150
+                    const T dx = g.x - c.px;
+                    const T dy = g.y - c.py;
+                    const T sigma = (T)0.5 * (g.a * dx * dx + g.c * dy * dy) + g.b * dx * dy;
+                    const T vis = M::exp_(-sigma);
+                    const T alpha = M::min_(clamp, g.o * vis);
+                    if (sigma < (T)0 || alpha < (T)1 / (T)255) continue;
+                    touched = true;
+                    T v_alpha = 0;
+                    acc[7] += alpha * c.vo0;
+                    acc[8] += alpha * c.vo1;
+                    acc[9] += alpha * c.vo2;
+                    v_alpha += g.r * c.vo0;
+                    v_alpha += g.g * c.vo1;
+                    v_alpha += g.bl * c.vo2;
+                    v_alpha += c.vw;
+                    acc[10] += vis * v_alpha;
+                    const T v_sigma = -alpha * v_alpha;
+                    acc[4] += (T)0.5 * v_sigma * dx * dx;
+                    acc[5] += v_sigma * dx * dy;
+                    acc[6] += (T)0.5 * v_sigma * dy * dy;
+                    const T gx = v_sigma * (g.a * dx + g.b * dy);
+                    const T gy = v_sigma * (g.b * dx + g.c * dy);
+                    acc[0] += gx;
+                    acc[1] += gy;
+                    acc[2] += M::abs_(gx);
+                    acc[3] += M::abs_(gy);
+                } else {
+                    // csrc/gradient_aware_rasterizer.cu:201-315
+                    const T dx = c.px - g.x;
+                    const T dy = c.py - g.y;
+                    const T sigma = (T)0.5 * (g.a * dx * dx + g.c * dy * dy) + g.b * dx * dy;
+                    const T vis = M::exp_(-sigma);
+                    const T alpha = M::min_(clamp, g.o * vis);
+                    if (sigma < (T)0 || alpha < (T)1 / (T)255) continue;
+                    touched = true;
+                    const T sx = g.a * dx + g.b * dy;
+                    const T sy = g.b * dx + g.c * dy;
+                    const T a = g.a, b = g.b, cc = g.c;
+                    const T ax = -alpha * sx;
+                    const T ay = -alpha * sy;
+                    const T axy = alpha * (sx * sy - b);
+                    const T vo[3] = {c.vo0, c.vo1, c.vo2};
+                    const T *vdx = c.vd, *vdy = c.vd + 3, *vdxy = c.vd + 6;
+                    acc[7] += vo[0] * alpha + vdx[0] * ax + vdy[0] * ay + vdxy[0] * axy;
+                    acc[8] += vo[1] * alpha + vdx[1] * ax + vdy[1] * ay + vdxy[1] * axy;
+                    acc[9] += vo[2] * alpha + vdx[2] * ax + vdy[2] * ay + vdxy[2] * axy;
+                    const T va = (vo[0] * g.r + vo[1] * g.g + vo[2] * g.bl) + c.vw;
+                    const T vax = vdx[0] * g.r + vdx[1] * g.g + vdx[2] * g.bl;
+                    const T vay = vdy[0] * g.r + vdy[1] * g.g + vdy[2] * g.bl;
+                    const T vaxy = vdxy[0] * g.r + vdxy[1] * g.g + vdxy[2] * g.bl;
+                    const T sx2 = sx * sx, sy2 = sy * sy, sxsy = sx * sy;
+                    acc[0] += alpha * (va * sx + vax * (a - sx2) + vay * (b - sxsy) +
+                                       vaxy * (sx2 * sy - (T)2 * b * sx - a * sy));
+                    acc[1] += alpha * (va * sy + vax * (b - sxsy) + vay * (cc - sy2) +
+                                       vaxy * (sx * sy2 - (T)2 * b * sy - cc * sx));
+                    const T dx2 = dx * dx, dy2 = dy * dy, dxdy = dx * dy;
+                    const T P = sxsy - b;
+                    acc[4] += alpha * (va * (-(T)0.5 * dx2) + vax * ((T)0.5 * dx2 * sx - dx) +
+                                       vay * ((T)0.5 * dx2 * sy) +
+                                       vaxy * (-(T)0.5 * dx2 * P + dx * sy));
+                    acc[5] += alpha * (va * (-dxdy) + vax * (dxdy * sx - dy) +
+                                       vay * (dxdy * sy - dx) +
+                                       vaxy * (-dxdy * P + dy * sy + dx * sx - (T)1));
+                    acc[6] += alpha * (va * (-(T)0.5 * dy2) + vax * ((T)0.5 * dy2 * sx) +
+                                       vay * ((T)0.5 * dy2 * sy - dy) +
+                                       vaxy * (-(T)0.5 * dy2 * P + dy * sx));
+                    acc[10] += vis * va;
+                }
+            }
+            if (touched) {
+                if (GA) {  // |sum over the reference warp| (= this region)
+                    acc[2] = M::abs_(acc[0]);
+                    acc[3] = M::abs_(acc[1]);
+                }
+                T *dst = packed + (size_t)s_ids[slot] * 12;
+                if constexpr (sizeof(T) == 4) {
+                    float4 *d4 = reinterpret_cast<float4 *>(dst);
+                    atomicAdd(d4, make_float4(acc[0], acc[1], acc[2], acc[3]));
+                    atomicAdd(d4 + 1, make_float4(acc[4], acc[5], acc[6], acc[7]));
+                    atomicAdd(d4 + 2, make_float4(acc[8], acc[9], acc[10], 0.f));
+                } else {
 #pragma unroll
-                for (int p = 0; p < PPL; ++p) {
-                    if (k > fin[p]) continue;
-                    if (!GA) {
-                        // csrc/backward.cu:102-150
-                        const T dx = g.x - px[p];
-                        const T dy = g.y - py[p];
-                        const T sigma = (T)0.5 * (g.a * dx * dx + g.c * dy * dy) + g.b * dx * dy;
-                        const T vis = M::exp_(-sigma);
-                        const T alpha = M::min_(clamp, g.o * vis);
-                        if (sigma < (T)0 || alpha < (T)1 / (T)255) continue;
-                        any = true;
-                        T v_alpha = 0;
-                        v[7] += alpha * vo[p][0];
-                        v[8] += alpha * vo[p][1];
-                        v[9] += alpha * vo[p][2];
-                        v_alpha += g.r * vo[p][0];
-                        v_alpha += g.g * vo[p][1];
-                        v_alpha += g.bl * vo[p][2];
-                        v_alpha += vw[p];
-                        v[10] += vis * v_alpha;
-                        const T v_sigma = -alpha * v_alpha;
-                        v[4] += (T)0.5 * v_sigma * dx * dx;
-                        v[5] += v_sigma * dx * dy;
-                        v[6] += (T)0.5 * v_sigma * dy * dy;
-                        const T gx = v_sigma * (g.a * dx + g.b * dy);
-                        const T gy = v_sigma * (g.b * dx + g.c * dy);
-                        v[0] += gx;
-                        v[1] += gy;
-                        v[2] += M::abs_(gx);
-                        v[3] += M::abs_(gy);
-                    } else {
-                        // csrc/gradient_aware_rasterizer.cu:201-315
-                        const T dx = px[p] - g.x;
-                        const T dy = py[p] - g.y;
-                        const T sigma = (T)0.5 * (g.a * dx * dx + g.c * dy * dy) + g.b * dx * dy;
-                        const T vis = M::exp_(-sigma);
-                        const T alpha = M::min_(clamp, g.o * vis);
-                        if (sigma < (T)0 || alpha < (T)1 / (T)255) continue;
-                        any = true;
-                        const T sx = g.a * dx + g.b * dy;
-                        const T sy = g.b * dx + g.c * dy;
-                        const T a = g.a, b = g.b, cc = g.c;
-                        const T ax = -alpha * sx;
-                        const T ay = -alpha * sy;
-                        const T axy = alpha * (sx * sy - b);
-                        v[7] += vo[p][0] * alpha + vdx[0][0] * ax + vdy[0][0] * ay + vdxy[0][0] * axy;
-                        v[8] += vo[p][1] * alpha + vdx[0][1] * ax + vdy[0][1] * ay + vdxy[0][1] * axy;
-                        v[9] += vo[p][2] * alpha + vdx[0][2] * ax + vdy[0][2] * ay + vdxy[0][2] * axy;
-                        const T va = (vo[p][0] * g.r + vo[p][1] * g.g + vo[p][2] * g.bl) + vw[p];
-                        const T vax = vdx[0][0] * g.r + vdx[0][1] * g.g + vdx[0][2] * g.bl;
-                        const T vay = vdy[0][0] * g.r + vdy[0][1] * g.g + vdy[0][2] * g.bl;
-                        const T vaxy = vdxy[0][0] * g.r + vdxy[0][1] * g.g + vdxy[0][2] * g.bl;
-                        const T sx2 = sx * sx, sy2 = sy * sy, sxsy = sx * sy;
-                        v[0] += alpha * (va * sx + vax * (a - sx2) + vay * (b - sxsy) +
-                                         vaxy * (sx2 * sy - (T)2 * b * sx - a * sy));
-                        v[1] += alpha * (va * sy + vax * (b - sxsy) + vay * (cc - sy2) +
-                                         vaxy * (sx * sy2 - (T)2 * b * sy - cc * sx));
-                        const T dx2 = dx * dx, dy2 = dy * dy, dxdy = dx * dy;
-                        const T P = sxsy - b;
-                        v[4] += alpha * (va * (-(T)0.5 * dx2) + vax * ((T)0.5 * dx2 * sx - dx) +
-                                         vay * ((T)0.5 * dx2 * sy) +
-                                         vaxy * (-(T)0.5 * dx2 * P + dx * sy));
-                        v[5] += alpha * (va * (-dxdy) + vax * (dxdy * sx - dy) +
-                                         vay * (dxdy * sy - dx) +
-                                         vaxy * (-dxdy * P + dy * sy + dx * sx - (T)1));
-                        v[6] += alpha * (va * (-(T)0.5 * dy2) + vax * ((T)0.5 * dy2 * sx) +
-                                         vay * ((T)0.5 * dy2 * sy - dy) +
-                                         vaxy * (-(T)0.5 * dy2 * P + dy * sx));
-                        v[10] += vis * va;
-                    }
+                    for (int q = 0; q < 11; ++q) atomicAdd(dst + q, acc[q]);
                 }
-                if (!__any_sync(FULL, any)) continue;
-                transpose_reduce16(v, lane);
-                const int kk = (lane >> 1) & 15;
-                T val = v[0];
-                if (GA) {
-                    // lanes of values 2/3 take |warp sum of v_xy| from lanes of values 0/1
-                    const T src = __shfl_sync(FULL, v[0], (lane - 4) & 31);
-                    if (kk == 2 || kk == 3) val = M::abs_(src);
-                }
-                if ((lane & 1) == 0 && kk < 11) out.add(kk, s_ids[slot], val);
             }
         }
     }
+}
+
+// Packed per-Gaussian gradients [N][12] -> the five output arrays of the ABI.
+template <typename T>
+__global__ void unpack_grads_kernel(int n, const T *__restrict__ packed, Grads<T> out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const T *g = packed + (size_t)i * 12;
+    out.v_xy[2 * i] = g[0];
+    out.v_xy[2 * i + 1] = g[1];
+    out.v_abs[2 * i] = g[2];
+    out.v_abs[2 * i + 1] = g[3];
+    out.v_conic[3 * i] = g[4];
+    out.v_conic[3 * i + 1] = g[5];
+    out.v_conic[3 * i + 2] = g[6];
+    out.v_rgb[3 * i] = g[7];
+    out.v_rgb[3 * i + 1] = g[8];
+    out.v_rgb[3 * i + 2] = g[9];
+    if (out.v_opac) out.v_opac[i] = g[10];
 }
 
 // ------------------------------------------------------------------ host
@@ -582,39 +673,46 @@ int raster_fwd(int H, int W, int B, int n, const int32_t *ids, const int32_t *bi
     return LIG_OK;
 }
 
+// Backward workspace: packed records [N] followed by packed gradients [N][12].
+template <typename T>
+inline size_t bwd_grad_offset(int n) {
+    return (sizeof(Rec<T>) * (size_t)(n > 0 ? n : 1) + 255) & ~(size_t)255;
+}
+
 template <typename T>
 int raster_bwd(int H, int W, int B, int n, const int32_t *ids, const int32_t *bins,
                const int32_t *d_total, const void *xys, const void *con, const void *col,
-               const void *op, const int32_t *fin, const void *v_img, const void *v_wsum,
-               const void *v_dx, const void *v_dy, const void *v_dxy, double clamp, void *ws,
-               size_t ws_bytes, void *v_xy, void *v_abs, void *v_con, void *v_rgb, void *v_op,
-               cudaStream_t s) {
-    cudaMemsetAsync(v_xy, 0, sizeof(T) * 2 * (size_t)n, s);
-    cudaMemsetAsync(v_abs, 0, sizeof(T) * 2 * (size_t)n, s);
-    cudaMemsetAsync(v_con, 0, sizeof(T) * 3 * (size_t)n, s);
-    cudaMemsetAsync(v_rgb, 0, sizeof(T) * 3 * (size_t)n, s);
-    if (v_op) cudaMemsetAsync(v_op, 0, sizeof(T) * (size_t)n, s);
-    int rc = pack<T>(n, xys, con, col, op, ws, ws_bytes, s);
+               const void *op, const int32_t *fin, CotSrc<T> cot, const void *v_dx,
+               const void *v_dy, const void *v_dxy, double clamp, void *ws, size_t ws_bytes,
+               void *v_xy, void *v_abs, void *v_con, void *v_rgb, void *v_op, cudaStream_t s) {
+    const size_t goff = bwd_grad_offset<T>(n);
+    if (ws_bytes < goff + sizeof(T) * 12 * (size_t)n) return LIG_ERR_WORKSPACE;
+    T *packed = reinterpret_cast<T *>((char *)ws + goff);
+    cudaMemsetAsync(packed, 0, sizeof(T) * 12 * (size_t)n, s);
+    int rc = pack<T>(n, xys, con, col, op, ws, goff, s);
     if (rc) return rc;
     const bool ga = v_dx != nullptr;
     const T cl = (T)(clamp > 0 ? clamp : (ga ? 0.999 : 0.99));
     const int tbx = (W + B - 1) / B, tby = (H + B - 1) / B;
-    const int nt = 32 * Regions::make(ga ? 2 : 1, B).count;
-    const size_t sm = (size_t)nt * (sizeof(Rec<T>) + 2 * sizeof(uint32_t));
+    const int nt = 32 * Regions::make(ga ? 2 : 0, B).count;
+    const int nw = nt / 32;
+    const size_t pix = ga ? sizeof(PixRec<T, true>) : sizeof(PixRec<T, false>);
+    const size_t sm = (size_t)nt * pix + (size_t)nt * (sizeof(Rec<T>) + 2 * sizeof(uint32_t)) +
+                      (size_t)nw * nt * sizeof(uint16_t);
     const void *fn = ga ? (const void *)raster_bwd_kernel<T, true>
                         : (const void *)raster_bwd_kernel<T, false>;
     if (!set_dyn_smem(fn, sm)) return LIG_ERR_LAUNCH;
-    Grads<T> g{(T *)v_xy, (T *)v_abs, (T *)v_con, (T *)v_rgb, (T *)v_op};
     if (ga)
         raster_bwd_kernel<T, true><<<tbx * tby, nt, sm, s>>>(
-            H, W, B, tbx, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws, fin,
-            (const T *)v_img, (const T *)v_wsum, (const T *)v_dx, (const T *)v_dy,
-            (const T *)v_dxy, cl, g);
+            H, W, B, tbx, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws, fin, cot,
+            (const T *)v_dx, (const T *)v_dy, (const T *)v_dxy, cl, packed);
     else
         raster_bwd_kernel<T, false><<<tbx * tby, nt, sm, s>>>(
-            H, W, B, tbx, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws, fin,
-            (const T *)v_img, (const T *)v_wsum, nullptr, nullptr, nullptr, cl, g);
-    note_launches(1);
+            H, W, B, tbx, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws, fin, cot,
+            nullptr, nullptr, nullptr, cl, packed);
+    Grads<T> g{(T *)v_xy, (T *)v_abs, (T *)v_con, (T *)v_rgb, (T *)v_op};
+    if (n > 0) unpack_grads_kernel<T><<<(n + 255) / 256, 256, 0, s>>>(n, packed, g);
+    note_launches(n > 0 ? 2 : 1);
     LIG_LAUNCH_CHECK();
     return LIG_OK;
 }
@@ -628,8 +726,9 @@ inline bool raster_args_ok(int H, int W, int B, int n) {
 using namespace lig;
 
 extern "C" size_t lig_raster_workspace_bytes(int dtype, int n) {
-    size_t rec = dtype == LIG_F64 ? sizeof(Rec<double>) : sizeof(Rec<float>);
-    return rec * (size_t)(n > 0 ? n : 1);
+    size_t m = (size_t)(n > 0 ? n : 1);
+    if (dtype == LIG_F64) return bwd_grad_offset<double>(n) + sizeof(double) * 12 * m;
+    return bwd_grad_offset<float>(n) + sizeof(float) * 12 * m;
 }
 
 extern "C" int lig_raster_fwd(int dtype, int H, int W, int B, int n, const int32_t *ids,
@@ -657,20 +756,54 @@ extern "C" int lig_raster_bwd(int dtype, int H, int W, int B, int n, const int32
                               const void *v_dx, const void *v_dy, const void *v_dxy,
                               double clamp, void *ws, size_t ws_bytes, void *v_xy, void *v_abs,
                               void *v_con, void *v_rgb, void *v_op, void *stream) {
-    if (!raster_args_ok(H, W, B, n) || !bins || !d_total || !fin || !v_img || !v_wsum || !ws ||
+    if (!raster_args_ok(H, W, B, n) || !bins || !d_total || !fin || !v_img || !ws ||
         (n > 0 && (!xys || !con || !col || !v_xy || !v_abs || !v_con || !v_rgb)) ||
         ((v_dx || v_dy || v_dxy) && !(v_dx && v_dy && v_dxy)))
         return LIG_ERR_INVALID;
     cudaStream_t s = (cudaStream_t)stream;
     if (n == 0) return LIG_OK;
-    if (dtype == LIG_F32)
-        return raster_bwd<float>(H, W, B, n, ids, bins, d_total, xys, con, col, op, fin, v_img,
-                                 v_wsum, v_dx, v_dy, v_dxy, clamp, ws, ws_bytes, v_xy, v_abs,
+    if (dtype == LIG_F32) {
+        CotSrc<float> cot{(const float *)v_img, (const float *)v_wsum, nullptr, nullptr, nullptr, 0.f};
+        return raster_bwd<float>(H, W, B, n, ids, bins, d_total, xys, con, col, op, fin, cot,
+                                 v_dx, v_dy, v_dxy, clamp, ws, ws_bytes, v_xy, v_abs, v_con,
+                                 v_rgb, v_op, s);
+    }
+    if (dtype == LIG_F64) {
+        CotSrc<double> cot{(const double *)v_img, (const double *)v_wsum, nullptr, nullptr, nullptr, 0.0};
+        return raster_bwd<double>(H, W, B, n, ids, bins, d_total, xys, con, col, op, fin, cot,
+                                  v_dx, v_dy, v_dxy, clamp, ws, ws_bytes, v_xy, v_abs, v_con,
+                                  v_rgb, v_op, s);
+    }
+    return LIG_ERR_INVALID;
+}
+
+extern "C" int lig_raster_bwd_l2(int dtype, int H, int W, int B, int n, const int32_t *ids,
+                                 const int32_t *bins, const int32_t *d_total, const void *xys,
+                                 const void *con, const void *col, const void *op,
+                                 const int32_t *fin, const void *img, const void *target,
+                                 const void *grad_loss, double clamp, void *ws, size_t ws_bytes,
+                                 void *v_xy, void *v_abs, void *v_con, void *v_rgb, void *v_op,
+                                 void *stream) {
+    if (!raster_args_ok(H, W, B, n) || !bins || !d_total || !fin || !img || !target ||
+        !grad_loss || !ws || (n > 0 && (!xys || !con || !col || !v_xy || !v_abs || !v_con || !v_rgb)))
+        return LIG_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (n == 0) return LIG_OK;
+    const double scale = 2.0 / (3.0 * (double)H * (double)W);
+    if (dtype == LIG_F32) {
+        CotSrc<float> cot{nullptr, nullptr, (const float *)img, (const float *)target,
+                          (const float *)grad_loss, (float)scale};
+        return raster_bwd<float>(H, W, B, n, ids, bins, d_total, xys, con, col, op, fin, cot,
+                                 nullptr, nullptr, nullptr, clamp, ws, ws_bytes, v_xy, v_abs,
                                  v_con, v_rgb, v_op, s);
-    if (dtype == LIG_F64)
-        return raster_bwd<double>(H, W, B, n, ids, bins, d_total, xys, con, col, op, fin, v_img,
-                                  v_wsum, v_dx, v_dy, v_dxy, clamp, ws, ws_bytes, v_xy, v_abs,
+    }
+    if (dtype == LIG_F64) {
+        CotSrc<double> cot{nullptr, nullptr, (const double *)img, (const double *)target,
+                           (const double *)grad_loss, scale};
+        return raster_bwd<double>(H, W, B, n, ids, bins, d_total, xys, con, col, op, fin, cot,
+                                  nullptr, nullptr, nullptr, clamp, ws, ws_bytes, v_xy, v_abs,
                                   v_con, v_rgb, v_op, s);
+    }
     return LIG_ERR_INVALID;
 }
 

@@ -18,6 +18,7 @@ import torch
 import torch.nn.functional as F
 
 from . import synthetic
+from .fused import render_l2_loss
 from .gsplat2d import gradient_aware_upscale, project_gaussians_cholesky, rasterize_gaussians
 
 
@@ -25,8 +26,10 @@ class LevelFit:
     """One LIG level: N Gaussians fitted to an [H, W, 3] target."""
 
     def __init__(self, n: int, H: int, W: int, device="cuda", lr: float = 1e-3, block: int = 16,
-                 diag=(0.5, 6.0), seed: int = synthetic.SEED_INIT, fused_adam: bool = True):
+                 diag=(0.5, 6.0), seed: int = synthetic.SEED_INIT, fused_adam: bool = True,
+                 fused_loss: bool = True):
         self.H, self.W, self.block = H, W, block
+        self.fused_loss = fused_loss
         means, chol, colors = synthetic.gaussians(n, H, W, diag=diag, seed=seed)
         self.means = torch.nn.Parameter(means.to(device))
         self.chol = torch.nn.Parameter(chol.to(device))
@@ -47,9 +50,14 @@ class LevelFit:
 
     def step(self, target_hwc: torch.Tensor) -> torch.Tensor:
         """One iteration: render, clamp, L2, backward, Adam.  Returns the loss
-        as a device tensor (no host synchronisation)."""
-        img = torch.clamp(self.render()[0], 0, 1)
-        loss = F.mse_loss(img, target_hwc)
+        as a device tensor (no host synchronisation).  fused_loss=True runs the
+        same math through the fused render+L2 node (lig_b200.fused)."""
+        if self.fused_loss:
+            loss = render_l2_loss(self.chol, self.means, self.rgbs, None, target_hwc, self.H,
+                                  self.W, self.block)
+        else:
+            img = torch.clamp(self.render()[0], 0, 1)
+            loss = F.mse_loss(img, target_hwc)
         self.opt.zero_grad(set_to_none=True)
         loss.backward()
         self.opt.step()

@@ -82,6 +82,7 @@ class _RasterizeGaussians(Function):
         out_img, out_wsum, out_dx, out_dy, out_dxy, final_idx = outs
         if not compute_upscale_gradients:
             out_dx = out_dy = out_dxy = None
+        ctx.set_materialize_grads(False)  # unused outputs (e.g. wsum) get no zero tensor
         ctx.img_width = img_width
         ctx.img_height = img_height
         ctx.num_intersects = binning.num_intersects
@@ -99,8 +100,7 @@ class _RasterizeGaussians(Function):
         h, w = ctx.img_height, ctx.img_width
         if v_out_img is None:
             v_out_img = torch.zeros((h, w, 3), dtype=xys.dtype, device=xys.device)
-        if v_out_wsum is None:
-            v_out_wsum = torch.zeros((h, w), dtype=xys.dtype, device=xys.device)
+        # v_out_wsum None: the wsum output was unused; the kernel treats it as zero
         ga = ctx.compute_upscale_gradients
         if ga:
             z = None

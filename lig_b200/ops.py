@@ -353,7 +353,7 @@ def raster_fwd(img_h, img_w, block, gaussian_ids_sorted, tile_bins, total, xys, 
 def raster_bwd(img_h, img_w, block, gaussian_ids_sorted, tile_bins, total, xys, conics, colors,
                opacities, final_idx, v_img, v_wsum, v_dx=None, v_dy=None, v_dxy=None,
                alpha_clamp: float = 0.0):
-    _check_cuda(xys, conics, colors, final_idx, v_img, v_wsum)
+    _check_cuda(xys, conics, colors, final_idx, v_img)
     xys = _c(xys)
     dt = xys.dtype
     conics, colors, opacities = _c(conics, dt), _c(colors, dt), _c(opacities, dt)
@@ -374,6 +374,46 @@ def raster_bwd(img_h, img_w, block, gaussian_ids_sorted, tile_bins, total, xys, 
          float(alpha_clamp), _p(ws), wsb, _p(v_xy), _p(v_abs), _p(v_con), _p(v_rgb), _p(v_op),
          _stream(dev))
     return v_xy, v_abs, v_con, v_rgb, v_op
+
+
+def raster_bwd_l2(img_h, img_w, block, gaussian_ids_sorted, tile_bins, total, xys, conics,
+                  colors, opacities, final_idx, img, target, grad_loss, alpha_clamp: float = 0.0):
+    """Sum backward with the clamped-L2 loss gradient computed in-kernel."""
+    _check_cuda(xys, conics, colors, final_idx, img, target, grad_loss)
+    xys = _c(xys)
+    dt = xys.dtype
+    conics, colors, opacities = _c(conics, dt), _c(colors, dt), _c(opacities, dt)
+    img, target, grad_loss = _c(img, dt), _c(target, dt), _c(grad_loss.reshape(1), dt)
+    n = xys.shape[0]
+    dev = xys.device
+    code = _dt(xys)
+    ws, wsb = _raster_ws(code, n, dev)
+    v_xy = torch.empty((n, 2), dtype=dt, device=dev)
+    v_abs = torch.empty((n, 2), dtype=dt, device=dev)
+    v_con = torch.empty((n, 3), dtype=dt, device=dev)
+    v_rgb = torch.empty((n, 3), dtype=dt, device=dev)
+    v_op = torch.empty((n,), dtype=dt, device=dev) if opacities is not None else None
+    call("lig_raster_bwd_l2", code, int(img_h), int(img_w), int(block), n,
+         _p(gaussian_ids_sorted), _p(tile_bins), _p(total), _p(xys), _p(conics), _p(colors),
+         _p(opacities), _p(_c(final_idx, torch.int32)), _p(img), _p(target), _p(grad_loss),
+         float(alpha_clamp), _p(ws), wsb, _p(v_xy), _p(v_abs), _p(v_con), _p(v_rgb), _p(v_op),
+         _stream(dev))
+    return v_xy, v_abs, v_con, v_rgb, v_op
+
+
+def l2_clamped_loss(img, target):
+    """mean((clamp(img, 0, 1) - target)^2) as a 0-d device tensor."""
+    _check_cuda(img, target)
+    img = _c(img)
+    target = _c(target, img.dtype)
+    if img.numel() != target.numel():
+        raise ValueError("img and target must have the same number of elements")
+    out = torch.empty((), dtype=img.dtype, device=img.device)
+    wsb = _lib.lib.lig_l2_workspace_bytes()
+    ws = torch.empty((wsb,), dtype=torch.uint8, device=img.device)
+    call("lig_l2_clamped_loss", _dt(img), img.numel(), _p(img), _p(target), _p(out), _p(ws), wsb,
+         _stream(img.device))
+    return out
 
 
 # ------------------------------------------------------------------ upscale

@@ -161,3 +161,28 @@ def test_lig_training_step_decreases_loss():
         opt.step()
         losses.append(loss.item())
     assert losses[-1] < 0.7 * losses[0]
+
+
+def test_fused_render_l2_matches_unfused_chain():
+    """lig_b200.fused.render_l2_loss == project + rasterize + clamp + mse_loss,
+    value and gradients (the fused backward forms dL/dimg in-kernel)."""
+    from lig_b200.fused import render_l2_loss
+    H, W, B, n = 150, 170, 16, 3000
+    means, L, colors, _ = scene(n, H, W, diag=(0.5, 5.0), seed=4)
+    g = torch.Generator().manual_seed(9)
+    target = torch.rand(H, W, 3, generator=g).cuda()
+
+    def unfused(p):
+        xys, ext, con, cnt = gsplat2d.project_gaussians_cholesky(p[1], p[0], H, W, B)
+        img = gsplat2d.rasterize_gaussians(xys, ext, con, cnt, p[2], None, H, W, B)[0]
+        return torch.nn.functional.mse_loss(torch.clamp(img, 0, 1), target)
+
+    p1 = [t.clone().requires_grad_() for t in (means, L, colors)]
+    p2 = [t.clone().requires_grad_() for t in (means, L, colors)]
+    l1 = unfused(p1)
+    l1.backward()
+    l2 = render_l2_loss(p2[1], p2[0], p2[2], None, target, H, W, B)
+    l2.backward()
+    assert abs(l1.item() - l2.item()) <= 1e-6 * abs(l1.item())
+    for a, b in zip(p2, p1):
+        assert rel_err(np_(a.grad), np_(b.grad)) <= 1e-5
