@@ -224,6 +224,99 @@ int lig_upscale_bwd(int dtype, int mode, int src_h, int src_w, int dst_h, int ds
                     const void *grad_out, void *grad_render, void *grad_dx, void *grad_dy,
                     void *grad_dxy, void *stream);
 
+/* ---------------------------------------------------------------- batched */
+
+/* A batch of up to LIG_MAX_BATCH images processed by one launch per stage.
+ * Image i has heights[i] x widths[i] pixels and counts[i] Gaussians (host
+ * arrays of n_img int32).  Per-Gaussian arrays are the images' arrays
+ * concatenated in batch order; [H,W,3] buffers likewise (image i starts at
+ * pixel sum_{j<i} H_j W_j); tile lists are flattened image-major, so the
+ * global tile of image i's local tile t is sum_{j<i} tiles_j + t.  Each image
+ * behaves as if rendered alone: its tile keys, sorted ids (as global ids),
+ * tile ranges (shifted), images and final indices are those of the
+ * single-image calls, and its empty-list branch applies per image.  No
+ * reference counterpart: the reference renders one image per call
+ * (gaussianlig.py:88-93 in a per-image loop, train.py:112-158). */
+#define LIG_MAX_BATCH 64
+
+/* Projection of every Gaussian of the batch against its own image. */
+int lig_project_fwd_batch(int dtype, int n_img, const int32_t *heights, const int32_t *widths,
+                          const int32_t *counts, int cholesky, const void *in3,
+                          const void *means2d, const void *opacities, int block_width,
+                          void *xys, void *extents, void *conics, int32_t *num_tiles_hit,
+                          void *stream);
+int lig_project_bwd_batch(int dtype, int n_img, const int32_t *heights, const int32_t *widths,
+                          const int32_t *counts, int cholesky, const void *in3,
+                          const void *means2d, const void *opacities, int block_width,
+                          const void *v_xy, int64_t v_xy_stride, const void *v_conic,
+                          int64_t v_conic_stride, void *v_in3, void *v_mean2d, void *stream);
+
+/* Emission + stable radix sort + tile ranges over the whole batch (one sort);
+ * tile_bins has sum_i tiles_i entries.  Workspace: lig_bin_workspace_bytes
+ * with the batch's total tile count.  cum / num_intersects as lig_bin (the
+ * inclusive prefix sum over the concatenated counts). */
+int lig_bin_batch(int dtype, int n_img, const int32_t *heights, const int32_t *widths,
+                  const int32_t *counts, int block_width, const void *xys, const void *extents,
+                  const int32_t *cum, const int32_t *num_intersects, int capacity,
+                  void *workspace, size_t workspace_bytes, int32_t *gaussian_ids_sorted,
+                  int32_t *tile_bins, int32_t *status, void *stream);
+
+/* Sum / gradient-aware forward over the flattened (image, tile) list.
+ * persistent != 0: one CTA per resident slot pulls work items from *work
+ * (one int32 of device memory, overwritten); else one CTA per tile.  cum:
+ * the inclusive prefix sum of the counts (per-image empty test).
+ * Workspace: lig_raster_workspace_bytes(dtype, total points). */
+int lig_raster_fwd_batch(int dtype, int n_img, const int32_t *heights, const int32_t *widths,
+                         const int32_t *counts, int block_width,
+                         const int32_t *gaussian_ids_sorted, const int32_t *tile_bins,
+                         const int32_t *num_intersects, const int32_t *cum, const void *xys,
+                         const void *conics, const void *colors, const void *opacities,
+                         int persistent, int32_t *work, void *workspace, size_t workspace_bytes,
+                         void *out_img, void *out_wsum, void *out_dx, void *out_dy,
+                         void *out_dxy, int32_t *final_idx, void *stream);
+
+/* Sum backward of loss = sum_i mean((clamp(img_i, 0, 1) - target_i)^2),
+ * the pixel cotangent 2/(3 H_i W_i) (clamp - target) * grad_loss formed in
+ * the kernel (as lig_raster_bwd_l2 per image). */
+int lig_raster_bwd_l2_batch(int dtype, int n_img, const int32_t *heights, const int32_t *widths,
+                            const int32_t *counts, int block_width,
+                            const int32_t *gaussian_ids_sorted, const int32_t *tile_bins,
+                            const int32_t *num_intersects, const int32_t *cum, const void *xys,
+                            const void *conics, const void *colors, const void *opacities,
+                            const int32_t *final_idx, const void *img, const void *target,
+                            const void *grad_loss, double alpha_clamp, int persistent,
+                            int32_t *work, void *workspace, size_t workspace_bytes, void *v_xy,
+                            void *v_xy_abs, void *v_conic, void *v_colors, void *v_opacity,
+                            void *stream);
+
+/* Workspace bytes of lig_l2_clamped_loss_batch. */
+size_t lig_l2_batch_workspace_bytes(int n_img);
+
+/* loss = sum_i mean((clamp(img_i, 0, 1) - target_i)^2) (0-d), per_image[i] =
+ * that image's mean (may be NULL); deterministic; a batch of one gives
+ * lig_l2_clamped_loss's value bit for bit. */
+int lig_l2_clamped_loss_batch(int dtype, int n_img, const int32_t *heights,
+                              const int32_t *widths, const void *img, const void *target,
+                              void *loss, void *per_image, void *workspace,
+                              size_t workspace_bytes, void *stream);
+
+/* -------------------------------------------------------------- optimiser */
+
+/* Scratch bytes of lig_adam_step (device memory, 16 B). */
+size_t lig_adam_scratch_bytes(void);
+
+/* One Adam step over a flat fp32 buffer of n parameters (16-byte aligned
+ * params / grads / moments), for the fit loops' optimiser
+ * (gaussianlig.py:64-68: Adam over every Gaussian parameter).  *step
+ * (device int32) counts applied steps and gives the bias corrections.  If
+ * status (device int32, may be NULL) has LIG_STATUS_OVERFLOW set — the
+ * binning of this step overflowed its capacity — nothing is updated and
+ * *skipped (device int32, may be NULL) is incremented. */
+int lig_adam_step(int64_t n, float *params, const float *grads, float *exp_avg,
+                  float *exp_avg_sq, double lr, double beta1, double beta2, double eps,
+                  const int32_t *status, int32_t *step, int32_t *skipped, void *scratch,
+                  void *stream);
+
 /* ----------------------------------------------------------------- probes */
 
 /* FP32 FMA throughput probe: blocks x 256 threads, each `iters` x 8

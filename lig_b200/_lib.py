@@ -64,7 +64,19 @@ SIGNATURES = {
                               P, P, P]),
     "lig_l2_workspace_bytes": (SZ, []),
     "lig_l2_clamped_loss": (I, [I, I64, P, P, P, P, SZ, P]),
+    "lig_project_fwd_batch": (I, [I, I, P, P, P, I, P, P, P, I, P, P, P, P, P]),
+    "lig_project_bwd_batch": (I, [I, I, P, P, P, I, P, P, P, I, P, I64, P, I64, P, P, P]),
+    "lig_bin_batch": (I, [I, I, P, P, P, I, P, P, P, P, I, P, SZ, P, P, P, P]),
+    "lig_raster_fwd_batch": (I, [I, I, P, P, P, I, P, P, P, P, P, P, P, P, I, P, P, SZ, P, P, P,
+                                 P, P, P, P]),
+    "lig_raster_bwd_l2_batch": (I, [I, I, P, P, P, I, P, P, P, P, P, P, P, P, P, P, P, P, D, I,
+                                    P, P, SZ, P, P, P, P, P, P]),
+    "lig_l2_batch_workspace_bytes": (SZ, [I]),
+    "lig_l2_clamped_loss_batch": (I, [I, I, P, P, P, P, P, P, P, SZ, P]),
+    "lig_adam_scratch_bytes": (SZ, []),
+    "lig_adam_step": (I, [I64, P, P, P, P, D, D, D, D, P, P, P, P, P]),
 }
+LIG_MAX_BATCH = 64
 
 
 class LigError(RuntimeError):

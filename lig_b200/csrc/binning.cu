@@ -13,6 +13,8 @@
 // stable LSD radix sort over exactly those bits with <= 10-bit digits, so the
 // order inside a tile is emission order (ascending Gaussian id), which is the
 // order of the reference's stable torch.sort.
+#include <atomic>
+
 #include "common.cuh"
 
 namespace lig {
@@ -139,8 +141,8 @@ inline int device_scan(const uint32_t *in, uint32_t *out, int n, bool inclusive,
 // values the reference leaves in its zero-initialised buffers.
 template <typename T>
 __global__ void emit_kernel(int n, const T *__restrict__ xys, const T *__restrict__ extents,
-                            const int32_t *__restrict__ cum, unsigned tbx, unsigned tby,
-                            unsigned block, int capacity, uint32_t *__restrict__ keys,
+                            const int32_t *__restrict__ cum, BatchGeo geo, int capacity,
+                            uint32_t *__restrict__ keys,
                             int32_t *__restrict__ vals, int64_t *__restrict__ keys64,
                             int32_t *__restrict__ vals_extra, int32_t *__restrict__ status) {
     const unsigned FULL = 0xffffffffu;
@@ -150,8 +152,13 @@ __global__ void emit_kernel(int n, const T *__restrict__ xys, const T *__restric
     if (g0 >= n) return;
     int g = (int)(g0 + lane);
     int cnt = 0, start = 0, x0 = 0, y0 = 0, bw = 1, bh = 0;
+    unsigned tbx = 1, toff = 0, g_first = 0;
     bool valid = false;
     if (g < n) {
+        const int im = geo.image_of_gauss(g);
+        tbx = geo.tbx[im];
+        toff = (unsigned)geo.tile_off[im];
+        g_first = (unsigned)geo.g_off[im];
         int prev = g > 0 ? cum[g - 1] : 0;
         start = prev;
         cnt = cum[g] - prev;
@@ -159,7 +166,7 @@ __global__ void emit_kernel(int n, const T *__restrict__ xys, const T *__restric
         valid = !(ex <= (T)0 || ey <= (T)0);
         if (valid && cnt > 0) {
             int x1, y1;
-            tile_bbox(xys[2 * g], xys[2 * g + 1], ex, ey, tbx, tby, block, x0, y0, x1, y1);
+            tile_bbox(xys[2 * g], xys[2 * g + 1], ex, ey, tbx, geo.tby(im), geo.B, x0, y0, x1, y1);
             bw = x1 - x0;
             bh = y1 - y0;
             if (bw <= 0 || bw * bh != cnt) {
@@ -197,6 +204,9 @@ __global__ void emit_kernel(int n, const T *__restrict__ xys, const T *__restric
         int o_y0 = __shfl_sync(FULL, y0, owner);
         int o_bw = __shfl_sync(FULL, bw, owner);
         int o_valid = __shfl_sync(FULL, (int)valid, owner);
+        unsigned o_tbx = __shfl_sync(FULL, tbx, owner);
+        unsigned o_toff = __shfl_sync(FULL, toff, owner);
+        unsigned o_first = __shfl_sync(FULL, g_first, owner);
         if (s >= total) continue;
         int j = s - (o_incl - o_cnt);
         int slot = o_start + j;
@@ -204,12 +214,14 @@ __global__ void emit_kernel(int n, const T *__restrict__ xys, const T *__restric
             overflow = true;
             continue;
         }
-        uint32_t key = 0;
-        int32_t gid = 0;
+        // phantom slots: the image's first tile and first Gaussian (0 / 0 for
+        // a single image)
+        uint32_t key = o_toff;
+        int32_t gid = (int32_t)o_first;
         if (o_valid) {
             int q = j / o_bw;
             int r = j - q * o_bw;
-            key = (uint32_t)(o_y0 + q) * tbx + (uint32_t)(o_x0 + r);
+            key = o_toff + (uint32_t)(o_y0 + q) * o_tbx + (uint32_t)(o_x0 + r);
             gid = (int32_t)(g0 + owner);
         }
         if (keys) keys[slot] = key;
@@ -437,12 +449,12 @@ inline BinPlan make_plan(int capacity, int num_tiles) {
 }
 
 template <typename T>
-int run_bin(int n, const void *xys, const void *ext, const int32_t *cum, const int32_t *d_total,
-            int h, int w, int b, int capacity, void *ws, size_t ws_bytes, int32_t *gid_sorted,
+int run_bin(const BatchGeo &geo, const void *xys, const void *ext, const int32_t *cum,
+            const int32_t *d_total, int capacity, void *ws, size_t ws_bytes, int32_t *gid_sorted,
             int32_t *tile_bins, int64_t *isect, int32_t *gids, int64_t *isect_sorted,
             int32_t *status, cudaStream_t s) {
-    unsigned tbx = (w + b - 1) / b, tby = (h + b - 1) / b;
-    int T_ = (int)(tbx * tby);
+    const int n = geo.total_points();
+    const int T_ = geo.total_tiles();
     BinPlan p = make_plan(capacity, T_);
     if (ws_bytes < p.total) return LIG_ERR_WORKSPACE;
     char *base = (char *)ws;
@@ -468,16 +480,25 @@ int run_bin(int n, const void *xys, const void *ext, const int32_t *cum, const i
 
     int warps = (n + 31) / 32;
     int eblocks = (warps * 32 + 255) / 256;
-    emit_kernel<T><<<eblocks, 256, 0, s>>>(n, (const T *)xys, (const T *)ext, cum, tbx, tby, b,
-                                           capacity, ka, va, isect, gids, status);
+    emit_kernel<T><<<eblocks, 256, 0, s>>>(n, (const T *)xys, (const T *)ext, cum, geo, capacity,
+                                           ka, va, isect, gids, status);
     flag_overflow_kernel<<<1, 1, 0, s>>>(d_total, capacity, status);
     note_launches(2);
     LIG_LAUNCH_CHECK();
 
     size_t dsm = downsweep_smem(p.bins);
-    if (dsm > 48 * 1024)
-        cudaFuncSetAttribute(radix_downsweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)dsm);
+    if (dsm > 48 * 1024) {
+        // set once per device (and never during stream capture)
+        static std::atomic<uint64_t> opted{0};
+        int dev = 0;
+        cudaGetDevice(&dev);
+        const uint64_t bit = 1ull << (dev & 63);
+        if (!(opted.load() & bit)) {
+            cudaFuncSetAttribute(radix_downsweep_kernel,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
+            opted.fetch_or(bit);
+        }
+    }
     int hist_n = p.bins * p.nblk;
     for (int pass = 0; pass < p.passes; ++pass) {
         int shift = pass * p.dbits;
@@ -539,12 +560,36 @@ extern "C" int lig_bin(int dtype, int n, const void *xys, const void *ext, const
         (n > 0 && (!xys || !ext || !cum)) || (capacity > 0 && (!gid_sorted || !ws)))
         return LIG_ERR_INVALID;
     cudaStream_t s = (cudaStream_t)stream;
+    const BatchGeo geo = BatchGeo::single(h, w, b, n);
     if (dtype == LIG_F32)
-        return run_bin<float>(n, xys, ext, cum, d_total, h, w, b, capacity, ws, ws_bytes,
-                              gid_sorted, tile_bins, isect, gids, isect_sorted, status, s);
+        return run_bin<float>(geo, xys, ext, cum, d_total, capacity, ws, ws_bytes, gid_sorted,
+                              tile_bins, isect, gids, isect_sorted, status, s);
     if (dtype == LIG_F64)
-        return run_bin<double>(n, xys, ext, cum, d_total, h, w, b, capacity, ws, ws_bytes,
-                               gid_sorted, tile_bins, isect, gids, isect_sorted, status, s);
+        return run_bin<double>(geo, xys, ext, cum, d_total, capacity, ws, ws_bytes, gid_sorted,
+                               tile_bins, isect, gids, isect_sorted, status, s);
+    return LIG_ERR_INVALID;
+}
+
+extern "C" int lig_bin_batch(int dtype, int n_img, const int32_t *heights, const int32_t *widths,
+                             const int32_t *counts_per_image, int b, const void *xys,
+                             const void *ext, const int32_t *cum, const int32_t *d_total,
+                             int capacity, void *ws, size_t ws_bytes, int32_t *gid_sorted,
+                             int32_t *tile_bins, int32_t *status, void *stream) {
+    BatchGeo geo;
+    if (!heights || !widths || !counts_per_image ||
+        !BatchGeo::make(n_img, heights, widths, counts_per_image, b, geo))
+        return LIG_ERR_INVALID;
+    const int n = geo.total_points();
+    if (capacity < 0 || !d_total || !tile_bins || !status || (n > 0 && (!xys || !ext || !cum)) ||
+        (capacity > 0 && (!gid_sorted || !ws)))
+        return LIG_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (dtype == LIG_F32)
+        return run_bin<float>(geo, xys, ext, cum, d_total, capacity, ws, ws_bytes, gid_sorted,
+                              tile_bins, nullptr, nullptr, nullptr, status, s);
+    if (dtype == LIG_F64)
+        return run_bin<double>(geo, xys, ext, cum, d_total, capacity, ws, ws_bytes, gid_sorted,
+                               tile_bins, nullptr, nullptr, nullptr, status, s);
     return LIG_ERR_INVALID;
 }
 
@@ -561,14 +606,14 @@ extern "C" int lig_map_intersects(int dtype, int n, int m, const void *xys, cons
     cudaMemsetAsync(gids, 0, sizeof(int32_t) * (size_t)m, s);
     int warps = (n + 31) / 32;
     int eblocks = (warps * 32 + 255) / 256;
+    const BatchGeo geo = BatchGeo::single(tby * b, tbx * b, b, n);
     if (dtype == LIG_F32)
         emit_kernel<float><<<eblocks, 256, 0, s>>>(n, (const float *)xys, (const float *)ext, cum,
-                                                   tbx, tby, b, m, nullptr, gids, isect, nullptr,
-                                                   nullptr);
+                                                   geo, m, nullptr, gids, isect, nullptr, nullptr);
     else if (dtype == LIG_F64)
         emit_kernel<double><<<eblocks, 256, 0, s>>>(n, (const double *)xys, (const double *)ext,
-                                                    cum, tbx, tby, b, m, nullptr, gids, isect,
-                                                    nullptr, nullptr);
+                                                    cum, geo, m, nullptr, gids, isect, nullptr,
+                                                    nullptr);
     else
         return LIG_ERR_INVALID;
     note_launches(1);

@@ -81,6 +81,73 @@ __device__ __forceinline__ bool cov2d_bounds(T cx, T cy, T cz, T opacity, T &ca,
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31; }
 
+// Geometry of a batch of images rasterised in one launch, passed by value as a
+// kernel parameter (constant bank; ~1.6 KB).  Image i owns Gaussians
+// [g_off[i], g_off[i+1]), tiles [tile_off[i], tile_off[i+1]) of the flattened
+// tile list and pixels [pix_off[i], pix_off[i+1]) of the concatenated HWC
+// buffers.  A single image is the batch {n_img = 1}.
+constexpr int kMaxBatch = LIG_MAX_BATCH;
+struct BatchGeo {
+    int n_img, B;
+    int tile_off[kMaxBatch + 1], g_off[kMaxBatch + 1], pix_off[kMaxBatch + 1];
+    int H[kMaxBatch], W[kMaxBatch], tbx[kMaxBatch];
+
+    // index i with off[i] <= x < off[i+1] (off non-decreasing, x < off[n])
+    __host__ __device__ __forceinline__ static int find(const int *off, int n, int x) {
+        int lo = 0, hi = n - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (off[mid] <= x) lo = mid; else hi = mid - 1;
+        }
+        return lo;
+    }
+    __host__ __device__ __forceinline__ int image_of_tile(int t) const {
+        return n_img == 1 ? 0 : find(tile_off, n_img, t);
+    }
+    __host__ __device__ __forceinline__ int image_of_gauss(int g) const {
+        return n_img == 1 ? 0 : find(g_off, n_img, g);
+    }
+    __host__ __device__ __forceinline__ int image_of_pixel(int p) const {
+        return n_img == 1 ? 0 : find(pix_off, n_img, p);
+    }
+    __host__ __device__ __forceinline__ int tby(int i) const { return (H[i] + B - 1) / B; }
+    __host__ __device__ int total_tiles() const { return tile_off[n_img]; }
+    __host__ __device__ int total_pixels() const { return pix_off[n_img]; }
+    __host__ __device__ int total_points() const { return g_off[n_img]; }
+
+    // host-side construction; false on bad sizes
+    static bool make(int n_img, const int32_t *h, const int32_t *w, const int32_t *n_pts, int B,
+                     BatchGeo &g) {
+        if (n_img < 1 || n_img > kMaxBatch || B < 1) return false;
+        g.n_img = n_img;
+        g.B = B;
+        long long t = 0, gp = 0, px = 0;
+        g.tile_off[0] = g.g_off[0] = g.pix_off[0] = 0;
+        for (int i = 0; i < n_img; ++i) {
+            if (h[i] <= 0 || w[i] <= 0 || n_pts[i] < 0) return false;
+            g.H[i] = h[i];
+            g.W[i] = w[i];
+            g.tbx[i] = (w[i] + B - 1) / B;
+            t += (long long)g.tbx[i] * ((h[i] + B - 1) / B);
+            gp += n_pts[i];
+            px += (long long)h[i] * w[i];
+            // batched pixel offsets index HWC buffers with 32-bit ints
+            if (t > 0x7fffffffLL || gp > 0x7fffffffLL || (n_img > 1 && 3 * px > 0x7fffffffLL))
+                return false;
+            g.tile_off[i + 1] = (int)t;
+            g.g_off[i + 1] = (int)gp;
+            g.pix_off[i + 1] = (int)(px < 0x7fffffffLL ? px : 0x7fffffffLL);
+        }
+        return true;
+    }
+    static BatchGeo single(int H, int W, int B, int n) {
+        BatchGeo g;
+        int32_t h = H, w = W, np = n;
+        make(1, &h, &w, &np, B, g);
+        return g;
+    }
+};
+
 // Process-wide count of kernel launches issued by this library.
 void note_launches(int n);
 

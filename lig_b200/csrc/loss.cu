@@ -43,6 +43,84 @@ __global__ void l2_final_kernel(int nblocks, int64_t n, const double *__restrict
 
 inline int loss_blocks() { return 148 * 8; }
 
+// Batched: loss = sum over images of mean_i((clamp(img_i) - target_i)^2).
+// Image i gets its own run of blocks (about its share of loss_blocks(), at
+// least one), each striding over that image's values only, so a block's
+// partial belongs to one image and the reduction stays deterministic.  For a
+// batch of one this is exactly the single-image reduction above.
+struct LossSplit {
+    int n_img;
+    int blk_off[kMaxBatch + 1];
+    long long elem_off[kMaxBatch + 1];
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kLossThreads)
+l2_partial_batch_kernel(const LossSplit sp, const T *__restrict__ img,
+                        const T *__restrict__ target, double *__restrict__ partials) {
+    __shared__ double s_warp[kLossThreads / 32];
+    const int b = blockIdx.x;
+    int lo = 0, hi = sp.n_img - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (sp.blk_off[mid] <= b) lo = mid; else hi = mid - 1;
+    }
+    const int im = lo;
+    const int lb = b - sp.blk_off[im], nb = sp.blk_off[im + 1] - sp.blk_off[im];
+    const int64_t e0 = sp.elem_off[im], n = sp.elem_off[im + 1] - e0;
+    double acc = 0;
+    for (int64_t i = (int64_t)lb * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)nb * blockDim.x) {
+        const T x = img[e0 + i];
+        const T d = min(max(x, (T)0), (T)1) - target[e0 + i];
+        acc += (double)(d * d);
+    }
+    for (int o = 16; o >= 1; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) s_warp[w] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int k = 0; k < kLossThreads / 32; ++k) t += s_warp[k];
+        partials[b] = t;
+    }
+}
+
+template <typename T>
+__global__ void l2_final_batch_kernel(const LossSplit sp, const double *__restrict__ partials,
+                                      T *__restrict__ out, T *__restrict__ per_image) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double total = 0;
+    for (int im = 0; im < sp.n_img; ++im) {
+        double t = 0;
+        for (int k = sp.blk_off[im]; k < sp.blk_off[im + 1]; ++k) t += partials[k];
+        const double m = t / (double)(sp.elem_off[im + 1] - sp.elem_off[im]);
+        if (per_image) per_image[im] = (T)m;
+        total += m;
+    }
+    *out = (T)total;
+}
+
+inline bool make_split(int n_img, const int32_t *h, const int32_t *w, LossSplit &sp) {
+    if (n_img < 1 || n_img > kMaxBatch || !h || !w) return false;
+    long long tot = 0;
+    for (int i = 0; i < n_img; ++i) {
+        if (h[i] <= 0 || w[i] <= 0) return false;
+        tot += 3ll * h[i] * w[i];
+    }
+    sp.n_img = n_img;
+    sp.blk_off[0] = 0;
+    sp.elem_off[0] = 0;
+    for (int i = 0; i < n_img; ++i) {
+        const long long e = 3ll * h[i] * w[i];
+        long long nb = n_img == 1 ? loss_blocks() : (long long)loss_blocks() * e / tot;
+        if (nb < 1) nb = 1;
+        sp.blk_off[i + 1] = sp.blk_off[i] + (int)nb;
+        sp.elem_off[i + 1] = sp.elem_off[i] + e;
+    }
+    return true;
+}
+
 }  // namespace lig
 
 using namespace lig;
@@ -64,6 +142,38 @@ extern "C" int lig_l2_clamped_loss(int dtype, int64_t n, const void *img, const 
         l2_partial_kernel<double><<<nb, kLossThreads, 0, s>>>(n, (const double *)img,
                                                               (const double *)target, part);
         l2_final_kernel<double><<<1, 32, 0, s>>>(nb, n, part, (double *)loss);
+    } else {
+        return LIG_ERR_INVALID;
+    }
+    note_launches(2);
+    LIG_LAUNCH_CHECK();
+    return LIG_OK;
+}
+
+extern "C" size_t lig_l2_batch_workspace_bytes(int n_img) {
+    return sizeof(double) * (size_t)(loss_blocks() + (n_img > 0 ? n_img : 0));
+}
+
+extern "C" int lig_l2_clamped_loss_batch(int dtype, int n_img, const int32_t *heights,
+                                         const int32_t *widths, const void *img,
+                                         const void *target, void *loss, void *per_image,
+                                         void *ws, size_t ws_bytes, void *stream) {
+    LossSplit sp;
+    if (!make_split(n_img, heights, widths, sp) || !img || !target || !loss || !ws)
+        return LIG_ERR_INVALID;
+    if (ws_bytes < sizeof(double) * (size_t)sp.blk_off[n_img]) return LIG_ERR_WORKSPACE;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int nb = sp.blk_off[n_img];
+    double *part = (double *)ws;
+    if (dtype == LIG_F32) {
+        l2_partial_batch_kernel<float><<<nb, kLossThreads, 0, s>>>(sp, (const float *)img,
+                                                                   (const float *)target, part);
+        l2_final_batch_kernel<float><<<1, 32, 0, s>>>(sp, part, (float *)loss, (float *)per_image);
+    } else if (dtype == LIG_F64) {
+        l2_partial_batch_kernel<double><<<nb, kLossThreads, 0, s>>>(sp, (const double *)img,
+                                                                    (const double *)target, part);
+        l2_final_batch_kernel<double><<<1, 32, 0, s>>>(sp, part, (double *)loss,
+                                                       (double *)per_image);
     } else {
         return LIG_ERR_INVALID;
     }

@@ -1,0 +1,113 @@
+// Fused Adam over one flat parameter buffer, guarded by the binning status.
+//
+// The fit loops keep every Gaussian parameter of a level (or of a batch of
+// levels) in one flat fp32 buffer — means [N,2] | cholesky [N,3] | rgb [N,3] —
+// with the gradient buffer laid out the same way, so one elementwise kernel
+// updates them all (the optimiser of gaussianlig.py:64-68, Adam on every
+// parameter, here without per-tensor launches).
+//
+// Guard: when the binning of this step overflowed its intersection capacity
+// (status word has LIG_STATUS_OVERFLOW), the gradients are those of truncated
+// tile lists.  The prologue then marks the step skipped — no moment update,
+// no step increment, parameters untouched — and counts it, so a caller that
+// captured the step in a CUDA graph with a fixed capacity can grow the
+// capacity and redo exactly the skipped steps.
+//
+// Update rule: Adam (Kingma & Ba, "Adam: A Method for Stochastic
+// Optimization", Algorithm 1) with the bias corrections folded as
+// p -= (lr / (1 - b1^t)) * m / (sqrt(v) / sqrt(1 - b2^t) + eps).
+#include "common.cuh"
+
+namespace lig {
+
+struct AdamScalars {
+    float step_size;     // lr / (1 - b1^t)
+    float bc2_sqrt;      // sqrt(1 - b2^t)
+    int skip;            // 1: leave everything unchanged
+    int pad;
+};
+
+__global__ void adam_prologue_kernel(const int32_t *__restrict__ status, int32_t *step,
+                                     int32_t *skipped, double lr, double b1, double b2,
+                                     AdamScalars *out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    AdamScalars a{0.f, 1.f, 0, 0};
+    if (status && (*status & LIG_STATUS_OVERFLOW)) {
+        a.skip = 1;
+        if (skipped) *skipped += 1;
+    } else {
+        const int t = *step + 1;
+        *step = t;
+        a.step_size = (float)(lr / (1.0 - pow(b1, (double)t)));
+        a.bc2_sqrt = (float)sqrt(1.0 - pow(b2, (double)t));
+    }
+    *out = a;
+}
+
+__global__ void __launch_bounds__(256)
+adam_kernel(int64_t n, float *__restrict__ p, const float *__restrict__ g,
+            float *__restrict__ m, float *__restrict__ v, float b1, float b2, float eps,
+            const AdamScalars *__restrict__ sc) {
+    const AdamScalars a = *sc;
+    if (a.skip) return;
+    const int64_t n4 = n / 4;
+    float4 *p4 = reinterpret_cast<float4 *>(p);
+    const float4 *g4 = reinterpret_cast<const float4 *>(g);
+    float4 *m4 = reinterpret_cast<float4 *>(m);
+    float4 *v4 = reinterpret_cast<float4 *>(v);
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) {
+        float4 pp = p4[i], gg = g4[i], mm = m4[i], vv = v4[i];
+        float *pe = &pp.x, *ge = &gg.x, *me = &mm.x, *ve = &vv.x;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            me[k] = b1 * me[k] + (1.f - b1) * ge[k];
+            ve[k] = b2 * ve[k] + (1.f - b2) * ge[k] * ge[k];
+            pe[k] -= a.step_size * me[k] / (sqrtf(ve[k]) / a.bc2_sqrt + eps);
+        }
+        p4[i] = pp; m4[i] = mm; v4[i] = vv;
+    }
+    for (int64_t i = n4 * 4 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += stride) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        p[i] -= a.step_size * mi / (sqrtf(vi) / a.bc2_sqrt + eps);
+    }
+}
+
+}  // namespace lig
+
+using namespace lig;
+
+extern "C" size_t lig_adam_scratch_bytes(void) { return sizeof(AdamScalars); }
+
+extern "C" int lig_adam_step(int64_t n, float *params, const float *grads, float *exp_avg,
+                             float *exp_avg_sq, double lr, double beta1, double beta2,
+                             double eps, const int32_t *status, int32_t *step, int32_t *skipped,
+                             void *scratch, void *stream) {
+    if (n < 0 || !step || !scratch || (n > 0 && (!params || !grads || !exp_avg || !exp_avg_sq)))
+        return LIG_ERR_INVALID;
+    // float4 path needs 16-byte aligned buffers
+    const uintptr_t al = (uintptr_t)params | (uintptr_t)grads | (uintptr_t)exp_avg |
+                         (uintptr_t)exp_avg_sq;
+    if (al & 15) return LIG_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    AdamScalars *sc = (AdamScalars *)scratch;
+    adam_prologue_kernel<<<1, 32, 0, s>>>(status, step, skipped, lr, beta1, beta2, sc);
+    int launches = 1;
+    if (n > 0) {
+        int64_t blocks = (n / 4 + 255) / 256;
+        const int64_t cap = 148 * 16;
+        if (blocks > cap) blocks = cap;
+        if (blocks < 1) blocks = 1;
+        adam_kernel<<<(int)blocks, 256, 0, s>>>(n, params, grads, exp_avg, exp_avg_sq,
+                                               (float)beta1, (float)beta2, (float)eps, sc);
+        ++launches;
+    }
+    note_launches(launches);
+    LIG_LAUNCH_CHECK();
+    return LIG_OK;
+}

@@ -33,11 +33,12 @@ __device__ __forceinline__ void input_cov(bool chol, const T *in3, int i, T &cx,
 template <typename T>
 __global__ void project_fwd_kernel(int n, bool chol, const T *__restrict__ in3,
                                    const T *__restrict__ means, const T *__restrict__ opac,
-                                   unsigned tbx, unsigned tby, unsigned block,
-                                   T *__restrict__ xys, T *__restrict__ extents,
+                                   BatchGeo geo, T *__restrict__ xys, T *__restrict__ extents,
                                    T *__restrict__ conics, int32_t *__restrict__ counts) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const int im = geo.image_of_gauss(i);
+    const unsigned tbx = geo.tbx[im], tby = geo.tby(im), block = geo.B;
     T cx, cy, cz;
     input_cov(chol, in3, i, cx, cy, cz);
     T o = opac ? opac[i] : (T)1;
@@ -106,12 +107,13 @@ __device__ __forceinline__ void chol_chain(T l11, T l21, T l22, T va, T vb, T vc
 template <typename T>
 __global__ void project_bwd_kernel(int n, bool chol, const T *__restrict__ in3,
                                    const T *__restrict__ means, const T *__restrict__ opac,
-                                   unsigned tbx, unsigned tby, unsigned block,
-                                   const T *__restrict__ v_xy, int64_t sxy,
+                                   BatchGeo geo, const T *__restrict__ v_xy, int64_t sxy,
                                    const T *__restrict__ v_conic, int64_t sco,
                                    T *__restrict__ v_in3, T *__restrict__ v_mean) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const int im = geo.image_of_gauss(i);
+    const unsigned tbx = geo.tbx[im], tby = geo.tby(im), block = geo.B;
     T cx, cy, cz;
     input_cov(chol, in3, i, cx, cy, cz);
     T o = opac ? opac[i] : (T)1;
@@ -198,12 +200,12 @@ inline bool valid_geometry(int n, int h, int w, int b) {
 }
 
 template <typename T>
-int project_fwd(int n, int chol, const void *in3, const void *means, const void *opac, int h,
-                int w, int b, void *xys, void *ext, void *con, int32_t *cnt, cudaStream_t s) {
+int project_fwd(int n, int chol, const void *in3, const void *means, const void *opac,
+                const BatchGeo &geo, void *xys, void *ext, void *con, int32_t *cnt,
+                cudaStream_t s) {
     if (n == 0) return LIG_OK;
-    unsigned tbx = (w + b - 1) / b, tby = (h + b - 1) / b;
     project_fwd_kernel<T><<<proj_blocks(n), kProjThreads, 0, s>>>(
-        n, chol != 0, (const T *)in3, (const T *)means, (const T *)opac, tbx, tby, b, (T *)xys,
+        n, chol != 0, (const T *)in3, (const T *)means, (const T *)opac, geo, (T *)xys,
         (T *)ext, (T *)con, cnt);
     note_launches(1);
     LIG_LAUNCH_CHECK();
@@ -211,14 +213,13 @@ int project_fwd(int n, int chol, const void *in3, const void *means, const void 
 }
 
 template <typename T>
-int project_bwd(int n, int chol, const void *in3, const void *means, const void *opac, int h,
-                int w, int b, const void *v_xy, int64_t sxy, const void *v_con, int64_t sco,
-                void *v_in3, void *v_mean, cudaStream_t s) {
+int project_bwd(int n, int chol, const void *in3, const void *means, const void *opac,
+                const BatchGeo &geo, const void *v_xy, int64_t sxy, const void *v_con,
+                int64_t sco, void *v_in3, void *v_mean, cudaStream_t s) {
     if (n == 0) return LIG_OK;
-    unsigned tbx = (w + b - 1) / b, tby = (h + b - 1) / b;
     project_bwd_kernel<T><<<proj_blocks(n), kProjThreads, 0, s>>>(
-        n, chol != 0, (const T *)in3, (const T *)means, (const T *)opac, tbx, tby, b,
-        (const T *)v_xy, sxy, (const T *)v_con, sco, (T *)v_in3, (T *)v_mean);
+        n, chol != 0, (const T *)in3, (const T *)means, (const T *)opac, geo, (const T *)v_xy,
+        sxy, (const T *)v_con, sco, (T *)v_in3, (T *)v_mean);
     note_launches(1);
     LIG_LAUNCH_CHECK();
     return LIG_OK;
@@ -243,8 +244,9 @@ extern "C" int lig_project_fwd(int dtype, int n, int chol, const void *in3, cons
     if (!valid_geometry(n, h, w, b) || (n > 0 && (!in3 || !means || !xys || !ext || !con || !cnt)))
         return LIG_ERR_INVALID;
     cudaStream_t s = (cudaStream_t)stream;
-    if (dtype == LIG_F32) return project_fwd<float>(n, chol, in3, means, opac, h, w, b, xys, ext, con, cnt, s);
-    if (dtype == LIG_F64) return project_fwd<double>(n, chol, in3, means, opac, h, w, b, xys, ext, con, cnt, s);
+    const BatchGeo geo = BatchGeo::single(h, w, b, n);
+    if (dtype == LIG_F32) return project_fwd<float>(n, chol, in3, means, opac, geo, xys, ext, con, cnt, s);
+    if (dtype == LIG_F64) return project_fwd<double>(n, chol, in3, means, opac, geo, xys, ext, con, cnt, s);
     return LIG_ERR_INVALID;
 }
 
@@ -256,10 +258,11 @@ extern "C" int lig_project_bwd(int dtype, int n, int chol, const void *in3, cons
         (n > 0 && (!in3 || !means || !v_xy || !v_con || !v_in3 || !v_mean)))
         return LIG_ERR_INVALID;
     cudaStream_t s = (cudaStream_t)stream;
+    const BatchGeo geo = BatchGeo::single(h, w, b, n);
     if (dtype == LIG_F32)
-        return project_bwd<float>(n, chol, in3, means, opac, h, w, b, v_xy, sxy, v_con, sco, v_in3, v_mean, s);
+        return project_bwd<float>(n, chol, in3, means, opac, geo, v_xy, sxy, v_con, sco, v_in3, v_mean, s);
     if (dtype == LIG_F64)
-        return project_bwd<double>(n, chol, in3, means, opac, h, w, b, v_xy, sxy, v_con, sco, v_in3, v_mean, s);
+        return project_bwd<double>(n, chol, in3, means, opac, geo, v_xy, sxy, v_con, sco, v_in3, v_mean, s);
     return LIG_ERR_INVALID;
 }
 
@@ -303,4 +306,41 @@ extern "C" int lig_cov2d_bounds(int dtype, int n, const void *cov, const void *o
     note_launches(1);
     LIG_LAUNCH_CHECK();
     return LIG_OK;
+}
+
+extern "C" int lig_project_fwd_batch(int dtype, int n_img, const int32_t *heights,
+                                     const int32_t *widths, const int32_t *counts_per_image,
+                                     int chol, const void *in3, const void *means,
+                                     const void *opac, int b, void *xys, void *ext, void *con,
+                                     int32_t *cnt, void *stream) {
+    BatchGeo geo;
+    if (!heights || !widths || !counts_per_image ||
+        !BatchGeo::make(n_img, heights, widths, counts_per_image, b, geo))
+        return LIG_ERR_INVALID;
+    const int n = geo.total_points();
+    if (n > 0 && (!in3 || !means || !xys || !ext || !con || !cnt)) return LIG_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (dtype == LIG_F32) return project_fwd<float>(n, chol, in3, means, opac, geo, xys, ext, con, cnt, s);
+    if (dtype == LIG_F64) return project_fwd<double>(n, chol, in3, means, opac, geo, xys, ext, con, cnt, s);
+    return LIG_ERR_INVALID;
+}
+
+extern "C" int lig_project_bwd_batch(int dtype, int n_img, const int32_t *heights,
+                                     const int32_t *widths, const int32_t *counts_per_image,
+                                     int chol, const void *in3, const void *means,
+                                     const void *opac, int b, const void *v_xy, int64_t sxy,
+                                     const void *v_con, int64_t sco, void *v_in3, void *v_mean,
+                                     void *stream) {
+    BatchGeo geo;
+    if (!heights || !widths || !counts_per_image || sxy < 2 || sco < 3 ||
+        !BatchGeo::make(n_img, heights, widths, counts_per_image, b, geo))
+        return LIG_ERR_INVALID;
+    const int n = geo.total_points();
+    if (n > 0 && (!in3 || !means || !v_xy || !v_con || !v_in3 || !v_mean)) return LIG_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (dtype == LIG_F32)
+        return project_bwd<float>(n, chol, in3, means, opac, geo, v_xy, sxy, v_con, sco, v_in3, v_mean, s);
+    if (dtype == LIG_F64)
+        return project_bwd<double>(n, chol, in3, means, opac, geo, v_xy, sxy, v_con, sco, v_in3, v_mean, s);
+    return LIG_ERR_INVALID;
 }

@@ -25,6 +25,8 @@
 // roundings, and with them the alpha-threshold decisions, are the same, and
 // each pixel adds its terms in list order.
 #include <mutex>
+#include <tuple>
+#include <vector>
 
 #include "common.cuh"
 
@@ -214,6 +216,52 @@ __device__ __forceinline__ uint32_t region_bits(const Rec<T> &g, const Regions &
     return keep;
 }
 
+// ------------------------------------------------------------ tile setup
+// Work item -> image and tile origin.  Work items index the flattened
+// (image, tile) list of a BatchGeo; a single image is a batch of one.
+struct TileCtx {
+    int im, H, W, B, tx0, ty0, poff;
+    bool empty;  // the image has no intersections (reference empty-list branch)
+};
+
+// Intersections of image im: from the inclusive prefix sum of per-Gaussian
+// counts when given (batched), else the whole list's total.
+__device__ __forceinline__ bool image_empty(const BatchGeo &geo, const int32_t *cum,
+                                            const int32_t *d_total, int im) {
+    if (!cum) return *d_total == 0;
+    const int g0 = geo.g_off[im], g1 = geo.g_off[im + 1];
+    if (g1 <= g0) return true;
+    const int hi = cum[g1 - 1], lo = g0 > 0 ? cum[g0 - 1] : 0;
+    return hi - lo == 0;
+}
+
+__device__ __forceinline__ TileCtx tile_ctx(const BatchGeo &geo, const int32_t *cum,
+                                            const int32_t *d_total, int tile) {
+    TileCtx t;
+    t.im = geo.image_of_tile(tile);
+    const int lt = tile - geo.tile_off[t.im];
+    const int tbx = geo.tbx[t.im];
+    t.H = geo.H[t.im];
+    t.W = geo.W[t.im];
+    t.B = geo.B;
+    t.tx0 = (lt % tbx) * t.B;
+    t.ty0 = (lt / tbx) * t.B;
+    t.poff = geo.pix_off[t.im];
+    t.empty = image_empty(geo, cum, d_total, t.im);
+    return t;
+}
+
+// Next work item: blockIdx.x in a plain launch (one CTA per tile); in a
+// persistent launch (work != null) the CTA pulls items from a global counter
+// until the list is exhausted.  The loop ends because the counter only grows.
+__device__ __forceinline__ int next_tile(int *work, int &s_slot, bool first) {
+    if (!work) return first ? (int)blockIdx.x : 0x7fffffff;
+    __syncthreads();  // everyone is done with the previous item
+    if (threadIdx.x == 0) s_slot = atomicAdd(work, 1);
+    __syncthreads();
+    return s_slot;
+}
+
 // --------------------------------------------------------------- forward
 // One CTA per tile, warp w = region w (8x4 pixels), one pixel per lane.
 // Batches of blockDim Gaussians (list order) are staged in shared memory, one
@@ -266,29 +314,26 @@ struct FwdAcc {
 };
 
 template <typename T, bool GA>
-__global__ void __launch_bounds__(1024)
-raster_fwd_kernel(int H, int W, int B, int tbx, const int32_t *__restrict__ ids,
-                  const int2 *__restrict__ tile_bins, const int32_t *__restrict__ d_total,
-                  const Rec<T> *__restrict__ recs, T *__restrict__ img, T *__restrict__ wsum,
-                  T *__restrict__ odx, T *__restrict__ ody, T *__restrict__ odxy,
-                  int32_t *__restrict__ final_idx) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int32_t *__restrict__ ids,
+                                         const int2 *__restrict__ tile_bins,
+                                         const Rec<T> *__restrict__ recs, T *__restrict__ img,
+                                         T *__restrict__ wsum, T *__restrict__ odx,
+                                         T *__restrict__ ody, T *__restrict__ odxy,
+                                         int32_t *__restrict__ final_idx, Rec<T> *s_rec,
+                                         uint32_t *s_bits) {
     const int nt = blockDim.x;
-    Rec<T> *s_rec = reinterpret_cast<Rec<T> *>(smem_raw);
-    uint32_t *s_bits = reinterpret_cast<uint32_t *>(s_rec + nt);
     const unsigned FULL = 0xffffffffu;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int tile = blockIdx.x;
-    const int tx0 = (tile % tbx) * B, ty0 = (tile / tbx) * B;
+    const int B = tc.B, tx0 = tc.tx0, ty0 = tc.ty0;
     const Regions R = Regions::make(0, B);
     int lx, ly;
     R.pixel(w, lane, 0, lx, ly);
     const int gx = tx0 + lx, gy = ty0 + ly;
-    const bool inside = lx < B && ly < B && gx < W && gy < H;
-    const int pix = gy * W + gx;
+    const bool inside = lx < B && ly < B && gx < tc.W && gy < tc.H;
+    const int pix = tc.poff + gy * tc.W + gx;
     const T px = (T)gx + (T)0.5, py = (T)gy + (T)0.5;
 
-    if (*d_total == 0) {  // the reference's empty-list branch (rasterize.py:80-90)
+    if (tc.empty) {  // the reference's empty-list branch (rasterize.py:80-90)
         if (inside) {
             img[3 * pix] = (T)1; img[3 * pix + 1] = (T)1; img[3 * pix + 2] = (T)1;
             wsum[pix] = 0;
@@ -351,6 +396,26 @@ raster_fwd_kernel(int H, int W, int B, int tbx, const int32_t *__restrict__ ids,
                 odxy[3 * pix + ch] = acc.dxy[ch];
             }
         }
+    }
+}
+
+template <typename T, bool GA>
+__global__ void __launch_bounds__(1024)
+raster_fwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work,
+                  const int32_t *__restrict__ ids, const int2 *__restrict__ tile_bins,
+                  const int32_t *__restrict__ d_total, const Rec<T> *__restrict__ recs,
+                  T *__restrict__ img, T *__restrict__ wsum, T *__restrict__ odx,
+                  T *__restrict__ ody, T *__restrict__ odxy, int32_t *__restrict__ final_idx) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int s_slot;
+    Rec<T> *s_rec = reinterpret_cast<Rec<T> *>(smem_raw);
+    uint32_t *s_bits = reinterpret_cast<uint32_t *>(s_rec + blockDim.x);
+    const int n_tiles = geo.total_tiles();
+    for (int tile = next_tile(work, s_slot, true); tile < n_tiles;
+         tile = next_tile(work, s_slot, false)) {
+        const TileCtx tc = tile_ctx(geo, cum, d_total, tile);
+        fwd_tile<T, GA>(tc, tile, ids, tile_bins, recs, img, wsum, odx, ody, odxy, final_idx,
+                        s_rec, s_bits);
     }
 }
 
@@ -419,12 +484,14 @@ struct alignas(16) PixRec {
 };
 
 template <typename T, bool GA>
-__global__ void __launch_bounds__(1024)
-raster_bwd_kernel(int H, int W, int B, int tbx, const int32_t *__restrict__ ids,
-                  const int2 *__restrict__ tile_bins, const int32_t *__restrict__ d_total,
-                  const Rec<T> *__restrict__ recs, const int32_t *__restrict__ final_idx,
-                  CotSrc<T> cot, const T *__restrict__ v_dx, const T *__restrict__ v_dy,
-                  const T *__restrict__ v_dxy, T clamp, T *__restrict__ packed) {
+__device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
+                                         const int32_t *__restrict__ ids,
+                                         const int2 *__restrict__ tile_bins,
+                                         const Rec<T> *__restrict__ recs,
+                                         const int32_t *__restrict__ final_idx, CotSrc<T> cot,
+                                         const T *__restrict__ v_dx, const T *__restrict__ v_dy,
+                                         const T *__restrict__ v_dxy, T clamp,
+                                         T *__restrict__ packed, int &s_end) {
     using M = Math<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nt = blockDim.x;  // = 32 * regions: region-major pixel slots
@@ -433,12 +500,12 @@ raster_bwd_kernel(int H, int W, int B, int tbx, const int32_t *__restrict__ ids,
     uint32_t *s_bits = reinterpret_cast<uint32_t *>(s_rec + nt);
     int32_t *s_ids = reinterpret_cast<int32_t *>(s_bits + nt);
     uint16_t *s_list = reinterpret_cast<uint16_t *>(s_ids + nt);
-    __shared__ int s_end;
     const unsigned FULL = 0xffffffffu;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    if (*d_total == 0) return;  // gradients stay zero (rasterize.py:156-161)
-    const int tile = blockIdx.x;
-    const int tx0 = (tile % tbx) * B, ty0 = (tile / tbx) * B;
+    if (tc.empty) return;  // gradients stay zero (rasterize.py:156-161)
+    const int B = tc.B, H = tc.H, W = tc.W, tx0 = tc.tx0, ty0 = tc.ty0;
+    // fused L2: mean over this image's 3HW values (a batch sums per-image means)
+    if (!cot.v_img) cot.scale = (T)(2.0 / (3.0 * (double)H * (double)W));
     const Regions R = Regions::make(GA ? 2 : 0, B);
     uint16_t *my_list = s_list + w * nt;
     const PixRec<T, GA> *my_pix = s_pix + w * 32;
@@ -450,7 +517,7 @@ raster_bwd_kernel(int H, int W, int B, int tbx, const int32_t *__restrict__ ids,
         R.pixel(w, lane, 0, lx, ly);
         const int gx = tx0 + lx, gy = ty0 + ly;
         const bool inside = lx < B && ly < B && gx < W && gy < H;
-        const int p = inside ? gy * W + gx : 0;
+        const int p = inside ? tc.poff + gy * W + gx : 0;
         PixRec<T, GA> c;
         c.px = (T)gx + (T)0.5;
         c.py = (T)gy + (T)0.5;
@@ -608,6 +675,24 @@ raster_bwd_kernel(int H, int W, int B, int tbx, const int32_t *__restrict__ ids,
     }
 }
 
+template <typename T, bool GA>
+__global__ void __launch_bounds__(1024)
+raster_bwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work,
+                  const int32_t *__restrict__ ids, const int2 *__restrict__ tile_bins,
+                  const int32_t *__restrict__ d_total, const Rec<T> *__restrict__ recs,
+                  const int32_t *__restrict__ final_idx, CotSrc<T> cot,
+                  const T *__restrict__ v_dx, const T *__restrict__ v_dy,
+                  const T *__restrict__ v_dxy, T clamp, T *__restrict__ packed) {
+    __shared__ int s_end, s_slot;
+    const int n_tiles = geo.total_tiles();
+    for (int tile = next_tile(work, s_slot, true); tile < n_tiles;
+         tile = next_tile(work, s_slot, false)) {
+        const TileCtx tc = tile_ctx(geo, cum, d_total, tile);
+        bwd_tile<T, GA>(tc, tile, ids, tile_bins, recs, final_idx, cot, v_dx, v_dy, v_dxy, clamp,
+                        packed, s_end);
+    }
+}
+
 // Packed per-Gaussian gradients [N][12] -> the five output arrays of the ABI.
 template <typename T>
 __global__ void unpack_grads_kernel(int n, const T *__restrict__ packed, Grads<T> out) {
@@ -640,34 +725,80 @@ int pack(int n, const void *xys, const void *con, const void *col, const void *o
     return LIG_OK;
 }
 
+// Opt a kernel into `bytes` of dynamic shared memory, once per (kernel,
+// device, size): repeated calls cost nothing, and none is made during a
+// stream capture after the first eager call.
 inline bool set_dyn_smem(const void *fn, size_t bytes) {
     if (bytes <= 48 * 1024) return true;
-    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) ==
-           cudaSuccess;
+    static std::mutex mu;
+    static std::vector<std::tuple<const void *, int, size_t>> done;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    std::lock_guard<std::mutex> lock(mu);
+    for (auto &e : done)
+        if (std::get<0>(e) == fn && std::get<1>(e) == dev && std::get<2>(e) >= bytes) return true;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) !=
+        cudaSuccess)
+        return false;
+    done.emplace_back(fn, dev, bytes);
+    return true;
 }
 
+// Grid of a persistent launch: every CTA that fits on the device at once.
+inline int persistent_grid(const void *fn, int threads, size_t smem) {
+    static std::mutex mu;
+    static std::vector<std::tuple<const void *, int, int, size_t, int>> cache;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    std::lock_guard<std::mutex> lock(mu);
+    for (auto &e : cache)
+        if (std::get<0>(e) == fn && std::get<1>(e) == dev && std::get<2>(e) == threads &&
+            std::get<3>(e) == smem)
+            return std::get<4>(e);
+    int per_sm = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return 0;
+    const int g = per_sm * sms;
+    cache.emplace_back(fn, dev, threads, smem, g);
+    return g;
+}
+
+// How a raster kernel walks the flattened (image, tile) list.
+struct TileWalk {
+    const int32_t *cum = nullptr;  // per-image empty test (batched); null: *d_total
+    int *work = nullptr;           // persistent: global work counter; null: CTA per tile
+};
+
 template <typename T>
-int raster_fwd(int H, int W, int B, int n, const int32_t *ids, const int32_t *bins,
+int raster_fwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int32_t *bins,
                const int32_t *d_total, const void *xys, const void *con, const void *col,
                const void *op, void *ws, size_t ws_bytes, void *img, void *wsum, void *dx,
                void *dy, void *dxy, int32_t *fin, cudaStream_t s) {
+    const int n = geo.total_points();
     int rc = pack<T>(n, xys, con, col, op, ws, ws_bytes, s);
     if (rc) return rc;
     const bool ga = dx != nullptr;
-    const int tbx = (W + B - 1) / B, tby = (H + B - 1) / B;
-    const int nt = 32 * Regions::make(0, B).count;
+    const int nt = 32 * Regions::make(0, geo.B).count;
     const size_t sm = (size_t)nt * (sizeof(Rec<T>) + sizeof(uint32_t));
     const void *fn = ga ? (const void *)raster_fwd_kernel<T, true>
                         : (const void *)raster_fwd_kernel<T, false>;
     if (!set_dyn_smem(fn, sm)) return LIG_ERR_LAUNCH;
+    int grid = geo.total_tiles();
+    if (walk.work) {
+        const int pg = persistent_grid(fn, nt, sm);
+        if (pg <= 0) return LIG_ERR_LAUNCH;
+        grid = grid < pg ? grid : pg;
+        cudaMemsetAsync(walk.work, 0, sizeof(int), s);
+    }
     if (ga)
-        raster_fwd_kernel<T, true><<<tbx * tby, nt, sm, s>>>(
-            H, W, B, tbx, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws, (T *)img,
-            (T *)wsum, (T *)dx, (T *)dy, (T *)dxy, fin);
+        raster_fwd_kernel<T, true><<<grid, nt, sm, s>>>(
+            geo, walk.cum, walk.work, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws,
+            (T *)img, (T *)wsum, (T *)dx, (T *)dy, (T *)dxy, fin);
     else
-        raster_fwd_kernel<T, false><<<tbx * tby, nt, sm, s>>>(
-            H, W, B, tbx, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws, (T *)img,
-            (T *)wsum, nullptr, nullptr, nullptr, fin);
+        raster_fwd_kernel<T, false><<<grid, nt, sm, s>>>(
+            geo, walk.cum, walk.work, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws,
+            (T *)img, (T *)wsum, nullptr, nullptr, nullptr, fin);
     note_launches(1);
     LIG_LAUNCH_CHECK();
     return LIG_OK;
@@ -680,11 +811,12 @@ inline size_t bwd_grad_offset(int n) {
 }
 
 template <typename T>
-int raster_bwd(int H, int W, int B, int n, const int32_t *ids, const int32_t *bins,
+int raster_bwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int32_t *bins,
                const int32_t *d_total, const void *xys, const void *con, const void *col,
                const void *op, const int32_t *fin, CotSrc<T> cot, const void *v_dx,
                const void *v_dy, const void *v_dxy, double clamp, void *ws, size_t ws_bytes,
                void *v_xy, void *v_abs, void *v_con, void *v_rgb, void *v_op, cudaStream_t s) {
+    const int n = geo.total_points();
     const size_t goff = bwd_grad_offset<T>(n);
     if (ws_bytes < goff + sizeof(T) * 12 * (size_t)n) return LIG_ERR_WORKSPACE;
     T *packed = reinterpret_cast<T *>((char *)ws + goff);
@@ -693,8 +825,7 @@ int raster_bwd(int H, int W, int B, int n, const int32_t *ids, const int32_t *bi
     if (rc) return rc;
     const bool ga = v_dx != nullptr;
     const T cl = (T)(clamp > 0 ? clamp : (ga ? 0.999 : 0.99));
-    const int tbx = (W + B - 1) / B, tby = (H + B - 1) / B;
-    const int nt = 32 * Regions::make(ga ? 2 : 0, B).count;
+    const int nt = 32 * Regions::make(ga ? 2 : 0, geo.B).count;
     const int nw = nt / 32;
     const size_t pix = ga ? sizeof(PixRec<T, true>) : sizeof(PixRec<T, false>);
     const size_t sm = (size_t)nt * pix + (size_t)nt * (sizeof(Rec<T>) + 2 * sizeof(uint32_t)) +
@@ -702,14 +833,21 @@ int raster_bwd(int H, int W, int B, int n, const int32_t *ids, const int32_t *bi
     const void *fn = ga ? (const void *)raster_bwd_kernel<T, true>
                         : (const void *)raster_bwd_kernel<T, false>;
     if (!set_dyn_smem(fn, sm)) return LIG_ERR_LAUNCH;
+    int grid = geo.total_tiles();
+    if (walk.work) {
+        const int pg = persistent_grid(fn, nt, sm);
+        if (pg <= 0) return LIG_ERR_LAUNCH;
+        grid = grid < pg ? grid : pg;
+        cudaMemsetAsync(walk.work, 0, sizeof(int), s);
+    }
     if (ga)
-        raster_bwd_kernel<T, true><<<tbx * tby, nt, sm, s>>>(
-            H, W, B, tbx, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws, fin, cot,
-            (const T *)v_dx, (const T *)v_dy, (const T *)v_dxy, cl, packed);
+        raster_bwd_kernel<T, true><<<grid, nt, sm, s>>>(
+            geo, walk.cum, walk.work, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws, fin,
+            cot, (const T *)v_dx, (const T *)v_dy, (const T *)v_dxy, cl, packed);
     else
-        raster_bwd_kernel<T, false><<<tbx * tby, nt, sm, s>>>(
-            H, W, B, tbx, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws, fin, cot,
-            nullptr, nullptr, nullptr, cl, packed);
+        raster_bwd_kernel<T, false><<<grid, nt, sm, s>>>(
+            geo, walk.cum, walk.work, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws, fin,
+            cot, nullptr, nullptr, nullptr, cl, packed);
     Grads<T> g{(T *)v_xy, (T *)v_abs, (T *)v_con, (T *)v_rgb, (T *)v_op};
     if (n > 0) unpack_grads_kernel<T><<<(n + 255) / 256, 256, 0, s>>>(n, packed, g);
     note_launches(n > 0 ? 2 : 1);
@@ -718,7 +856,9 @@ int raster_bwd(int H, int W, int B, int n, const int32_t *ids, const int32_t *bi
 }
 
 inline bool raster_args_ok(int H, int W, int B, int n) {
-    return H > 0 && W > 0 && B >= 2 && B <= 32 && n >= 0;
+    // pixel-channel indices are 32-bit
+    return H > 0 && W > 0 && B >= 2 && B <= 32 && n >= 0 &&
+           3ll * H * W <= 0x7fffffffll;
 }
 
 }  // namespace lig
@@ -741,11 +881,11 @@ extern "C" int lig_raster_fwd(int dtype, int H, int W, int B, int n, const int32
         return LIG_ERR_INVALID;
     cudaStream_t s = (cudaStream_t)stream;
     if (dtype == LIG_F32)
-        return raster_fwd<float>(H, W, B, n, ids, bins, d_total, xys, con, col, op, ws, ws_bytes,
-                                 img, wsum, dx, dy, dxy, fin, s);
+        return raster_fwd<float>(BatchGeo::single(H, W, B, n), TileWalk{}, ids, bins, d_total,
+                                 xys, con, col, op, ws, ws_bytes, img, wsum, dx, dy, dxy, fin, s);
     if (dtype == LIG_F64)
-        return raster_fwd<double>(H, W, B, n, ids, bins, d_total, xys, con, col, op, ws, ws_bytes,
-                                  img, wsum, dx, dy, dxy, fin, s);
+        return raster_fwd<double>(BatchGeo::single(H, W, B, n), TileWalk{}, ids, bins, d_total,
+                                  xys, con, col, op, ws, ws_bytes, img, wsum, dx, dy, dxy, fin, s);
     return LIG_ERR_INVALID;
 }
 
@@ -764,13 +904,15 @@ extern "C" int lig_raster_bwd(int dtype, int H, int W, int B, int n, const int32
     if (n == 0) return LIG_OK;
     if (dtype == LIG_F32) {
         CotSrc<float> cot{(const float *)v_img, (const float *)v_wsum, nullptr, nullptr, nullptr, 0.f};
-        return raster_bwd<float>(H, W, B, n, ids, bins, d_total, xys, con, col, op, fin, cot,
+        return raster_bwd<float>(BatchGeo::single(H, W, B, n), TileWalk{}, ids, bins, d_total,
+                                 xys, con, col, op, fin, cot,
                                  v_dx, v_dy, v_dxy, clamp, ws, ws_bytes, v_xy, v_abs, v_con,
                                  v_rgb, v_op, s);
     }
     if (dtype == LIG_F64) {
         CotSrc<double> cot{(const double *)v_img, (const double *)v_wsum, nullptr, nullptr, nullptr, 0.0};
-        return raster_bwd<double>(H, W, B, n, ids, bins, d_total, xys, con, col, op, fin, cot,
+        return raster_bwd<double>(BatchGeo::single(H, W, B, n), TileWalk{}, ids, bins, d_total,
+                                  xys, con, col, op, fin, cot,
                                   v_dx, v_dy, v_dxy, clamp, ws, ws_bytes, v_xy, v_abs, v_con,
                                   v_rgb, v_op, s);
     }
@@ -793,14 +935,16 @@ extern "C" int lig_raster_bwd_l2(int dtype, int H, int W, int B, int n, const in
     if (dtype == LIG_F32) {
         CotSrc<float> cot{nullptr, nullptr, (const float *)img, (const float *)target,
                           (const float *)grad_loss, (float)scale};
-        return raster_bwd<float>(H, W, B, n, ids, bins, d_total, xys, con, col, op, fin, cot,
+        return raster_bwd<float>(BatchGeo::single(H, W, B, n), TileWalk{}, ids, bins, d_total,
+                                 xys, con, col, op, fin, cot,
                                  nullptr, nullptr, nullptr, clamp, ws, ws_bytes, v_xy, v_abs,
                                  v_con, v_rgb, v_op, s);
     }
     if (dtype == LIG_F64) {
         CotSrc<double> cot{nullptr, nullptr, (const double *)img, (const double *)target,
                            (const double *)grad_loss, scale};
-        return raster_bwd<double>(H, W, B, n, ids, bins, d_total, xys, con, col, op, fin, cot,
+        return raster_bwd<double>(BatchGeo::single(H, W, B, n), TileWalk{}, ids, bins, d_total,
+                                  xys, con, col, op, fin, cot,
                                   nullptr, nullptr, nullptr, clamp, ws, ws_bytes, v_xy, v_abs,
                                   v_con, v_rgb, v_op, s);
     }
@@ -857,8 +1001,85 @@ extern "C" int lig_raster_fwd_noalloc(int H, int W, int B, int n, const int32_t 
     int rc = LIG_OK;
     void *scratch = noalloc_scratch_ptr(rc);
     if (rc != LIG_OK) return rc;
-    return raster_fwd<float>(H, W, B, n, ids, bins, d_total, xys, con, col, op, scratch,
-                             sizeof(g_noalloc_scratch), img, wsum, nullptr, nullptr, nullptr, fin,
-                             (cudaStream_t)stream);
+    return raster_fwd<float>(BatchGeo::single(H, W, B, n), TileWalk{}, ids, bins, d_total, xys,
+                             con, col, op, scratch, sizeof(g_noalloc_scratch), img, wsum, nullptr,
+                             nullptr, nullptr, fin, (cudaStream_t)stream);
 }
 
+// ------------------------------------------------------------ batched entries
+// A batch of images in one launch per stage: image i has heights[i] x
+// widths[i] pixels and counts[i] Gaussians; Gaussians, tile lists and the
+// HWC buffers are the images' arrays concatenated in batch order.  The
+// (image, tile) work list is flattened (image-major, row-major tiles within
+// an image); persistent != 0 runs one CTA per resident slot pulling work
+// items from `work` (one int of device memory, overwritten).
+namespace lig {
+inline bool batch_geo(int n_img, const int32_t *h, const int32_t *w, const int32_t *c, int B,
+                      BatchGeo &geo) {
+    if (!h || !w || !c || B < 2 || B > 32) return false;
+    return BatchGeo::make(n_img, h, w, c, B, geo);
+}
+}  // namespace lig
+
+extern "C" int lig_raster_fwd_batch(int dtype, int n_img, const int32_t *heights,
+                                    const int32_t *widths, const int32_t *counts, int B,
+                                    const int32_t *ids, const int32_t *bins,
+                                    const int32_t *d_total, const int32_t *cum, const void *xys,
+                                    const void *con, const void *col, const void *op,
+                                    int persistent, int32_t *work, void *ws, size_t ws_bytes,
+                                    void *img, void *wsum, void *dx, void *dy, void *dxy,
+                                    int32_t *fin, void *stream) {
+    BatchGeo geo;
+    if (!batch_geo(n_img, heights, widths, counts, B, geo)) return LIG_ERR_INVALID;
+    const int n = geo.total_points();
+    if (!bins || !d_total || !img || !wsum || !fin || !ws || (persistent && !work) ||
+        (n > 0 && (!xys || !con || !col || !cum)) || ((dx || dy || dxy) && !(dx && dy && dxy)))
+        return LIG_ERR_INVALID;
+    TileWalk walk{n > 0 ? cum : nullptr, persistent ? work : nullptr};
+    cudaStream_t s = (cudaStream_t)stream;
+    if (dtype == LIG_F32)
+        return raster_fwd<float>(geo, walk, ids, bins, d_total, xys, con, col, op, ws, ws_bytes,
+                                 img, wsum, dx, dy, dxy, fin, s);
+    if (dtype == LIG_F64)
+        return raster_fwd<double>(geo, walk, ids, bins, d_total, xys, con, col, op, ws, ws_bytes,
+                                  img, wsum, dx, dy, dxy, fin, s);
+    return LIG_ERR_INVALID;
+}
+
+extern "C" int lig_raster_bwd_l2_batch(int dtype, int n_img, const int32_t *heights,
+                                       const int32_t *widths, const int32_t *counts, int B,
+                                       const int32_t *ids, const int32_t *bins,
+                                       const int32_t *d_total, const int32_t *cum,
+                                       const void *xys, const void *con, const void *col,
+                                       const void *op, const int32_t *fin, const void *img,
+                                       const void *target, const void *grad_loss, double clamp,
+                                       int persistent, int32_t *work, void *ws, size_t ws_bytes,
+                                       void *v_xy, void *v_abs, void *v_con, void *v_rgb,
+                                       void *v_op, void *stream) {
+    BatchGeo geo;
+    if (!batch_geo(n_img, heights, widths, counts, B, geo)) return LIG_ERR_INVALID;
+    const int n = geo.total_points();
+    if (!bins || !d_total || !fin || !img || !target || !grad_loss || !ws ||
+        (persistent && !work) ||
+        (n > 0 && (!xys || !con || !col || !cum || !v_xy || !v_abs || !v_con || !v_rgb)))
+        return LIG_ERR_INVALID;
+    if (n == 0) return LIG_OK;
+    TileWalk walk{cum, persistent ? work : nullptr};
+    cudaStream_t s = (cudaStream_t)stream;
+    if (dtype == LIG_F32) {
+        // per-image scale 2 / (3 H_i W_i) is formed in the kernel
+        CotSrc<float> cot{nullptr, nullptr, (const float *)img, (const float *)target,
+                          (const float *)grad_loss, 0.f};
+        return raster_bwd<float>(geo, walk, ids, bins, d_total, xys, con, col, op, fin, cot,
+                                 nullptr, nullptr, nullptr, clamp, ws, ws_bytes, v_xy, v_abs,
+                                 v_con, v_rgb, v_op, s);
+    }
+    if (dtype == LIG_F64) {
+        CotSrc<double> cot{nullptr, nullptr, (const double *)img, (const double *)target,
+                           (const double *)grad_loss, 0.0};
+        return raster_bwd<double>(geo, walk, ids, bins, d_total, xys, con, col, op, fin, cot,
+                                  nullptr, nullptr, nullptr, clamp, ws, ws_bytes, v_xy, v_abs,
+                                  v_con, v_rgb, v_op, s);
+    }
+    return LIG_ERR_INVALID;
+}
