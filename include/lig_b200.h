@@ -224,6 +224,18 @@ int lig_upscale_bwd(int dtype, int mode, int src_h, int src_w, int dst_h, int ds
                     const void *grad_out, void *grad_render, void *grad_dx, void *grad_dy,
                     void *grad_dxy, void *stream);
 
+/* Forward projection of a view of the Gaussians (region decode at a scale):
+ * every Gaussian is first mapped to means' = (means - origin) * (sx, sy) and
+ * L' = diag(sx, sy) L (cholesky != 0; the scale_to rule of
+ * minimal_trainer_upscale.py:139-157) or cov' = S cov S, then projected as
+ * lig_project_fwd onto an img_h x img_w output — a crop / rescaled render
+ * without materialising the transformed parameters. */
+int lig_project_fwd_view(int dtype, int num_points, int cholesky, const void *in3,
+                         const void *means2d, const void *opacities, int img_h, int img_w,
+                         int block_width, double origin_x, double origin_y, double scale_x,
+                         double scale_y, void *xys, void *extents, void *conics,
+                         int32_t *num_tiles_hit, void *stream);
+
 /* ---------------------------------------------------------------- batched */
 
 /* A batch of up to LIG_MAX_BATCH images processed by one launch per stage.
@@ -316,6 +328,19 @@ int lig_adam_step(int64_t n, float *params, const float *grads, float *exp_avg,
                   float *exp_avg_sq, double lr, double beta1, double beta2, double eps,
                   const int32_t *status, int32_t *step, int32_t *skipped, void *scratch,
                   void *stream);
+
+/* Scratch bytes of lig_adam_step_batch (device memory). */
+size_t lig_adam_batch_scratch_bytes(int n_img);
+
+/* Adam over a batch of fits in one flat fp32 buffer laid out
+ * [means 2N | cholesky 3N | rgb 3N] (N = sum of counts, image i owning
+ * Gaussians [sum_{j<i} counts_j, sum_{j<=i} counts_j)); steps (device
+ * int32[n_img]) are per image, so each image follows the updates of its own
+ * fit.  status / skipped as lig_adam_step. */
+int lig_adam_step_batch(int n_img, const int32_t *counts, float *params, const float *grads,
+                        float *exp_avg, float *exp_avg_sq, double lr, double beta1, double beta2,
+                        double eps, const int32_t *status, int32_t *steps, int32_t *skipped,
+                        void *scratch, size_t scratch_bytes, void *stream);
 
 /* ----------------------------------------------------------------- probes */
 

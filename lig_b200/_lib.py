@@ -75,6 +75,9 @@ SIGNATURES = {
     "lig_l2_clamped_loss_batch": (I, [I, I, P, P, P, P, P, P, P, SZ, P]),
     "lig_adam_scratch_bytes": (SZ, []),
     "lig_adam_step": (I, [I64, P, P, P, P, D, D, D, D, P, P, P, P, P]),
+    "lig_adam_batch_scratch_bytes": (SZ, [I]),
+    "lig_project_fwd_view": (I, [I, I, I, P, P, P, I, I, I, D, D, D, D, P, P, P, P, P]),
+    "lig_adam_step_batch": (I, [I, P, P, P, P, P, D, D, D, D, P, P, P, P, SZ, P]),
 }
 LIG_MAX_BATCH = 64
 

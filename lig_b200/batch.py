@@ -110,6 +110,16 @@ class BatchLayout:
 
 
 @dataclass
+class FitState:
+    """One image's fit state: (means, cholesky, rgb) parameters, the matching
+    Adam first / second moments (None: zeros) and the Adam step count."""
+    params: tuple
+    exp_avg: Optional[tuple] = None
+    exp_avg_sq: Optional[tuple] = None
+    step: int = 0
+
+
+@dataclass
 class BatchStats:
     iters: int = 0
     skipped: int = 0
@@ -121,8 +131,9 @@ class BatchedFit:
     """Fits one Gaussian set per target image, all images per launch.
 
     targets: list of [H_i, W_i, 3] fp32 CUDA tensors; counts: Gaussians per
-    image; init: optional list of (means, cholesky, colors) per image (else
-    seeded synthetic Gaussians, seed seed_base + i); block: tile size;
+    image; init: optional list per image of (means, cholesky, colors) or of
+    a FitState (parameters plus Adam moments and step, to resume a fit); else
+    seeded synthetic Gaussians, seed seed_base + i; block: tile size;
     persistent: persistent tile walk in the rasterizer; graph: capture the
     iteration as a CUDA graph (after two eager iterations)."""
 
@@ -153,10 +164,15 @@ class BatchedFit:
         self.v = torch.zeros(8 * N, dtype=f32, **kw)
         self.means, self.chol, self.rgbs = self._views(self.flat)
         self.g_means, self.g_chol, self.g_rgbs = self._views(self.grad)
+        self.steps = torch.zeros(L.n, dtype=i32, **kw)  # Adam steps per image
         with torch.no_grad():
             for i in range(L.n):
-                if init is not None:
-                    mu, ch, co = init[i]
+                src = init[i] if init is not None else None
+                if isinstance(src, FitState):
+                    self._load_state(i, src)
+                    continue
+                if src is not None:
+                    mu, ch, co = src
                 else:
                     mu, ch, co = synthetic.gaussians(L.counts[i], L.heights[i], L.widths[i],
                                                      diag=diag, seed=seed_base + i)
@@ -188,9 +204,9 @@ class BatchedFit:
         self.v_con = torch.empty(N, 3, dtype=f32, **kw)
         self.one = torch.ones((), dtype=f32, **kw)
         self.work = torch.zeros(1, dtype=i32, **kw)
-        self.step_count = torch.zeros(1, dtype=i32, **kw)
         self.skipped = torch.zeros(1, dtype=i32, **kw)
-        self.adam_scratch = torch.empty(64, dtype=torch.uint8, **kw)
+        self.adam_scratch = torch.empty(_lib.lib.lig_adam_batch_scratch_bytes(L.n),
+                                        dtype=torch.uint8, **kw)
         self.host_skipped = torch.zeros(1, dtype=i32, pin_memory=True)
         self.capacity = 0
         self.gids = None
@@ -200,6 +216,23 @@ class BatchedFit:
         self._size_capacity(self._count_intersections())
 
     # ------------------------------------------------------------ helpers
+    def _segments(self, flat, i):
+        """Image i's (means, cholesky, rgb) views in a flat [8N] buffer."""
+        return tuple(self.L.points_of(v, i) for v in self._views(flat))
+
+    def _load_state(self, i, st: "FitState"):
+        for buf, parts in ((self.flat, st.params), (self.m, st.exp_avg), (self.v, st.exp_avg_sq)):
+            if parts is None:
+                continue
+            for dst, src in zip(self._segments(buf, i), parts):
+                dst.copy_(src)
+        self.steps[i] = int(st.step)
+
+    def state_of(self, i: int) -> "FitState":
+        """Copy of image i's parameters, Adam moments and step (device)."""
+        seg = lambda buf: tuple(t.clone() for t in self._segments(buf, i))  # noqa: E731
+        return FitState(seg(self.flat), seg(self.m), seg(self.v), int(self.steps[i].item()))
+
     def _views(self, flat):
         N = self.L.points
         return (flat[:2 * N].view(N, 2), flat[2 * N:5 * N].view(N, 3),
@@ -257,22 +290,23 @@ class BatchedFit:
         call("lig_project_bwd_batch", _lib.LIG_F32, *L.args(), 1, _p(self.chol), _p(self.means),
              None, L.block, _p(self.v_xy), 2, _p(self.v_con), 3, _p(self.g_chol),
              _p(self.g_means), st)
-        call("lig_adam_step", self.flat.numel(), _p(self.flat), _p(self.grad), _p(self.m),
-             _p(self.v), self.lr, self.b1, self.b2, self.eps, _p(self.status),
-             _p(self.step_count), _p(self.skipped), _p(self.adam_scratch), st)
+        call("lig_adam_step_batch", L.n, L.args()[3], _p(self.flat), _p(self.grad), _p(self.m),
+             _p(self.v), self.lr, self.b1, self.b2, self.eps, _p(self.status), _p(self.steps),
+             _p(self.skipped), _p(self.adam_scratch), self.adam_scratch.numel(), st)
         self.host_skipped.copy_(self.skipped, non_blocking=True)
 
     def _capture(self):
-        torch.cuda.synchronize(self.dev)
+        torch.cuda.current_stream(self.dev).synchronize()
         g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g):
+        # thread-local: other threads (e.g. a render loop) keep working
+        with torch.cuda.graph(g, capture_error_mode="thread_local"):
             self._enqueue_step()
         self.graph = g
         self.stats.recaptures += 1
 
     def _recover(self):
         """A step overflowed the capacity (and was skipped): grow, recapture."""
-        torch.cuda.synchronize(self.dev)
+        torch.cuda.current_stream(self.dev).synchronize()
         k = int(self.skipped.item())
         self.skipped.zero_()
         self.host_skipped.zero_()
@@ -301,7 +335,7 @@ class BatchedFit:
                 applied += 1
                 if int(self.host_skipped[0]) > 0:  # pinned copy, no sync
                     applied -= self._recover()
-            torch.cuda.synchronize(self.dev)
+            torch.cuda.current_stream(self.dev).synchronize()
             if int(self.skipped.item()) == 0:
                 return self.stats
             applied -= self._recover()

@@ -78,9 +78,102 @@ adam_kernel(int64_t n, float *__restrict__ p, const float *__restrict__ g,
     }
 }
 
+// ---------------------------------------------------------------- batched
+// A batch of fits in one flat buffer laid out [means 2N | cholesky 3N |
+// rgb 3N] (N = total Gaussians, image i owning Gaussians [g_off[i],
+// g_off[i+1])).  Every image keeps its own step count, so a fit that joins
+// or leaves a running batch follows exactly the updates it would get alone.
+struct AdamBatch {
+    int n_img, n_pts;
+    int g_off[kMaxBatch + 1];
+};
+
+__global__ void adam_batch_prologue_kernel(AdamBatch ab, const int32_t *__restrict__ status,
+                                           int32_t *steps, int32_t *skipped, double lr,
+                                           double b1, double b2, AdamScalars *out) {
+    const int i = threadIdx.x;
+    const bool skip = status && (*status & LIG_STATUS_OVERFLOW);
+    if (i == 0 && skip && skipped) *skipped += 1;
+    if (i >= ab.n_img) return;
+    AdamScalars a{0.f, 1.f, skip ? 1 : 0, 0};
+    if (!skip) {
+        const int t = steps[i] + 1;
+        steps[i] = t;
+        a.step_size = (float)(lr / (1.0 - pow(b1, (double)t)));
+        a.bc2_sqrt = (float)sqrt(1.0 - pow(b2, (double)t));
+    }
+    out[i] = a;
+}
+
+__device__ __forceinline__ int elem_image(const AdamBatch &ab, int64_t e) {
+    const int64_t n = ab.n_pts;
+    const int g = (int)(e < 2 * n ? e / 2 : (e < 5 * n ? (e - 2 * n) / 3 : (e - 5 * n) / 3));
+    return BatchGeo::find(ab.g_off, ab.n_img, g);
+}
+
+__global__ void __launch_bounds__(256)
+adam_batch_kernel(AdamBatch ab, float *__restrict__ p, const float *__restrict__ g,
+                  float *__restrict__ m, float *__restrict__ v, float b1, float b2, float eps,
+                  const AdamScalars *__restrict__ sc) {
+    if (sc[0].skip) return;
+    const int64_t n = 8ll * ab.n_pts;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const AdamScalars a = sc[elem_image(ab, i)];
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        p[i] -= a.step_size * mi / (sqrtf(vi) / a.bc2_sqrt + eps);
+    }
+}
+
 }  // namespace lig
 
 using namespace lig;
+
+extern "C" size_t lig_adam_batch_scratch_bytes(int n_img) {
+    return sizeof(AdamScalars) * (size_t)(n_img > 0 ? n_img : 1);
+}
+
+extern "C" int lig_adam_step_batch(int n_img, const int32_t *counts, float *params,
+                                   const float *grads, float *exp_avg, float *exp_avg_sq,
+                                   double lr, double beta1, double beta2, double eps,
+                                   const int32_t *status, int32_t *steps, int32_t *skipped,
+                                   void *scratch, size_t scratch_bytes, void *stream) {
+    if (n_img < 1 || n_img > kMaxBatch || !counts || !steps || !scratch) return LIG_ERR_INVALID;
+    if (scratch_bytes < lig_adam_batch_scratch_bytes(n_img)) return LIG_ERR_WORKSPACE;
+    AdamBatch ab;
+    ab.n_img = n_img;
+    ab.g_off[0] = 0;
+    long long tot = 0;
+    for (int i = 0; i < n_img; ++i) {
+        if (counts[i] < 0) return LIG_ERR_INVALID;
+        tot += counts[i];
+        if (8 * tot > 0x7fffffffffffll) return LIG_ERR_INVALID;
+        if (tot > 0x7fffffffll) return LIG_ERR_INVALID;
+        ab.g_off[i + 1] = (int)tot;
+    }
+    ab.n_pts = (int)tot;
+    if (tot > 0 && (!params || !grads || !exp_avg || !exp_avg_sq)) return LIG_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    AdamScalars *sc = (AdamScalars *)scratch;
+    adam_batch_prologue_kernel<<<1, kMaxBatch, 0, s>>>(ab, status, steps, skipped, lr, beta1,
+                                                       beta2, sc);
+    int launches = 1;
+    if (tot > 0) {
+        int64_t blocks = (8 * tot + 255) / 256;
+        const int64_t cap = 148 * 16;
+        if (blocks > cap) blocks = cap;
+        adam_batch_kernel<<<(int)blocks, 256, 0, s>>>(ab, params, grads, exp_avg, exp_avg_sq,
+                                                     (float)beta1, (float)beta2, (float)eps, sc);
+        ++launches;
+    }
+    note_launches(launches);
+    LIG_LAUNCH_CHECK();
+    return LIG_OK;
+}
 
 extern "C" size_t lig_adam_scratch_bytes(void) { return sizeof(AdamScalars); }
 

@@ -5,6 +5,7 @@
 // Every output element is written, so callers need no zero-fill (the reference
 // pre-zeroes with torch::zeros, csrc/bindings.cu:89-97).
 #include <atomic>
+#include <cmath>
 
 #include "common.cuh"
 
@@ -13,11 +14,27 @@ namespace lig {
 template <typename T> struct V2 { T x, y; };
 template <typename T> struct V3 { T x, y, z; };
 
+// Optional view transform of a render (region decode, scale_to): output
+// pixel coordinates are ((x - ox) sx, (y - oy) sy) in the Gaussians' frame,
+// so every Gaussian maps to means' = (means - origin) * (sx, sy) and
+// L' = diag(sx, sy) L (Cholesky; the scale_to rule of
+// minimal_trainer_upscale.py:139-157) or cov' = S cov S.  Off: inputs are used
+// as they are.
+template <typename T> struct View {
+    T ox, oy, sx, sy;
+    bool on;
+};
+
 // cov2d (a,b,c) from the input triple: pass-through, or the Cholesky product
 // [l11^2, l11 l21, l21^2 + l22^2] written as in csrc/forward.cu:79-83.
 template <typename T>
-__device__ __forceinline__ void input_cov(bool chol, const T *in3, int i, T &cx, T &cy, T &cz) {
+__device__ __forceinline__ void input_cov(bool chol, const T *in3, int i, T &cx, T &cy, T &cz,
+                                          const View<T> &v = View<T>{0, 0, 1, 1, false}) {
     T p = in3[3 * i], q = in3[3 * i + 1], r = in3[3 * i + 2];
+    if (v.on) {
+        if (chol) { p *= v.sx; q *= v.sy; r *= v.sy; }
+        else { p *= v.sx * v.sx; q *= v.sx * v.sy; r *= v.sy * v.sy; }
+    }
     if (chol) {
         cx = p * p;
         cy = p * q;
@@ -33,18 +50,23 @@ __device__ __forceinline__ void input_cov(bool chol, const T *in3, int i, T &cx,
 template <typename T>
 __global__ void project_fwd_kernel(int n, bool chol, const T *__restrict__ in3,
                                    const T *__restrict__ means, const T *__restrict__ opac,
-                                   BatchGeo geo, T *__restrict__ xys, T *__restrict__ extents,
-                                   T *__restrict__ conics, int32_t *__restrict__ counts) {
+                                   BatchGeo geo, View<T> view, T *__restrict__ xys,
+                                   T *__restrict__ extents, T *__restrict__ conics,
+                                   int32_t *__restrict__ counts) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int im = geo.image_of_gauss(i);
     const unsigned tbx = geo.tbx[im], tby = geo.tby(im), block = geo.B;
     T cx, cy, cz;
-    input_cov(chol, in3, i, cx, cy, cz);
+    input_cov(chol, in3, i, cx, cy, cz, view);
     T o = opac ? opac[i] : (T)1;
     T ca = 0, cb = 0, cc = 0, ex = 0, ey = 0;
     bool ok = cov2d_bounds(cx, cy, cz, o, ca, cb, cc, ex, ey);
     T mx = means[2 * i], my = means[2 * i + 1];
+    if (view.on) {
+        mx = (mx - view.ox) * view.sx;
+        my = (my - view.oy) * view.sy;
+    }
     int32_t area = 0;
     if (ok) {
         int x0, y0, x1, y1;
@@ -202,10 +224,10 @@ inline bool valid_geometry(int n, int h, int w, int b) {
 template <typename T>
 int project_fwd(int n, int chol, const void *in3, const void *means, const void *opac,
                 const BatchGeo &geo, void *xys, void *ext, void *con, int32_t *cnt,
-                cudaStream_t s) {
+                cudaStream_t s, View<T> view = View<T>{0, 0, 1, 1, false}) {
     if (n == 0) return LIG_OK;
     project_fwd_kernel<T><<<proj_blocks(n), kProjThreads, 0, s>>>(
-        n, chol != 0, (const T *)in3, (const T *)means, (const T *)opac, geo, (T *)xys,
+        n, chol != 0, (const T *)in3, (const T *)means, (const T *)opac, geo, view, (T *)xys,
         (T *)ext, (T *)con, cnt);
     note_launches(1);
     LIG_LAUNCH_CHECK();
@@ -342,5 +364,27 @@ extern "C" int lig_project_bwd_batch(int dtype, int n_img, const int32_t *height
         return project_bwd<float>(n, chol, in3, means, opac, geo, v_xy, sxy, v_con, sco, v_in3, v_mean, s);
     if (dtype == LIG_F64)
         return project_bwd<double>(n, chol, in3, means, opac, geo, v_xy, sxy, v_con, sco, v_in3, v_mean, s);
+    return LIG_ERR_INVALID;
+}
+
+extern "C" int lig_project_fwd_view(int dtype, int n, int chol, const void *in3,
+                                    const void *means, const void *opac, int h, int w, int b,
+                                    double origin_x, double origin_y, double scale_x,
+                                    double scale_y, void *xys, void *ext, void *con,
+                                    int32_t *cnt, void *stream) {
+    if (n < 0 || h <= 0 || w <= 0 || b < 1 || !(scale_x > 0.0) || !(scale_y > 0.0) ||
+        !std::isfinite(scale_x) || !std::isfinite(scale_y) || !std::isfinite(origin_x) ||
+        !std::isfinite(origin_y) ||
+        (n > 0 && (!in3 || !means || !xys || !ext || !con || !cnt)))
+        return LIG_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    const BatchGeo geo = BatchGeo::single(h, w, b, n);
+    if (dtype == LIG_F32)
+        return project_fwd<float>(n, chol, in3, means, opac, geo, xys, ext, con, cnt, s,
+                                  View<float>{(float)origin_x, (float)origin_y, (float)scale_x,
+                                              (float)scale_y, true});
+    if (dtype == LIG_F64)
+        return project_fwd<double>(n, chol, in3, means, opac, geo, xys, ext, con, cnt, s,
+                                   View<double>{origin_x, origin_y, scale_x, scale_y, true});
     return LIG_ERR_INVALID;
 }

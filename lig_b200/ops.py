@@ -141,6 +141,26 @@ def project_fwd(in3, means2d, opacities, img_h, img_w, block, cholesky: bool):
     return xys, ext, con, cnt
 
 
+def project_fwd_view(in3, means2d, opacities, img_h, img_w, block, cholesky: bool,
+                     origin=(0.0, 0.0), scale=(1.0, 1.0)):
+    """Projection of the view means' = (means - origin) * scale,
+    L' = diag(scale) L (or cov' = S cov S) onto an img_h x img_w output."""
+    _check_cuda(in3, means2d, opacities)
+    in3 = _c(in3)
+    means2d = _c(means2d, in3.dtype)
+    opacities = _c(opacities, in3.dtype)
+    n = in3.shape[0]
+    xys = torch.empty((n, 2), dtype=in3.dtype, device=in3.device)
+    ext = torch.empty((n, 2), dtype=in3.dtype, device=in3.device)
+    con = torch.empty((n, 3), dtype=in3.dtype, device=in3.device)
+    cnt = torch.empty((n,), dtype=torch.int32, device=in3.device)
+    call("lig_project_fwd_view", _dt(in3), n, int(cholesky), _p(in3), _p(means2d),
+         _p(opacities), int(img_h), int(img_w), int(block), float(origin[0]), float(origin[1]),
+         float(scale[0]), float(scale[1]), _p(xys), _p(ext), _p(con), _p(cnt),
+         _stream(in3.device))
+    return xys, ext, con, cnt
+
+
 def _rows(t: torch.Tensor, width: int) -> torch.Tensor:
     """Row-strided view accepted by the kernels (unit inner stride)."""
     if t.dim() != 2 or t.shape[1] != width or t.stride(1) != 1 or t.stride(0) < width:
