@@ -1,0 +1,493 @@
+"""Serving loop: region decodes of resident Gaussian sets and fit requests on
+one GPU, with HBM-budget admission and continuous batching.
+
+The reference has no server: it fits one image per process and renders a
+level with ``Gaussian2D.forward`` (train.py:181-207, gaussianlig.py:70-93).
+This module serves both kinds of work at once:
+
+* **Render requests** decode a crop of a resident set at a scale: the view
+  transform means' = (means - origin) * s, L' = s L is folded into the
+  projection (lig_project_fwd_view), then binning and the forward rasterizer
+  produce the [h, w, 3] image in HBM.  They run on a high-priority CUDA
+  stream, so their thread blocks are scheduled ahead of queued fit blocks.
+* **Fit requests** (target image, Gaussian count, iterations) run on a
+  low-priority stream as one BatchedFit over every admitted fit: jobs join
+  and leave the batch between chunks of iterations (continuous batching);
+  each job keeps its own parameters, Adam moments and step, so its result
+  does not depend on what it was batched with.
+* **Admission**: every request reserves an estimate of its device bytes
+  against the HBM budget before it starts and releases it when done; a
+  request that does not fit waits in its queue (FIFO per kind).
+
+Latency is measured on the host from submission to the completion of the
+request's device work (a CUDA event on its stream).
+"""
+from __future__ import annotations
+
+import collections
+import math
+import threading
+import time
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional
+
+import torch
+
+from . import ops, synthetic
+from .batch import BatchedFit, FitState
+
+
+@dataclass
+class GaussianSet:
+    """A resident fitted level: means [N,2], cholesky [N,3] (or cov2d with
+    cholesky=False), rgb [N,3] on the device; H, W its native image size."""
+    means: torch.Tensor
+    chol: torch.Tensor
+    rgbs: torch.Tensor
+    H: int
+    W: int
+    opacities: Optional[torch.Tensor] = None
+    cholesky: bool = True
+
+    @property
+    def n(self) -> int:
+        return self.means.shape[0]
+
+    @property
+    def nbytes(self) -> int:
+        t = [self.means, self.chol, self.rgbs] + ([self.opacities] if self.opacities is not None
+                                                   else [])
+        return sum(x.numel() * x.element_size() for x in t)
+
+
+def render_view(gs: GaussianSet, out_h: int, out_w: int, origin=(0.0, 0.0), scale=(1.0, 1.0),
+                block: int = 16, grad_aware: bool = False):
+    """Decode the view ((x - ox) sx, (y - oy) sy) of a set as an
+    [out_h, out_w, 3] image (plus wsum and, with grad_aware, dx/dy/dxy) on
+    the current stream."""
+    with torch.no_grad():
+        xys, ext, con, cnt = ops.project_fwd_view(gs.chol, gs.means, gs.opacities, out_h, out_w,
+                                                  block, gs.cholesky, origin, scale)
+
+        def enqueue(b):
+            return ops.raster_fwd(out_h, out_w, block, b.gaussian_ids_sorted, b.tile_bins,
+                                  b.total, xys, con, gs.rgbs, gs.opacities, grad_aware)
+
+        _, outs = ops.bin_gaussians(xys, ext, cnt, out_h, out_w, block, after_enqueue=enqueue)
+    img, wsum, dx, dy, dxy, _ = outs
+    return (img, wsum, dx, dy, dxy) if grad_aware else (img, wsum)
+
+
+# ---------------------------------------------------------------- requests
+@dataclass
+class RenderRequest:
+    set_id: str
+    out_h: int
+    out_w: int
+    origin: tuple = (0.0, 0.0)
+    scale: float = 1.0
+    keep: bool = True   # keep the decoded image in the result
+
+
+@dataclass
+class FitRequest:
+    """target: [H, W, 3] device tensor, or a callable returning one (made
+    when the fit is admitted, so queued requests hold no device memory;
+    shape (H, W) is then required)."""
+    target: object
+    n_points: int
+    iters: int
+    lr: float = 1e-3
+    seed: int = 0
+    keep: bool = True        # keep the fitted parameters in the result
+    shape: Optional[tuple] = None
+
+    def hw(self):
+        return tuple(self.shape) if self.shape is not None else tuple(self.target.shape[:2])
+
+
+@dataclass
+class Result:
+    req_id: int
+    kind: str
+    t_submit: float
+    t_start: float = 0.0
+    t_done: float = 0.0
+    output: object = None
+    error: Optional[str] = None
+
+    @property
+    def latency(self) -> float:
+        return self.t_done - self.t_submit
+
+
+class MemoryBudget:
+    """Device bytes reserved by admitted requests and resident sets."""
+
+    def __init__(self, budget_bytes: int):
+        self.budget = int(budget_bytes)
+        self.used = 0
+        self.peak = 0
+        self._lock = threading.Lock()
+
+    def try_reserve(self, n: int) -> bool:
+        with self._lock:
+            if self.used + n > self.budget:
+                return False
+            self.used += n
+            self.peak = max(self.peak, self.used)
+            return True
+
+    def release(self, n: int):
+        with self._lock:
+            self.used -= n
+
+
+def render_bytes(gs: GaussianSet, out_h: int, out_w: int, block: int = 16) -> int:
+    """Upper estimate of a decode's device bytes: per-Gaussian projection and
+    record buffers, intersections (keys, ids, sort buffers) from the worst
+    tile coverage of a Gaussian of this set at this output size, outputs."""
+    n, p = gs.n, out_h * out_w
+    tiles = ((out_w + block - 1) // block) * ((out_h + block - 1) // block)
+    m = min(n * 16, n + 4 * tiles * 64)
+    return n * (36 + 48 + 8) + m * 20 + p * 20 + tiles * 8 + (1 << 20)
+
+
+def fit_bytes(h: int, w: int, n: int, block: int = 16) -> int:
+    """Estimate of a fit job's device bytes inside a batched fit: parameters,
+    gradients and moments (8 floats each), per-Gaussian buffers, per-pixel
+    target / render / wsum / final index, intersections (about 8 per Gaussian
+    at the configs' scales) with sort buffers."""
+    p = h * w
+    return n * (8 * 4 * 4 + 60 + 96 + 28) + p * 32 + n * 8 * 20 + (1 << 20)
+
+
+@dataclass(eq=False)
+class _FitJob:
+    req_id: int
+    req: FitRequest
+    target: Optional[torch.Tensor] = None
+    state: Optional[FitState] = None
+    done: int = 0
+    reserved: int = 0
+
+
+class Server:
+    """Render + fit server on one GPU (see module docstring).
+
+    budget_bytes: HBM budget for admission; max_fit_batch: images per batched
+    fit (<= 64); fit_chunk: iterations between batch changes."""
+
+    def __init__(self, budget_bytes: int = 150 * 10**9, device="cuda", block: int = 16,
+                 max_fit_batch: int = 64, fit_chunk: int = 20, fit_graph: bool = True):
+        self.dev = torch.device(device)
+        self.block = block
+        self.max_fit_batch = max_fit_batch
+        self.fit_chunk = fit_chunk
+        self.fit_graph = fit_graph
+        self.budget = MemoryBudget(budget_bytes)
+        # lower is higher priority; out-of-range values map to the extremes
+        self.render_stream = torch.cuda.Stream(self.dev, priority=-16)
+        self.fit_stream = torch.cuda.Stream(self.dev, priority=0)
+        self.sets: Dict[str, GaussianSet] = {}
+        self.results: Dict[int, Result] = {}
+        self._render_q: collections.deque = collections.deque()
+        self._fit_q: collections.deque = collections.deque()
+        self._cv = threading.Condition()
+        self._next_id = 0
+        self._running = False
+        self._abort = False
+        self._threads: List[threading.Thread] = []
+        self.fit_batches = 0
+        self.errors: List[str] = []
+
+    # ----------------------------------------------------------- resources
+    def add_set(self, set_id: str, gs: GaussianSet):
+        if not self.budget.try_reserve(gs.nbytes):
+            raise MemoryError(f"set {set_id}: {gs.nbytes} bytes exceed the HBM budget")
+        self.sets[set_id] = gs
+
+    def submit(self, req) -> int:
+        with self._cv:
+            rid = self._next_id
+            self._next_id += 1
+            kind = "render" if isinstance(req, RenderRequest) else "fit"
+            self.results[rid] = Result(rid, kind, time.perf_counter())
+            (self._render_q if kind == "render" else self._fit_q).append((rid, req))
+            self._cv.notify_all()
+        return rid
+
+    def start(self):
+        self._running = True
+        self._threads = [threading.Thread(target=self._render_loop, name="lig-render",
+                                          daemon=True),
+                         threading.Thread(target=self._fit_loop, name="lig-fit", daemon=True)]
+        for t in self._threads:
+            t.start()
+
+    def drain(self, timeout: Optional[float] = None) -> bool:
+        """Wait until every submitted request has finished."""
+        t_end = None if timeout is None else time.perf_counter() + timeout
+        while True:
+            with self._cv:
+                pending = [r for r in self.results.values() if r.t_done == 0.0]
+                if not pending:
+                    return True
+                left = None if t_end is None else t_end - time.perf_counter()
+                if left is not None and left <= 0:
+                    return False
+                self._cv.wait(0.05 if left is None else min(0.05, left))
+
+    def stop(self, abort: bool = False):
+        """Stop the workers after the queues drain (abort: drop what is
+        queued or running; those requests stay unfinished)."""
+        with self._cv:
+            self._running = False
+            self._abort = abort
+            if abort:
+                self._render_q.clear()
+                self._fit_q.clear()
+            self._cv.notify_all()
+        for t in self._threads:
+            t.join()
+
+    def _finish(self, rid: int, output=None, error: Optional[str] = None):
+        with self._cv:
+            r = self.results[rid]
+            r.output = output
+            r.error = error
+            r.t_done = time.perf_counter()
+            if error:
+                self.errors.append(f"{r.kind} {rid}: {error}")
+            self._cv.notify_all()
+
+    # -------------------------------------------------------------- renders
+    def _render_loop(self):
+        torch.cuda.set_device(self.dev)
+        while True:
+            with self._cv:
+                if self._abort:
+                    return
+                while self._running and not self._render_q:
+                    self._cv.wait(0.05)
+                if not self._render_q:
+                    if not self._running:
+                        return
+                    continue
+                rid, req = self._render_q[0]
+                gs = self.sets.get(req.set_id)
+                need = render_bytes(gs, req.out_h, req.out_w, self.block) if gs else 0
+                if gs is not None and not self.budget.try_reserve(need):
+                    self._cv.wait(0.01)  # head of line waits for memory
+                    continue
+                self._render_q.popleft()
+            if gs is None:
+                self._finish(rid, error=f"unknown set {req.set_id}")
+                continue
+            self.results[rid].t_start = time.perf_counter()
+            try:
+                with torch.cuda.stream(self.render_stream):
+                    img, _ = render_view(gs, req.out_h, req.out_w, req.origin,
+                                         (req.scale, req.scale), self.block)
+                    ev = torch.cuda.Event()
+                    ev.record(self.render_stream)
+                ev.synchronize()
+                self._finish(rid, img if req.keep else None)
+            except Exception as e:  # reported per request; the loop keeps serving
+                self._finish(rid, error=repr(e))
+            finally:
+                self.budget.release(need)
+
+    # ----------------------------------------------------------------- fits
+    def _admit_fits(self, active: List[_FitJob]) -> bool:
+        """Move queued fits into the running batch while memory and batch
+        slots allow (FIFO; fits with another learning rate wait until the
+        batch drains)."""
+        changed = False
+        with self._cv:
+            while self._fit_q and len(active) < self.max_fit_batch:
+                rid, req = self._fit_q[0]
+                if active and req.lr != active[0].req.lr:
+                    break
+                h, w = req.hw()
+                need = fit_bytes(h, w, req.n_points, self.block)
+                if not self.budget.try_reserve(need):
+                    break
+                self._fit_q.popleft()
+                self.results[rid].t_start = time.perf_counter()
+                active.append(_FitJob(rid, req, reserved=need))
+                changed = True
+        return changed
+
+    def _build_batch(self, jobs: List[_FitJob]) -> BatchedFit:
+        init = []
+        for j in jobs:
+            if j.target is None:
+                t = j.req.target() if callable(j.req.target) else j.req.target
+                j.target = t.to(self.dev, torch.float32).contiguous()
+            if j.state is None:
+                h, w = j.target.shape[:2]
+                mu, ch, co = synthetic.gaussians(j.req.n_points, h, w, seed=j.req.seed)
+                j.state = FitState((mu.to(self.dev), ch.to(self.dev), co.to(self.dev)))
+            init.append(j.state)
+        fit = BatchedFit([j.target for j in jobs], [j.req.n_points for j in jobs],
+                         block=self.block, lr=jobs[0].req.lr, init=init, graph=self.fit_graph)
+        self.fit_batches += 1
+        return fit
+
+    def _fit_loop(self):
+        torch.cuda.set_device(self.dev)
+        active: List[_FitJob] = []
+        batch: Optional[BatchedFit] = None
+        batch_jobs: List[_FitJob] = []
+        with torch.cuda.stream(self.fit_stream):
+            while True:
+                if self._abort:
+                    for j in active:
+                        self.budget.release(j.reserved)
+                    return
+                changed = self._admit_fits(active)
+                if not active:
+                    with self._cv:
+                        if not self._running and not self._fit_q:
+                            return
+                        self._cv.wait(0.05)
+                    continue
+                try:
+                    if changed or batch is None:
+                        if batch is not None:  # carry running jobs over
+                            for i, j in enumerate(batch_jobs):
+                                j.state = batch.state_of(i)
+                            batch = None
+                        batch_jobs = list(active)
+                        batch = self._build_batch(batch_jobs)
+                    k = min(self.fit_chunk, min(j.req.iters - j.done for j in batch_jobs))
+                    batch.fit(k)
+                except Exception as e:  # fail this batch's jobs, keep serving
+                    for j in active:
+                        self.budget.release(j.reserved)
+                        self._finish(j.req_id, error=repr(e))
+                    active, batch, batch_jobs = [], None, []
+                    continue
+                for j in batch_jobs:
+                    j.done += k
+                finished = [j for j in batch_jobs if j.done >= j.req.iters]
+                if finished:
+                    for i, j in enumerate(batch_jobs):
+                        st = batch.state_of(i)
+                        if j.done >= j.req.iters:
+                            self.budget.release(j.reserved)
+                            self._finish(j.req_id, st.params if j.req.keep else None)
+                        else:
+                            j.state = st
+                    active = [j for j in active if j.done < j.req.iters]
+                    batch, batch_jobs = None, []
+
+
+# ------------------------------------------------------------------ workload
+@dataclass
+class WorkloadStats:
+    n_render: int = 0
+    n_fit: int = 0
+    render_latency_ms: List[float] = field(default_factory=list)
+    render_2048_latency_ms: List[float] = field(default_factory=list)
+    fit_latency_s: List[float] = field(default_factory=list)
+    unfinished: int = 0
+    wall_s: float = 0.0
+
+
+def percentile(xs: List[float], q: float) -> float:
+    if not xs:
+        return float("nan")
+    s = sorted(xs)
+    k = min(len(s) - 1, max(0, int(math.ceil(q / 100.0 * len(s))) - 1))
+    return s[k]
+
+
+def resident_sets(n_sets: int = 64, n_min: int = 100_000, n_max: int = 3_000_000,
+                  seed: int = 5000, device="cuda") -> Dict[str, GaussianSet]:
+    """Seeded stand-ins for pre-fitted sets: set k has N_k ~ U[n_min, n_max]
+    Gaussians drawn as the fit configurations draw them, on an image whose
+    side gives 0.2 Gaussians per pixel."""
+    g = torch.Generator().manual_seed(seed)
+    out = {}
+    for k in range(n_sets):
+        n = int(n_min + (n_max - n_min) * torch.rand(1, generator=g).item())
+        side = int(round(math.sqrt(n / 0.2)))
+        mu, ch, co = synthetic.gaussians(n, side, side, diag=(0.5, 4.0), seed=seed + 1 + k)
+        out[f"set{k}"] = GaussianSet(mu.to(device), ch.to(device), co.to(device), side, side)
+    return out
+
+
+def poisson_requests(duration_s: float, rate: float, fit_frac: float, sets: Dict[str, GaussianSet],
+                     fit_iters: int = 300, fit_side=(512, 4096), render_side=(256, 4096),
+                     render_scale=(0.25, 2.0), seed: int = 5000):
+    """Arrival schedule [(t, kind, params)]: Poisson arrivals; fits draw a
+    square side U[fit_side] (0.2 Gaussians per pixel, capped at 1M); renders
+    draw a set, an output side U[render_side], a scale U[render_scale] and a
+    crop origin uniform over the set's image."""
+    g = torch.Generator().manual_seed(seed)
+    u = lambda: torch.rand(1, generator=g).item()  # noqa: E731
+    names = sorted(sets)
+    t, out = 0.0, []
+    while True:
+        t += -math.log(max(1e-12, 1.0 - u())) / rate
+        if t >= duration_s:
+            return out
+        if u() < fit_frac:
+            side = int(fit_side[0] + (fit_side[1] - fit_side[0]) * u())
+            out.append((t, "fit", {"side": side, "n": min(int(round(0.2 * side * side)),
+                                                          1_000_000), "iters": fit_iters,
+                                   "seed": 6000 + len(out)}))
+        else:
+            name = names[int(u() * len(names)) % len(names)]
+            gs = sets[name]
+            side = int(render_side[0] + (render_side[1] - render_side[0]) * u())
+            s = render_scale[0] + (render_scale[1] - render_scale[0]) * u()
+            span = side / s
+            ox = u() * max(0.0, gs.W - span)
+            oy = u() * max(0.0, gs.H - span)
+            out.append((t, "render", {"set": name, "side": side, "scale": s,
+                                      "origin": (ox, oy)}))
+
+
+def run_workload(server: Server, schedule, master_target: torch.Tensor, drain_s: float = 60.0,
+                 fit_lr: float = 1e-3) -> WorkloadStats:
+    """Submit `schedule` (from poisson_requests) at its arrival times, wait up
+    to drain_s after the last arrival, abort what is left and collect
+    latencies.  Fit targets are top-left crops of master_target, copied
+    when the fit is admitted."""
+    st = WorkloadStats()
+    kinds = {}
+    t0 = time.perf_counter()
+    server.start()
+    for t, kind, p in schedule:
+        delay = t0 + t - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        if kind == "render":
+            rid = server.submit(RenderRequest(p["set"], p["side"], p["side"], p["origin"],
+                                              p["scale"], keep=False))
+            st.n_render += 1
+        else:
+            side = p["side"]
+            rid = server.submit(FitRequest(
+                lambda side=side: master_target[:side, :side], p["n"], p["iters"], lr=fit_lr,
+                seed=p["seed"], keep=False, shape=(side, side)))
+            st.n_fit += 1
+        kinds[rid] = p
+    server.drain(timeout=drain_s)
+    server.stop(abort=True)
+    st.wall_s = time.perf_counter() - t0
+    for rid, r in server.results.items():
+        if r.t_done == 0.0 or r.error:
+            st.unfinished += 1
+            continue
+        if r.kind == "render":
+            ms = 1e3 * r.latency
+            st.render_latency_ms.append(ms)
+            if 1792 <= kinds[rid]["side"] <= 2304:
+                st.render_2048_latency_ms.append(ms)
+        else:
+            st.fit_latency_s.append(r.latency)
+    return st

@@ -1,0 +1,79 @@
+"""Serving loop under a Poisson mix of renders and fits (one GPU).
+
+Workload (seeded, synthetic): 64 resident sets of 100k-3M Gaussians
+(lig_b200.serve.resident_sets, 0.2 Gaussians per pixel of the set's image);
+Poisson arrivals at --rate per second for --duration seconds, a --fit-frac
+share of fits (square target side U[512, 4096], min(0.2 side^2, 1M)
+Gaussians, --fit-iters iterations, targets cropped from one 4096^2 teacher
+render with N(0, 0.02) noise) and the rest renders (a set, output side
+U[256, 4096], scale U[0.25, 2], crop origin uniform over the set's image).
+Admission against an HBM budget (--budget-gb).  After the last arrival the
+server gets --drain seconds; what is still queued or running then is
+counted as unfinished.
+
+Prints one JSON line: counts, render p50/p99 (all, and 2048^2 +-12.5%),
+fit latency p50/p99 of finished fits, throughput, unfinished, memory peak.
+
+    python tests/perf_serving.py [--duration 60] [--rate 200] [--drain 30]
+"""
+import argparse
+import json
+import os
+import sys
+import time
+
+import torch
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+from lig_b200.fit import make_target  # noqa: E402
+from lig_b200.serve import (Server, percentile, poisson_requests, resident_sets,  # noqa: E402
+                            run_workload)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--duration", type=float, default=60.0)
+    ap.add_argument("--rate", type=float, default=200.0)
+    ap.add_argument("--fit-frac", type=float, default=0.3)
+    ap.add_argument("--fit-iters", type=int, default=300)
+    ap.add_argument("--drain", type=float, default=30.0)
+    ap.add_argument("--budget-gb", type=float, default=150.0)
+    ap.add_argument("--sets", type=int, default=64)
+    ap.add_argument("--fit-chunk", type=int, default=20)
+    a = ap.parse_args()
+    t0 = time.time()
+    sets = resident_sets(a.sets)
+    master = make_target(4096, 4096, int(round(20000 / 512**2 * 4096**2)), (0.5, 4.0),
+                         noise="white", noise_std=0.02)
+    schedule = poisson_requests(a.duration, a.rate, a.fit_frac, sets, fit_iters=a.fit_iters,
+                                seed=5000)
+    srv = Server(budget_bytes=int(a.budget_gb * 1e9), fit_chunk=a.fit_chunk)
+    for k, gs in sets.items():
+        srv.add_set(k, gs)
+    # warm the render path (library load, allocator) before the clock starts
+    from lig_b200.serve import render_view
+    render_view(next(iter(sets.values())), 256, 256)
+    torch.cuda.synchronize()
+    setup = time.time() - t0
+    st = run_workload(srv, schedule, master, drain_s=a.drain)
+    r, r2, f = st.render_latency_ms, st.render_2048_latency_ms, st.fit_latency_s
+    out = {
+        "workload": "serving loop", "duration_s": a.duration, "rate": a.rate,
+        "fit_frac": a.fit_frac, "fit_iters": a.fit_iters, "drain_s": a.drain,
+        "setup_s": round(setup, 1), "wall_s": round(st.wall_s, 1),
+        "requests": {"render": st.n_render, "fit": st.n_fit},
+        "finished": {"render": len(r), "fit": len(f)}, "unfinished": st.unfinished,
+        "render_ms": {"p50": percentile(r, 50), "p99": percentile(r, 99), "n": len(r)},
+        "render_2048_ms": {"p50": percentile(r2, 50), "p99": percentile(r2, 99), "n": len(r2)},
+        "fit_s": {"p50": percentile(f, 50), "p99": percentile(f, 99), "n": len(f)},
+        "throughput_per_s": {"render": len(r) / st.wall_s, "fit": len(f) / st.wall_s},
+        "fit_batches": srv.fit_batches, "budget_peak_gb": srv.budget.peak / 1e9,
+        "errors": srv.errors[:5],
+    }
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()
