@@ -10,8 +10,9 @@ in for the DIV2K/STimage images (not available offline).
 
   value  device-timed iterations/s, target resident in HBM (inputs > L2).
   e2e    same loop through the public API with the step's input (the target
-         image) copied host->device from pinned memory and the loss read
-         back every step.
+         image) copied host->device from pinned memory every step (double
+         buffered on a copy stream, overlapping the previous step) and the
+         loss copied back to pinned host memory every step.
   roofline  the dominant kernel's algorithmic rate (reference-defined
          Gaussian-pixel evaluations x FLOP per evaluation) / measured FP32
          FMA peak of this device.
@@ -48,6 +49,11 @@ N_TEACHER = 2_000_000
 DIAG = (0.5, 6.0)
 BLOCK = 16
 FLOP_PER_EVAL = {"lig_raster_fwd": 20.0, "lig_raster_bwd": 40.0, "lig_raster_bwd_l2": 40.0}
+# DRAM bytes (read + write) per launch measured by an ncu capture of the same
+# kernels on the 2048^2 / 125k-Gaussian step (same density); traffic grows
+# with pixels and Gaussians, so a size-S launch is scaled by (S / 2048)^2.
+DRAM_BYTES_2048 = {"lig_raster_fwd": 9.189632e6 + 30.830080e6,
+                   "lig_raster_bwd_l2": 133.883392e6 + 4.826112e6}
 CLOCK_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -253,20 +259,41 @@ def run_lig(args, rank, world, local_rank):
     per = kt.summary()
     clk = clocks.summary()
 
-    # ---- end-to-end loop through the public API with host buffers
+    # ---- end-to-end loop through the public API with host buffers: every
+    # step uploads its target from pinned host memory (double-buffered on a
+    # copy stream, so step k+1's upload overlaps step k's kernels) and copies
+    # its loss back to pinned host memory; the losses are read at the end.
     host_target = target.cpu().pin_memory()
-    dev_target = torch.empty_like(target)
+    bufs = [torch.empty_like(target), torch.empty_like(target)]
+    host_loss = torch.empty(args.steps, dtype=torch.float32, pin_memory=True)
+    copy_stream = torch.cuda.Stream(dev)
+    ready = [torch.cuda.Event(), torch.cuda.Event()]
+    consumed = [torch.cuda.Event(), torch.cuda.Event()]
+    cur = torch.cuda.current_stream(dev)
     barrier()
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    for _ in range(args.steps):
-        dev_target.copy_(host_target, non_blocking=True)
-        loss = fit.step(dev_target)
-        _ = loss.item()
+    copy_stream.wait_stream(cur)
+    with torch.cuda.stream(copy_stream):
+        bufs[0].copy_(host_target, non_blocking=True)
+        ready[0].record(copy_stream)
+    for k in range(args.steps):
+        b = k % 2
+        if k + 1 < args.steps:
+            nb = (k + 1) % 2
+            with torch.cuda.stream(copy_stream):
+                if k >= 1:
+                    copy_stream.wait_event(consumed[nb])  # step k-1 is done with it
+                bufs[nb].copy_(host_target, non_blocking=True)
+                ready[nb].record(copy_stream)
+        cur.wait_event(ready[b])
+        loss = fit.step(bufs[b])
+        consumed[b].record(cur)
+        host_loss[k].copy_(loss, non_blocking=True)
     e1.record()
     torch.cuda.synchronize()
+    assert bool(torch.isfinite(host_loss).all())
     barrier()
     e2e_ms = torch.tensor([e0.elapsed_time(e1)], device=dev)
     if world > 1:
@@ -289,8 +316,12 @@ def run_lig(args, rank, world, local_rank):
     dk = kernels[dom]
     if dom in FLOP_PER_EVAL:
         achieved = FLOP_PER_EVAL[dom] * evals / (dk["ms_per_call"] / 1e3) / 1e12
+        traffic = None
+        if dom in DRAM_BYTES_2048:
+            traffic = DRAM_BYTES_2048[dom] * (size / 2048) ** 2
         roof = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak / 1e12,
-                "unit": "TFLOP/s", "frac": achieved * 1e12 / fp32_peak, "traffic": None,
+                "unit": "TFLOP/s", "frac": achieved * 1e12 / fp32_peak, "traffic": traffic,
+                "traffic_note": "ncu dram bytes of the 2048^2 capture x (size/2048)^2",
                 "kernel": dom, "per_launch_units": evals,
                 "note": "algorithmic = reference Gaussian-pixel evaluations x FLOP/eval "
                         f"({FLOP_PER_EVAL[dom]:.0f}); peak = FP32 FMA probe measured on this "

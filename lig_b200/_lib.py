@@ -76,6 +76,8 @@ SIGNATURES = {
     "lig_adam_scratch_bytes": (SZ, []),
     "lig_adam_step": (I, [I64, P, P, P, P, D, D, D, D, P, P, P, P, P]),
     "lig_adam_batch_scratch_bytes": (SZ, [I]),
+    "lig_level_residual": (I, [I64, P, P, P, P, P]),
+    "lig_level_compose": (I, [I, I, P, I, I, P, P, D, D, I, I, P, P]),
     "lig_project_fwd_view": (I, [I, I, I, P, P, P, I, I, I, D, D, D, D, P, P, P, P, P]),
     "lig_adam_step_batch": (I, [I, P, P, P, P, P, D, D, D, D, P, P, P, P, SZ, P]),
 }

@@ -32,13 +32,25 @@ l2_partial_kernel(int64_t n, const T *__restrict__ img, const T *__restrict__ ta
     }
 }
 
+// Sum of partials[k0, k1) by one warp in a fixed order (lane-strided
+// sums, then a butterfly): deterministic, and the same for the single-image
+// and the batched reduction.
+__device__ __forceinline__ double warp_sum_range(const double *__restrict__ partials, int k0,
+                                                 int k1) {
+    const int lane = threadIdx.x & 31;
+    double t = 0;
+    for (int k = k0 + lane; k < k1; k += 32) t += partials[k];
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    return t;
+}
+
 template <typename T>
 __global__ void l2_final_kernel(int nblocks, int64_t n, const double *__restrict__ partials,
                                 T *__restrict__ out) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double t = 0;
-    for (int k = 0; k < nblocks; ++k) t += partials[k];
-    *out = (T)(t / (double)n);
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+    const double t = warp_sum_range(partials, 0, nblocks);
+    if (threadIdx.x == 0) *out = (T)(t / (double)n);
 }
 
 inline int loss_blocks() { return 148 * 8; }
@@ -86,19 +98,28 @@ l2_partial_batch_kernel(const LossSplit sp, const T *__restrict__ img,
     }
 }
 
+// One block of 32 warps: warp w reduces images w, w + 32, ...; thread 0
+// then adds the per-image means in image order.
 template <typename T>
-__global__ void l2_final_batch_kernel(const LossSplit sp, const double *__restrict__ partials,
-                                      T *__restrict__ out, T *__restrict__ per_image) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double total = 0;
-    for (int im = 0; im < sp.n_img; ++im) {
-        double t = 0;
-        for (int k = sp.blk_off[im]; k < sp.blk_off[im + 1]; ++k) t += partials[k];
-        const double m = t / (double)(sp.elem_off[im + 1] - sp.elem_off[im]);
-        if (per_image) per_image[im] = (T)m;
-        total += m;
+__global__ void __launch_bounds__(1024)
+l2_final_batch_kernel(const LossSplit sp, const double *__restrict__ partials,
+                      T *__restrict__ out, T *__restrict__ per_image) {
+    __shared__ double s_mean[kMaxBatch];
+    const int w = threadIdx.x >> 5;
+    for (int im = w; im < sp.n_img; im += 32) {
+        const double t = warp_sum_range(partials, sp.blk_off[im], sp.blk_off[im + 1]);
+        if ((threadIdx.x & 31) == 0) {
+            const double m = t / (double)(sp.elem_off[im + 1] - sp.elem_off[im]);
+            s_mean[im] = m;
+            if (per_image) per_image[im] = (T)m;
+        }
     }
-    *out = (T)total;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double total = 0;
+        for (int im = 0; im < sp.n_img; ++im) total += s_mean[im];
+        *out = (T)total;
+    }
 }
 
 inline bool make_split(int n_img, const int32_t *h, const int32_t *w, LossSplit &sp) {
@@ -168,12 +189,13 @@ extern "C" int lig_l2_clamped_loss_batch(int dtype, int n_img, const int32_t *he
     if (dtype == LIG_F32) {
         l2_partial_batch_kernel<float><<<nb, kLossThreads, 0, s>>>(sp, (const float *)img,
                                                                    (const float *)target, part);
-        l2_final_batch_kernel<float><<<1, 32, 0, s>>>(sp, part, (float *)loss, (float *)per_image);
+        l2_final_batch_kernel<float><<<1, 1024, 0, s>>>(sp, part, (float *)loss,
+                                                        (float *)per_image);
     } else if (dtype == LIG_F64) {
         l2_partial_batch_kernel<double><<<nb, kLossThreads, 0, s>>>(sp, (const double *)img,
                                                                     (const double *)target, part);
-        l2_final_batch_kernel<double><<<1, 32, 0, s>>>(sp, part, (double *)loss,
-                                                       (double *)per_image);
+        l2_final_batch_kernel<double><<<1, 1024, 0, s>>>(sp, part, (double *)loss,
+                                                         (double *)per_image);
     } else {
         return LIG_ERR_INVALID;
     }

@@ -15,7 +15,8 @@
 //
 // Update rule: Adam (Kingma & Ba, "Adam: A Method for Stochastic
 // Optimization", Algorithm 1) with the bias corrections folded as
-// p -= (lr / (1 - b1^t)) * m / (sqrt(v) / sqrt(1 - b2^t) + eps).
+// p -= (lr / (1 - b1^t)) * m / (sqrt(v) / sqrt(1 - b2^t) + eps), the form of
+// torch.optim.Adam's update (which the fit loops used before).
 #include "common.cuh"
 
 namespace lig {
@@ -26,6 +27,17 @@ struct AdamScalars {
     int skip;            // 1: leave everything unchanged
     int pad;
 };
+
+// One element, in the form torch.optim.Adam evaluates it: m = lerp(m, g,
+// 1 - b1), v = v b2 + (1 - b2) g g, p -= step_size * m / (sqrt(v) / bc2 +
+// eps), with correctly rounded square root and divisions.
+__device__ __forceinline__ void adam_update(float &p, float g, float &m, float &v, float b1,
+                                            float b2, float eps, const AdamScalars &a) {
+    m = __fadd_rn(m, __fmul_rn(__fsub_rn(1.f, b1), __fsub_rn(g, m)));
+    v = __fadd_rn(__fmul_rn(v, b2), __fmul_rn(__fmul_rn(__fsub_rn(1.f, b2), g), g));
+    const float den = __fadd_rn(__fdiv_rn(__fsqrt_rn(v), a.bc2_sqrt), eps);
+    p = __fsub_rn(p, __fmul_rn(a.step_size, __fdiv_rn(m, den)));
+}
 
 __global__ void adam_prologue_kernel(const int32_t *__restrict__ status, int32_t *step,
                                      int32_t *skipped, double lr, double b1, double b2,
@@ -60,21 +72,14 @@ adam_kernel(int64_t n, float *__restrict__ p, const float *__restrict__ g,
         float4 pp = p4[i], gg = g4[i], mm = m4[i], vv = v4[i];
         float *pe = &pp.x, *ge = &gg.x, *me = &mm.x, *ve = &vv.x;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            me[k] = b1 * me[k] + (1.f - b1) * ge[k];
-            ve[k] = b2 * ve[k] + (1.f - b2) * ge[k] * ge[k];
-            pe[k] -= a.step_size * me[k] / (sqrtf(ve[k]) / a.bc2_sqrt + eps);
-        }
+        for (int k = 0; k < 4; ++k) adam_update(pe[k], ge[k], me[k], ve[k], b1, b2, eps, a);
         p4[i] = pp; m4[i] = mm; v4[i] = vv;
     }
     for (int64_t i = n4 * 4 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += stride) {
-        const float gi = g[i];
-        const float mi = b1 * m[i] + (1.f - b1) * gi;
-        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
-        m[i] = mi;
-        v[i] = vi;
-        p[i] -= a.step_size * mi / (sqrtf(vi) / a.bc2_sqrt + eps);
+        float pi = p[i], mi = m[i], vi = v[i];
+        adam_update(pi, g[i], mi, vi, b1, b2, eps, a);
+        p[i] = pi; m[i] = mi; v[i] = vi;
     }
 }
 
@@ -120,12 +125,9 @@ adam_batch_kernel(AdamBatch ab, float *__restrict__ p, const float *__restrict__
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const AdamScalars a = sc[elem_image(ab, i)];
-        const float gi = g[i];
-        const float mi = b1 * m[i] + (1.f - b1) * gi;
-        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
-        m[i] = mi;
-        v[i] = vi;
-        p[i] -= a.step_size * mi / (sqrtf(vi) / a.bc2_sqrt + eps);
+        float pi = p[i], mi = m[i], vi = v[i];
+        adam_update(pi, g[i], mi, vi, b1, b2, eps, a);
+        p[i] = pi; m[i] = mi; v[i] = vi;
     }
 }
 
