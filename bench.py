@@ -220,6 +220,16 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def job_rate(ms_local: float, steps: int, world: int, device) -> tuple:
+    """Whole-job throughput: the slowest rank's time (max over ranks of the
+    device-timed milliseconds) and world * steps units over it."""
+    t = torch.tensor([ms_local], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    return world * steps / (ms_max / 1e3), ms_max
+
+
 # -------------------------------------------------------------- GPU side
 def run_lig(args, rank, world, local_rank):
     from lig_b200 import _lib, ops
@@ -250,12 +260,7 @@ def run_lig(args, rank, world, local_rank):
         torch.cuda.synchronize()
     barrier()
     launches = (_lib.lib.lig_kernel_launches() - l0) / args.steps
-    ms = start.elapsed_time(end)
-    ms_t = torch.tensor([ms], device=dev)
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    value = world * args.steps / (ms_max / 1e3)
+    value, ms_max = job_rate(start.elapsed_time(end), args.steps, world, dev)
     per = kt.summary()
     clk = clocks.summary()
 
@@ -295,10 +300,7 @@ def run_lig(args, rank, world, local_rank):
     torch.cuda.synchronize()
     assert bool(torch.isfinite(host_loss).all())
     barrier()
-    e2e_ms = torch.tensor([e0.elapsed_time(e1)], device=dev)
-    if world > 1:
-        dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
-    e2e = world * args.steps / (float(e2e_ms.item()) / 1e3)
+    e2e, _ = job_rate(e0.elapsed_time(e1), args.steps, world, dev)
 
     if rank != 0:
         return
