@@ -174,6 +174,33 @@ int lig_raster_bwd_l2(int dtype, int img_h, int img_w, int block_width, int num_
                       void *v_xy_abs, void *v_conic, void *v_rgb, void *v_opacity,
                       void *stream);
 
+/* Bytes of the per-tile loss partials of lig_raster_fwd_l2 (num_tiles
+ * doubles; for the batched entry the batch's total tile count). */
+size_t lig_l2_tile_partials_bytes(int num_tiles);
+
+/* Fit-loop forward with the clamped-L2 loss fused in: the tile lists are
+ * rendered as lig_raster_fwd, but per pixel `diff` [H,W,3] receives
+ * (0 <= x <= 1) ? clamp(x, 0, 1) - target : 0 instead of the image x, and
+ * *loss = mean((clamp(x, 0, 1) - target)^2) (gaussianlig.py:95-102) is reduced
+ * deterministically from per-tile fp64 partials.  final_idx as
+ * lig_raster_fwd.  Workspace: lig_raster_workspace_bytes. */
+int lig_raster_fwd_l2(int dtype, int img_h, int img_w, int block_width, int num_points,
+                      const int32_t *gaussian_ids_sorted, const int32_t *tile_bins,
+                      const int32_t *num_intersects, const void *xys, const void *conics,
+                      const void *colors, const void *opacities, const void *target,
+                      void *workspace, size_t workspace_bytes, double *tile_partials,
+                      void *diff, int32_t *final_idx, void *loss, void *stream);
+
+/* Sum backward of that loss from the forward's diff: pixel cotangent
+ * diff * 2 / (3 H W) * grad_loss (equal to lig_raster_bwd_l2's). */
+int lig_raster_bwd_diff(int dtype, int img_h, int img_w, int block_width, int num_points,
+                        const int32_t *gaussian_ids_sorted, const int32_t *tile_bins,
+                        const int32_t *num_intersects, const void *xys, const void *conics,
+                        const void *colors, const void *opacities, const int32_t *final_idx,
+                        const void *diff, const void *grad_loss, double alpha_clamp,
+                        void *workspace, size_t workspace_bytes, void *v_xy, void *v_xy_abs,
+                        void *v_conic, void *v_colors, void *v_opacity, void *stream);
+
 /* Workspace bytes of lig_l2_clamped_loss. */
 size_t lig_l2_workspace_bytes(void);
 
@@ -301,6 +328,28 @@ int lig_raster_bwd_l2_batch(int dtype, int n_img, const int32_t *heights, const 
                             void *v_xy_abs, void *v_conic, void *v_colors, void *v_opacity,
                             void *stream);
 
+/* Batched lig_raster_fwd_l2: loss = sum_i mean_i(...), per_image[i] the
+ * image's mean (may be NULL); tile_partials holds the batch's total tiles. */
+int lig_raster_fwd_l2_batch(int dtype, int n_img, const int32_t *heights, const int32_t *widths,
+                            const int32_t *counts, int block_width,
+                            const int32_t *gaussian_ids_sorted, const int32_t *tile_bins,
+                            const int32_t *num_intersects, const int32_t *cum, const void *xys,
+                            const void *conics, const void *colors, const void *opacities,
+                            const void *target, int persistent, int32_t *work, void *workspace,
+                            size_t workspace_bytes, double *tile_partials, void *diff,
+                            int32_t *final_idx, void *loss, void *per_image, void *stream);
+
+/* Batched lig_raster_bwd_diff (per-image scale 2 / (3 H_i W_i)). */
+int lig_raster_bwd_diff_batch(int dtype, int n_img, const int32_t *heights,
+                              const int32_t *widths, const int32_t *counts, int block_width,
+                              const int32_t *gaussian_ids_sorted, const int32_t *tile_bins,
+                              const int32_t *num_intersects, const int32_t *cum, const void *xys,
+                              const void *conics, const void *colors, const void *opacities,
+                              const int32_t *final_idx, const void *diff, const void *grad_loss,
+                              double alpha_clamp, int persistent, int32_t *work, void *workspace,
+                              size_t workspace_bytes, void *v_xy, void *v_xy_abs, void *v_conic,
+                              void *v_colors, void *v_opacity, void *stream);
+
 /* Workspace bytes of lig_l2_clamped_loss_batch. */
 size_t lig_l2_batch_workspace_bytes(int n_img);
 
@@ -311,6 +360,27 @@ int lig_l2_clamped_loss_batch(int dtype, int n_img, const int32_t *heights,
                               const int32_t *widths, const void *img, const void *target,
                               void *loss, void *per_image, void *workspace,
                               size_t workspace_bytes, void *stream);
+
+/* ---------------------------------------------------------- level pipeline */
+
+/* Residual target of the next level (train.py:113-126): with
+ * r = gt - up + 0.5 over n floats, out = (r - min r) / (max r - min r) and
+ * minmax[0..1] = (min r, max r) (device floats; the level's store_min /
+ * store_max).  Bit-identical to the torch expression on NaN-free inputs. */
+int lig_level_residual(int64_t n, const float *gt, const float *up, float *out, float *minmax,
+                       void *stream);
+
+/* One level of a multi-level decode (train.py:188-200): out[H,W,3] =
+ * base + (r * (max - min) - 0.5 + min), r = render (clamped to [0,1] when
+ * clamp_render), base = prev [prev_h, prev_w, 3] resized to H x W by
+ * bilinear half-pixel sampling (F.interpolate mode='bilinear'), or prev itself
+ * when the sizes agree, or 0 when prev is NULL; (min, max) from minmax
+ * (device floats) when given, else store_min / store_max; clamp_out clamps
+ * the result to [0, 1]. */
+int lig_level_compose(int prev_h, int prev_w, const float *prev, int H, int W,
+                      const float *render, const float *minmax, double store_min,
+                      double store_max, int clamp_render, int clamp_out, float *out,
+                      void *stream);
 
 /* -------------------------------------------------------------- optimiser */
 

@@ -73,6 +73,14 @@ SIGNATURES = {
                                     P, P, SZ, P, P, P, P, P, P]),
     "lig_l2_batch_workspace_bytes": (SZ, [I]),
     "lig_l2_clamped_loss_batch": (I, [I, I, P, P, P, P, P, P, P, SZ, P]),
+    "lig_l2_tile_partials_bytes": (SZ, [I]),
+    "lig_raster_fwd_l2": (I, [I, I, I, I, I, P, P, P, P, P, P, P, P, P, SZ, P, P, P, P, P]),
+    "lig_raster_bwd_diff": (I, [I, I, I, I, I, P, P, P, P, P, P, P, P, P, P, D, P, SZ, P, P, P,
+                                P, P, P]),
+    "lig_raster_fwd_l2_batch": (I, [I, I, P, P, P, I, P, P, P, P, P, P, P, P, P, I, P, P, SZ,
+                                    P, P, P, P, P, P]),
+    "lig_raster_bwd_diff_batch": (I, [I, I, P, P, P, I, P, P, P, P, P, P, P, P, P, P, P, D, I,
+                                      P, P, SZ, P, P, P, P, P, P]),
     "lig_adam_scratch_bytes": (SZ, []),
     "lig_adam_step": (I, [I64, P, P, P, P, D, D, D, D, P, P, P, P, P]),
     "lig_adam_batch_scratch_bytes": (SZ, [I]),

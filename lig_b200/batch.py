@@ -13,8 +13,9 @@ backward launch per image.  Here every image of a batch shares each launch:
 * projection, prefix sum, emission + one stable radix sort over the batch's
   flattened tile keys, the forward rasterizer over the flattened
   (image, tile) work list (optionally persistent: CTAs pull work items from a
-  counter), the per-image clamped-L2 loss, the fused L2 backward and one
-  guarded Adam step — no host synchronisation anywhere;
+  counter) with the per-image clamped-L2 loss fused in, the backward from the
+  forward's masked difference and one guarded Adam step — no host
+  synchronisation anywhere;
 * the intersection capacity is fixed when the iteration is captured; a step
   whose binning overflows it is skipped on the device (lig_adam_step's
   guard) and counted, and the host grows the capacity, re-captures and redoes
@@ -195,8 +196,7 @@ class BatchedFit:
         self.fin = torch.empty(P, dtype=i32, **kw)
         self.loss = torch.zeros((), dtype=f32, **kw)
         self.per_image = torch.zeros(L.n, dtype=f32, **kw)
-        self.l_ws = torch.empty(_lib.lib.lig_l2_batch_workspace_bytes(L.n), dtype=torch.uint8,
-                                **kw)
+        self.partials = torch.empty(max(L.tiles, 1), dtype=torch.float64, **kw)
         self.r_ws = torch.empty(_lib.lib.lig_raster_workspace_bytes(_lib.LIG_F32, N),
                                 dtype=torch.uint8, **kw)
         self.v_xy = torch.empty(N, 2, dtype=f32, **kw)
@@ -263,29 +263,38 @@ class BatchedFit:
         self.graph = None
 
     # -------------------------------------------------------- the iteration
-    def _render(self, st):
-        """Projection, binning and the forward rasterizer (into self.img)."""
+    def _bin(self, st):
         L = self.L
         self._project(st)
         call("lig_bin_batch", _lib.LIG_F32, *L.args(), L.block, _p(self.xys), _p(self.ext),
              _p(self.cum), _p(self.total), self.capacity, _p(self.bin_ws), self.bin_ws.numel(),
              _p(self.gids), _p(self.bins), _p(self.status), st)
+
+    def _render(self, st):
+        """Projection, binning and the forward rasterizer (render into self.img)."""
+        L = self.L
+        self._bin(st)
         call("lig_raster_fwd_batch", _lib.LIG_F32, *L.args(), L.block, _p(self.gids),
              _p(self.bins), _p(self.total), _p(self.cum), _p(self.xys), _p(self.con),
              _p(self.rgbs), None, int(self.persistent), _p(self.work), _p(self.r_ws),
              self.r_ws.numel(), _p(self.img), _p(self.wsum), None, None, None, _p(self.fin), st)
 
     def _enqueue_step(self):
+        """Forward with the loss fused in (self.img receives the masked
+        difference clamp(x) - target, self.loss / self.per_image the losses),
+        the backward from that difference, the projection backward and Adam."""
         L = self.L
         st = self._stream()
-        self._render(st)
-        call("lig_l2_clamped_loss_batch", _lib.LIG_F32, *L.hw_args(), _p(self.img),
-             _p(self.target), _p(self.loss), _p(self.per_image), _p(self.l_ws),
-             self.l_ws.numel(), st)
-        call("lig_raster_bwd_l2_batch", _lib.LIG_F32, *L.args(), L.block, _p(self.gids),
+        self._bin(st)
+        call("lig_raster_fwd_l2_batch", _lib.LIG_F32, *L.args(), L.block, _p(self.gids),
              _p(self.bins), _p(self.total), _p(self.cum), _p(self.xys), _p(self.con),
-             _p(self.rgbs), None, _p(self.fin), _p(self.img), _p(self.target), _p(self.one),
-             0.0, int(self.persistent), _p(self.work), _p(self.r_ws), self.r_ws.numel(),
+             _p(self.rgbs), None, _p(self.target), int(self.persistent), _p(self.work),
+             _p(self.r_ws), self.r_ws.numel(), _p(self.partials), _p(self.img), _p(self.fin),
+             _p(self.loss), _p(self.per_image), st)
+        call("lig_raster_bwd_diff_batch", _lib.LIG_F32, *L.args(), L.block, _p(self.gids),
+             _p(self.bins), _p(self.total), _p(self.cum), _p(self.xys), _p(self.con),
+             _p(self.rgbs), None, _p(self.fin), _p(self.img), _p(self.one), 0.0,
+             int(self.persistent), _p(self.work), _p(self.r_ws), self.r_ws.numel(),
              _p(self.v_xy), _p(self.v_abs), _p(self.v_con), _p(self.g_rgbs), None, st)
         call("lig_project_bwd_batch", _lib.LIG_F32, *L.args(), 1, _p(self.chol), _p(self.means),
              None, L.block, _p(self.v_xy), 2, _p(self.v_con), 3, _p(self.g_chol),

@@ -313,6 +313,71 @@ struct FwdAcc {
     }
 };
 
+// Fused clamped-L2 loss in the forward (fit loops): instead of the image the
+// forward writes the masked difference diff = (0 <= x <= 1) ? clamp(x) - t : 0
+// (what the loss gradient needs per pixel) and each tile adds
+// (clamp(x) - t)^2 over its pixels into one fp64 partial (fixed-order block
+// reduction, so the loss is deterministic).  target == null: plain forward.
+template <typename T> struct L2Fwd {
+    const T *target;
+    double *tile_partial;  // [total tiles]
+};
+
+template <typename T>
+__device__ __forceinline__ void block_sum_to(double v, double *dst) {
+    __shared__ double s_part[32];
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) s_part[w] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += s_part[k];
+        *dst = t;
+    }
+    __syncthreads();
+}
+
+// Writes one pixel's forward outputs (or, in the fused-L2 mode, its masked
+// difference and the tile's loss partial; every thread of the CTA calls it).
+template <typename T, bool GA>
+__device__ __forceinline__ void fwd_store(const FwdAcc<T, GA> &acc, bool inside, int pix,
+                                          T *__restrict__ img, T *__restrict__ wsum,
+                                          T *__restrict__ odx, T *__restrict__ ody,
+                                          T *__restrict__ odxy, int32_t *__restrict__ final_idx,
+                                          const L2Fwd<T> &l2, int tile) {
+    if (l2.target) {
+        double sq = 0;
+        if (inside) {
+            final_idx[pix] = acc.cur;
+            const T x[3] = {acc.r, acc.g, acc.b};
+#pragma unroll
+            for (int ch = 0; ch < 3; ++ch) {
+                const T d = min(max(x[ch], (T)0), (T)1) - l2.target[3 * pix + ch];
+                sq += (double)(d * d);
+                img[3 * pix + ch] = (x[ch] >= (T)0 && x[ch] <= (T)1) ? d : (T)0;
+            }
+        }
+        block_sum_to<T>(sq, l2.tile_partial + tile);
+        return;
+    }
+    if (!inside) return;
+    final_idx[pix] = acc.cur;
+    img[3 * pix] = acc.r;
+    img[3 * pix + 1] = acc.g;
+    img[3 * pix + 2] = acc.b;
+    wsum[pix] = acc.w;
+    if (GA) {
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch) {
+            odx[3 * pix + ch] = acc.dx[ch];
+            ody[3 * pix + ch] = acc.dy[ch];
+            odxy[3 * pix + ch] = acc.dxy[ch];
+        }
+    }
+}
+
 template <typename T, bool GA>
 __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int32_t *__restrict__ ids,
                                          const int2 *__restrict__ tile_bins,
@@ -320,7 +385,7 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
                                          T *__restrict__ wsum, T *__restrict__ odx,
                                          T *__restrict__ ody, T *__restrict__ odxy,
                                          int32_t *__restrict__ final_idx, Rec<T> *s_rec,
-                                         uint32_t *s_bits) {
+                                         uint32_t *s_bits, const L2Fwd<T> &l2) {
     const int nt = blockDim.x;
     const unsigned FULL = 0xffffffffu;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -333,21 +398,14 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
     const int pix = tc.poff + gy * tc.W + gx;
     const T px = (T)gx + (T)0.5, py = (T)gy + (T)0.5;
 
+    FwdAcc<T, GA> acc;
     if (tc.empty) {  // the reference's empty-list branch (rasterize.py:80-90)
-        if (inside) {
-            img[3 * pix] = (T)1; img[3 * pix + 1] = (T)1; img[3 * pix + 2] = (T)1;
-            wsum[pix] = 0;
-            final_idx[pix] = 0;
-            if (GA) {
-#pragma unroll
-                for (int ch = 0; ch < 3; ++ch) { odx[3 * pix + ch] = 0; ody[3 * pix + ch] = 0; odxy[3 * pix + ch] = 0; }
-            }
-        }
+        acc.r = acc.g = acc.b = (T)1;
+        fwd_store<T, GA>(acc, inside, pix, img, wsum, odx, ody, odxy, final_idx, l2, tile);
         return;
     }
 
     const int2 range = tile_bins[tile];
-    FwdAcc<T, GA> acc;
     Rec<T> pre;
     if (range.x + tid < range.y) pre = recs[__ldg(ids + range.x + tid)];
     for (int base = range.x; base < range.y; base += nt) {
@@ -382,21 +440,7 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
             }
         }
     }
-    if (inside) {
-        final_idx[pix] = acc.cur;
-        img[3 * pix] = acc.r;
-        img[3 * pix + 1] = acc.g;
-        img[3 * pix + 2] = acc.b;
-        wsum[pix] = acc.w;
-        if (GA) {
-#pragma unroll
-            for (int ch = 0; ch < 3; ++ch) {
-                odx[3 * pix + ch] = acc.dx[ch];
-                ody[3 * pix + ch] = acc.dy[ch];
-                odxy[3 * pix + ch] = acc.dxy[ch];
-            }
-        }
-    }
+    fwd_store<T, GA>(acc, inside, pix, img, wsum, odx, ody, odxy, final_idx, l2, tile);
 }
 
 template <typename T, bool GA>
@@ -405,7 +449,8 @@ raster_fwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work
                   const int32_t *__restrict__ ids, const int2 *__restrict__ tile_bins,
                   const int32_t *__restrict__ d_total, const Rec<T> *__restrict__ recs,
                   T *__restrict__ img, T *__restrict__ wsum, T *__restrict__ odx,
-                  T *__restrict__ ody, T *__restrict__ odxy, int32_t *__restrict__ final_idx) {
+                  T *__restrict__ ody, T *__restrict__ odxy, int32_t *__restrict__ final_idx,
+                  L2Fwd<T> l2) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_slot;
     Rec<T> *s_rec = reinterpret_cast<Rec<T> *>(smem_raw);
@@ -415,7 +460,36 @@ raster_fwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work
          tile = next_tile(work, s_slot, false)) {
         const TileCtx tc = tile_ctx(geo, cum, d_total, tile);
         fwd_tile<T, GA>(tc, tile, ids, tile_bins, recs, img, wsum, odx, ody, odxy, final_idx,
-                        s_rec, s_bits);
+                        s_rec, s_bits, l2);
+    }
+}
+
+// Loss from the tile partials: image i's mean = (sum of its tiles' partials)
+// / (3 H_i W_i), summed over images.  Warp w reduces images w, w + 32, ...
+// (lane-strided, then a butterfly: fixed order), thread 0 adds the means in
+// image order.
+template <typename T>
+__global__ void __launch_bounds__(1024)
+l2_tiles_final_kernel(const BatchGeo geo, const double *__restrict__ partial,
+                      T *__restrict__ loss, T *__restrict__ per_image) {
+    __shared__ double s_mean[kMaxBatch];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int im = w; im < geo.n_img; im += 32) {
+        double t = 0;
+        for (int k = geo.tile_off[im] + lane; k < geo.tile_off[im + 1]; k += 32) t += partial[k];
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+        if (lane == 0) {
+            const double m = t / (3.0 * (double)geo.H[im] * (double)geo.W[im]);
+            s_mean[im] = m;
+            if (per_image) per_image[im] = (T)m;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double total = 0;
+        for (int im = 0; im < geo.n_img; ++im) total += s_mean[im];
+        *loss = (T)total;
     }
 }
 
@@ -456,6 +530,7 @@ struct CotSrc {
     const T *v_img, *v_wsum;              // explicit (v_wsum may be null: zero)
     const T *img, *target, *grad_loss;    // fused L2 (v_img == null)
     T scale;                              // 2 / numel
+    const T *diff = nullptr;              // fused L2 from the forward's masked difference
     __device__ __forceinline__ void get(int p, T &r, T &g, T &b, T &w) const {
         w = v_wsum ? v_wsum[p] : (T)0;
         if (v_img) {
@@ -465,6 +540,12 @@ struct CotSrc {
             return;
         }
         const T s = scale * *grad_loss;
+        if (diff) {
+            r = diff[3 * p] * s;
+            g = diff[3 * p + 1] * s;
+            b = diff[3 * p + 2] * s;
+            return;
+        }
         T v[3];
 #pragma unroll
         for (int ch = 0; ch < 3; ++ch) {
@@ -770,11 +851,17 @@ struct TileWalk {
     int *work = nullptr;           // persistent: global work counter; null: CTA per tile
 };
 
+// Loss outputs of the fused-L2 forward (l2.target != null).
+template <typename T> struct L2Out {
+    T *loss = nullptr, *per_image = nullptr;
+};
+
 template <typename T>
 int raster_fwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int32_t *bins,
                const int32_t *d_total, const void *xys, const void *con, const void *col,
                const void *op, void *ws, size_t ws_bytes, void *img, void *wsum, void *dx,
-               void *dy, void *dxy, int32_t *fin, cudaStream_t s) {
+               void *dy, void *dxy, int32_t *fin, cudaStream_t s,
+               L2Fwd<T> l2 = L2Fwd<T>{nullptr, nullptr}, L2Out<T> l2o = L2Out<T>{}) {
     const int n = geo.total_points();
     int rc = pack<T>(n, xys, con, col, op, ws, ws_bytes, s);
     if (rc) return rc;
@@ -794,12 +881,18 @@ int raster_fwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
     if (ga)
         raster_fwd_kernel<T, true><<<grid, nt, sm, s>>>(
             geo, walk.cum, walk.work, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws,
-            (T *)img, (T *)wsum, (T *)dx, (T *)dy, (T *)dxy, fin);
+            (T *)img, (T *)wsum, (T *)dx, (T *)dy, (T *)dxy, fin, l2);
     else
         raster_fwd_kernel<T, false><<<grid, nt, sm, s>>>(
             geo, walk.cum, walk.work, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws,
-            (T *)img, (T *)wsum, nullptr, nullptr, nullptr, fin);
-    note_launches(1);
+            (T *)img, (T *)wsum, nullptr, nullptr, nullptr, fin, l2);
+    int launches = 1;
+    if (l2.target) {
+        l2_tiles_final_kernel<T><<<1, 1024, 0, s>>>(geo, l2.tile_partial, l2o.loss,
+                                                    l2o.per_image);
+        ++launches;
+    }
+    note_launches(launches);
     LIG_LAUNCH_CHECK();
     return LIG_OK;
 }
@@ -1081,5 +1174,139 @@ extern "C" int lig_raster_bwd_l2_batch(int dtype, int n_img, const int32_t *heig
                                   nullptr, nullptr, nullptr, clamp, ws, ws_bytes, v_xy, v_abs,
                                   v_con, v_rgb, v_op, s);
     }
+    return LIG_ERR_INVALID;
+}
+
+// ------------------------------------------------------- fused-L2 forward
+// The fit loop's forward: tile lists rendered as lig_raster_fwd, but each
+// pixel stores diff = (0 <= x <= 1) ? clamp(x) - target : 0 (not the image)
+// and loss = sum_i mean_i((clamp(x) - target)^2) is reduced from per-tile
+// fp64 partials; lig_raster_bwd_diff then forms the loss gradient from diff.
+extern "C" size_t lig_l2_tile_partials_bytes(int num_tiles) {
+    return sizeof(double) * (size_t)(num_tiles > 0 ? num_tiles : 1);
+}
+
+namespace lig {
+template <typename T>
+int fwd_l2(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int32_t *bins,
+           const int32_t *d_total, const void *xys, const void *con, const void *col,
+           const void *op, const void *target, void *ws, size_t ws_bytes, double *partials,
+           void *diff, int32_t *fin, void *loss, void *per_image, cudaStream_t s) {
+    return raster_fwd<T>(geo, walk, ids, bins, d_total, xys, con, col, op, ws, ws_bytes, diff,
+                         nullptr, nullptr, nullptr, nullptr, fin, s,
+                         L2Fwd<T>{(const T *)target, partials},
+                         L2Out<T>{(T *)loss, (T *)per_image});
+}
+
+template <typename T>
+int bwd_diff(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int32_t *bins,
+             const int32_t *d_total, const void *xys, const void *con, const void *col,
+             const void *op, const int32_t *fin, const void *diff, const void *grad_loss,
+             double clamp, void *ws, size_t ws_bytes, void *v_xy, void *v_abs, void *v_con,
+             void *v_rgb, void *v_op, cudaStream_t s) {
+    // per-image scale 2 / (3 H_i W_i) is formed in the kernel
+    CotSrc<T> cot{nullptr, nullptr, nullptr, nullptr, (const T *)grad_loss, (T)0,
+                  (const T *)diff};
+    return raster_bwd<T>(geo, walk, ids, bins, d_total, xys, con, col, op, fin, cot, nullptr,
+                         nullptr, nullptr, clamp, ws, ws_bytes, v_xy, v_abs, v_con, v_rgb, v_op,
+                         s);
+}
+}  // namespace lig
+
+extern "C" int lig_raster_fwd_l2(int dtype, int H, int W, int B, int n, const int32_t *ids,
+                                 const int32_t *bins, const int32_t *d_total, const void *xys,
+                                 const void *con, const void *col, const void *op,
+                                 const void *target, void *ws, size_t ws_bytes,
+                                 double *tile_partials, void *diff, int32_t *fin, void *loss,
+                                 void *stream) {
+    if (!raster_args_ok(H, W, B, n) || !bins || !d_total || !target || !ws || !tile_partials ||
+        !diff || !fin || !loss || (n > 0 && (!xys || !con || !col)))
+        return LIG_ERR_INVALID;
+    const BatchGeo geo = BatchGeo::single(H, W, B, n);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (dtype == LIG_F32)
+        return fwd_l2<float>(geo, TileWalk{}, ids, bins, d_total, xys, con, col, op, target, ws,
+                             ws_bytes, tile_partials, diff, fin, loss, nullptr, s);
+    if (dtype == LIG_F64)
+        return fwd_l2<double>(geo, TileWalk{}, ids, bins, d_total, xys, con, col, op, target, ws,
+                              ws_bytes, tile_partials, diff, fin, loss, nullptr, s);
+    return LIG_ERR_INVALID;
+}
+
+extern "C" int lig_raster_bwd_diff(int dtype, int H, int W, int B, int n, const int32_t *ids,
+                                   const int32_t *bins, const int32_t *d_total, const void *xys,
+                                   const void *con, const void *col, const void *op,
+                                   const int32_t *fin, const void *diff, const void *grad_loss,
+                                   double clamp, void *ws, size_t ws_bytes, void *v_xy,
+                                   void *v_abs, void *v_con, void *v_rgb, void *v_op,
+                                   void *stream) {
+    if (!raster_args_ok(H, W, B, n) || !bins || !d_total || !fin || !diff || !grad_loss || !ws ||
+        (n > 0 && (!xys || !con || !col || !v_xy || !v_abs || !v_con || !v_rgb)))
+        return LIG_ERR_INVALID;
+    if (n == 0) return LIG_OK;
+    const BatchGeo geo = BatchGeo::single(H, W, B, n);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (dtype == LIG_F32)
+        return bwd_diff<float>(geo, TileWalk{}, ids, bins, d_total, xys, con, col, op, fin, diff,
+                               grad_loss, clamp, ws, ws_bytes, v_xy, v_abs, v_con, v_rgb, v_op, s);
+    if (dtype == LIG_F64)
+        return bwd_diff<double>(geo, TileWalk{}, ids, bins, d_total, xys, con, col, op, fin,
+                                diff, grad_loss, clamp, ws, ws_bytes, v_xy, v_abs, v_con, v_rgb,
+                                v_op, s);
+    return LIG_ERR_INVALID;
+}
+
+extern "C" int lig_raster_fwd_l2_batch(int dtype, int n_img, const int32_t *heights,
+                                       const int32_t *widths, const int32_t *counts, int B,
+                                       const int32_t *ids, const int32_t *bins,
+                                       const int32_t *d_total, const int32_t *cum,
+                                       const void *xys, const void *con, const void *col,
+                                       const void *op, const void *target, int persistent,
+                                       int32_t *work, void *ws, size_t ws_bytes,
+                                       double *tile_partials, void *diff, int32_t *fin,
+                                       void *loss, void *per_image, void *stream) {
+    BatchGeo geo;
+    if (!batch_geo(n_img, heights, widths, counts, B, geo)) return LIG_ERR_INVALID;
+    const int n = geo.total_points();
+    if (!bins || !d_total || !target || !ws || !tile_partials || !diff || !fin || !loss ||
+        (persistent && !work) || (n > 0 && (!xys || !con || !col || !cum)))
+        return LIG_ERR_INVALID;
+    TileWalk walk{n > 0 ? cum : nullptr, persistent ? work : nullptr};
+    cudaStream_t s = (cudaStream_t)stream;
+    if (dtype == LIG_F32)
+        return fwd_l2<float>(geo, walk, ids, bins, d_total, xys, con, col, op, target, ws,
+                             ws_bytes, tile_partials, diff, fin, loss, per_image, s);
+    if (dtype == LIG_F64)
+        return fwd_l2<double>(geo, walk, ids, bins, d_total, xys, con, col, op, target, ws,
+                              ws_bytes, tile_partials, diff, fin, loss, per_image, s);
+    return LIG_ERR_INVALID;
+}
+
+extern "C" int lig_raster_bwd_diff_batch(int dtype, int n_img, const int32_t *heights,
+                                         const int32_t *widths, const int32_t *counts, int B,
+                                         const int32_t *ids, const int32_t *bins,
+                                         const int32_t *d_total, const int32_t *cum,
+                                         const void *xys, const void *con, const void *col,
+                                         const void *op, const int32_t *fin, const void *diff,
+                                         const void *grad_loss, double clamp, int persistent,
+                                         int32_t *work, void *ws, size_t ws_bytes, void *v_xy,
+                                         void *v_abs, void *v_con, void *v_rgb, void *v_op,
+                                         void *stream) {
+    BatchGeo geo;
+    if (!batch_geo(n_img, heights, widths, counts, B, geo)) return LIG_ERR_INVALID;
+    const int n = geo.total_points();
+    if (!bins || !d_total || !fin || !diff || !grad_loss || !ws || (persistent && !work) ||
+        (n > 0 && (!xys || !con || !col || !cum || !v_xy || !v_abs || !v_con || !v_rgb)))
+        return LIG_ERR_INVALID;
+    if (n == 0) return LIG_OK;
+    TileWalk walk{cum, persistent ? work : nullptr};
+    cudaStream_t s = (cudaStream_t)stream;
+    if (dtype == LIG_F32)
+        return bwd_diff<float>(geo, walk, ids, bins, d_total, xys, con, col, op, fin, diff,
+                               grad_loss, clamp, ws, ws_bytes, v_xy, v_abs, v_con, v_rgb, v_op, s);
+    if (dtype == LIG_F64)
+        return bwd_diff<double>(geo, walk, ids, bins, d_total, xys, con, col, op, fin, diff,
+                                grad_loss, clamp, ws, ws_bytes, v_xy, v_abs, v_con, v_rgb, v_op,
+                                s);
     return LIG_ERR_INVALID;
 }

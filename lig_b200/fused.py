@@ -5,9 +5,10 @@ mean((clamp(render, 0, 1) - target)^2), the loss of gaussianlig.py:95-102
 (clamp -> loss_fn 'L2'), with the gradient flowing to the Gaussian
 parameters exactly as project_gaussians_cholesky + rasterize_gaussians +
 torch.clamp + F.mse_loss would give it — but without materialising the
-render's cotangent, the clamp mask or the unused wsum cotangent: the loss is
-one reduction kernel and its gradient is formed per pixel inside the
-rasterizer backward (lig_raster_bwd_l2).
+render, its cotangent, the clamp mask or the unused wsum cotangent: the
+forward rasterizer writes the masked difference clamp(x) - target and reduces
+the loss from per-tile partials (lig_raster_fwd_l2), and the backward forms
+the pixel cotangent from that difference (lig_raster_bwd_diff).
 """
 from __future__ import annotations
 
@@ -23,30 +24,29 @@ class _RenderL2(Function):
     @staticmethod
     def forward(ctx, chol, means, colors, opacities, target, H, W, block, alpha_clamp):
         xys, ext, con, cnt = ops.project_fwd(chol, means, opacities, H, W, block, True)
+        target = target.reshape(H, W, 3)
 
         def enqueue(b):
-            return ops.raster_fwd(H, W, block, b.gaussian_ids_sorted, b.tile_bins, b.total, xys,
-                                  con, colors, opacities, False)
+            return ops.raster_fwd_l2(H, W, block, b.gaussian_ids_sorted, b.tile_bins, b.total,
+                                     xys, con, colors, opacities, target)
 
-        binning, (img, wsum, _, _, _, fin) = ops.bin_gaussians(xys, ext, cnt, H, W, block,
-                                                               after_enqueue=enqueue)
-        target = target.reshape(img.shape)
-        loss = ops.l2_clamped_loss(img, target)
+        binning, (diff, fin, loss) = ops.bin_gaussians(xys, ext, cnt, H, W, block,
+                                                       after_enqueue=enqueue)
         ctx.geom = (H, W, block)
         ctx.alpha_clamp = alpha_clamp
-        ctx.save_for_backward(chol, means, colors, opacities, target, binning.gaussian_ids_sorted,
-                              binning.tile_bins, binning.total, xys, con, img, fin)
+        ctx.save_for_backward(chol, means, colors, opacities, binning.gaussian_ids_sorted,
+                              binning.tile_bins, binning.total, xys, con, diff, fin)
         return loss
 
     @staticmethod
     def backward(ctx, g):
-        (chol, means, colors, opacities, target, gids, bins, total, xys, con, img,
+        (chol, means, colors, opacities, gids, bins, total, xys, con, diff,
          fin) = ctx.saved_tensors
         H, W, block = ctx.geom
         clamp = ctx.alpha_clamp if ctx.alpha_clamp is not None else 0.0
-        v_xy, v_abs, v_con, v_rgb, v_op = ops.raster_bwd_l2(
-            H, W, block, gids, bins, total, xys, con, colors, opacities, fin, img, target,
-            g.to(img.dtype), alpha_clamp=clamp)
+        v_xy, v_abs, v_con, v_rgb, v_op = ops.raster_bwd_diff(
+            H, W, block, gids, bins, total, xys, con, colors, opacities, fin, diff,
+            g.to(diff.dtype), alpha_clamp=clamp)
         v_chol, v_mean = ops.project_bwd(chol, means, opacities, H, W, block, True, v_xy, v_con)
         return v_chol, v_mean, v_rgb, v_op, None, None, None, None, None
 

@@ -421,6 +421,57 @@ def raster_bwd_l2(img_h, img_w, block, gaussian_ids_sorted, tile_bins, total, xy
     return v_xy, v_abs, v_con, v_rgb, v_op
 
 
+def raster_fwd_l2(img_h, img_w, block, gaussian_ids_sorted, tile_bins, total, xys, conics,
+                  colors, opacities, target):
+    """Fit-loop forward with the clamped-L2 loss fused in.  Returns
+    (diff [H,W,3], final_idx [H,W], loss 0-d): diff = (0 <= x <= 1) ?
+    clamp(x) - target : 0 for the render x, loss = mean((clamp(x) - target)^2)."""
+    _check_cuda(xys, conics, colors, opacities, tile_bins, total, target)
+    xys = _c(xys)
+    dt = xys.dtype
+    conics, colors, opacities = _c(conics, dt), _c(colors, dt), _c(opacities, dt)
+    target = _c(target, dt)
+    n = xys.shape[0]
+    dev = xys.device
+    code = _dt(xys)
+    ws, wsb = _raster_ws(code, n, dev)
+    tbx, tby = tile_bounds(img_h, img_w, block)
+    part = torch.empty((tbx * tby,), dtype=torch.float64, device=dev)
+    diff = torch.empty((img_h, img_w, 3), dtype=dt, device=dev)
+    fin = torch.empty((img_h, img_w), dtype=torch.int32, device=dev)
+    loss = torch.empty((), dtype=dt, device=dev)
+    call("lig_raster_fwd_l2", code, int(img_h), int(img_w), int(block), n,
+         _p(gaussian_ids_sorted), _p(tile_bins), _p(total), _p(xys), _p(conics), _p(colors),
+         _p(opacities), _p(target), _p(ws), wsb, _p(part), _p(diff), _p(fin), _p(loss),
+         _stream(dev))
+    return diff, fin, loss
+
+
+def raster_bwd_diff(img_h, img_w, block, gaussian_ids_sorted, tile_bins, total, xys, conics,
+                    colors, opacities, final_idx, diff, grad_loss, alpha_clamp: float = 0.0):
+    """Sum backward of the fused-L2 forward's loss, from its diff."""
+    _check_cuda(xys, conics, colors, final_idx, diff, grad_loss)
+    xys = _c(xys)
+    dt = xys.dtype
+    conics, colors, opacities = _c(conics, dt), _c(colors, dt), _c(opacities, dt)
+    diff, grad_loss = _c(diff, dt), _c(grad_loss.reshape(1), dt)
+    n = xys.shape[0]
+    dev = xys.device
+    code = _dt(xys)
+    ws, wsb = _raster_ws(code, n, dev)
+    v_xy = torch.empty((n, 2), dtype=dt, device=dev)
+    v_abs = torch.empty((n, 2), dtype=dt, device=dev)
+    v_con = torch.empty((n, 3), dtype=dt, device=dev)
+    v_rgb = torch.empty((n, 3), dtype=dt, device=dev)
+    v_op = torch.empty((n,), dtype=dt, device=dev) if opacities is not None else None
+    call("lig_raster_bwd_diff", code, int(img_h), int(img_w), int(block), n,
+         _p(gaussian_ids_sorted), _p(tile_bins), _p(total), _p(xys), _p(conics), _p(colors),
+         _p(opacities), _p(_c(final_idx, torch.int32)), _p(diff), _p(grad_loss),
+         float(alpha_clamp), _p(ws), wsb, _p(v_xy), _p(v_abs), _p(v_con), _p(v_rgb), _p(v_op),
+         _stream(dev))
+    return v_xy, v_abs, v_con, v_rgb, v_op
+
+
 def l2_clamped_loss(img, target):
     """mean((clamp(img, 0, 1) - target)^2) as a 0-d device tensor."""
     _check_cuda(img, target)

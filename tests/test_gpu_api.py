@@ -186,3 +186,32 @@ def test_fused_render_l2_matches_unfused_chain():
     assert abs(l1.item() - l2.item()) <= 1e-6 * abs(l1.item())
     for a, b in zip(p2, p1):
         assert rel_err(np_(a.grad), np_(b.grad)) <= 1e-5
+
+
+def test_fused_l2_forward_diff_and_loss():
+    """lig_raster_fwd_l2: diff = mask * (clamp(x) - t) bit-exact against the
+    plain forward's image, loss against the separate loss kernel (different
+    summation order: 1e-6 relative), final_idx identical; and the backward
+    from diff equals the backward from (image, target)."""
+    H, W, B, n = 150, 170, 16, 3000
+    means, L, colors, _ = scene(n, H, W, diag=(0.5, 5.0), seed=6)
+    g = torch.Generator().manual_seed(10)
+    target = torch.rand(H, W, 3, generator=g).cuda()
+    xys, ext, con, cnt = ops.project_fwd(L, means, None, H, W, B, True)
+    b = ops.bin_gaussians(xys, ext, cnt, H, W, B)
+    img, _, _, _, _, fin = ops.raster_fwd(H, W, B, b.gaussian_ids_sorted, b.tile_bins, b.total,
+                                          xys, con, colors, None, False)
+    diff, fin2, loss = ops.raster_fwd_l2(H, W, B, b.gaussian_ids_sorted, b.tile_bins, b.total,
+                                         xys, con, colors, None, target)
+    exp = torch.where((img >= 0) & (img <= 1), torch.clamp(img, 0, 1) - target,
+                      torch.zeros_like(img))
+    assert torch.equal(diff, exp) and torch.equal(fin2, fin)
+    ref_loss = ops.l2_clamped_loss(img, target)
+    assert abs(loss.item() - ref_loss.item()) <= 1e-6 * ref_loss.item()
+    one = torch.ones((), device="cuda")
+    ga = ops.raster_bwd_l2(H, W, B, b.gaussian_ids_sorted, b.tile_bins, b.total, xys, con,
+                           colors, None, fin, img, target, one)
+    gb = ops.raster_bwd_diff(H, W, B, b.gaussian_ids_sorted, b.tile_bins, b.total, xys, con,
+                             colors, None, fin2, diff, one)
+    for x, y in zip(ga[:4], gb[:4]):
+        assert rel_err(np_(x), np_(y)) <= 1e-5

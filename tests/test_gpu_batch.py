@@ -97,9 +97,11 @@ def test_batch_fused_l2_gradients_match_single():
     fit2._render(fit2._stream())
     torch.cuda.synchronize()
     st = fit2._stream()
+    l_ws = torch.empty(_lib.lib.lig_l2_batch_workspace_bytes(L.n), dtype=torch.uint8,
+                       device="cuda")
     ops.call("lig_l2_clamped_loss_batch", _lib.LIG_F32, *L.hw_args(), ops._p(fit2.img),
-             ops._p(fit2.target), ops._p(fit2.loss), ops._p(fit2.per_image), ops._p(fit2.l_ws),
-             fit2.l_ws.numel(), st)
+             ops._p(fit2.target), ops._p(fit2.loss), ops._p(fit2.per_image), ops._p(l_ws),
+             l_ws.numel(), st)
     ops.call("lig_raster_bwd_l2_batch", _lib.LIG_F32, *L.args(), L.block, ops._p(fit2.gids),
              ops._p(fit2.bins), ops._p(fit2.total), ops._p(fit2.cum), ops._p(fit2.xys),
              ops._p(fit2.con), ops._p(fit2.rgbs), None, ops._p(fit2.fin), ops._p(fit2.img),
@@ -124,7 +126,10 @@ def test_batch_fused_l2_gradients_match_single():
         assert rel_err(np_(gc), np_(ch.grad)) <= 1e-5
         assert rel_err(np_(gr), np_(co.grad)) <= 1e-5
     assert abs(fit2.loss.item() - total) <= 1e-5 * total
-    # the first fit's gradients (same parameters, same kernels) agree as well
+    # the first fit's step (fused-L2 forward, backward from its difference)
+    # gives the same loss and gradients
+    assert abs(fit.loss.item() - fit2.loss.item()) <= 1e-6 * fit2.loss.item()
+    assert torch.allclose(fit.per_image, fit2.per_image, rtol=1e-6, atol=0)
     assert rel_err(np_(fit.grad), np_(fit2.grad)) <= 1e-5
 
 
