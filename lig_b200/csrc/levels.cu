@@ -113,21 +113,23 @@ compose_kernel(int ph, int pw, const float *__restrict__ prev, int H, int W,
 #pragma unroll
             for (int c = 0; c < 3; ++c) base[c] = prev ? prev[3 * p + c] : 0.f;
         } else {
-            const float ry = fmaxf(__fsub_rn(__fmul_rn(sh, __fadd_rn((float)y, 0.5f)), 0.5f), 0.f);
-            const float rx = fmaxf(__fsub_rn(__fmul_rn(sw, __fadd_rn((float)x, 0.5f)), 0.5f), 0.f);
+            // the half-pixel source index and weights written as the bilinear
+            // definition states them (src = s (d + 0.5) - 0.5, negative -> 0;
+            // lambda1 = src - floor, lambda0 = 1 - lambda1), so that the
+            // compiler contracts them as it does torch's upsample kernel
+            float ry = sh * ((float)y + 0.5f) - 0.5f;
+            float rx = sw * ((float)x + 0.5f) - 0.5f;
+            ry = ry < 0.f ? 0.f : ry;
+            rx = rx < 0.f ? 0.f : rx;
             const int y0 = (int)ry, x0 = (int)rx;
             const int y1 = y0 + (y0 < ph - 1 ? 1 : 0), x1 = x0 + (x0 < pw - 1 ? 1 : 0);
-            const float ly1 = __fsub_rn(ry, (float)y0), lx1 = __fsub_rn(rx, (float)x0);
-            const float ly0 = __fsub_rn(1.f, ly1), lx0 = __fsub_rn(1.f, lx1);
+            const float ly1 = ry - (float)y0, lx1 = rx - (float)x0;
+            const float ly0 = 1.f - ly1, lx0 = 1.f - lx1;
             const float *r0 = prev + 3 * ((int64_t)y0 * pw), *r1 = prev + 3 * ((int64_t)y1 * pw);
 #pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                const float top = __fadd_rn(__fmul_rn(lx0, r0[3 * x0 + c]),
-                                            __fmul_rn(lx1, r0[3 * x1 + c]));
-                const float bot = __fadd_rn(__fmul_rn(lx0, r1[3 * x0 + c]),
-                                            __fmul_rn(lx1, r1[3 * x1 + c]));
-                base[c] = __fadd_rn(__fmul_rn(ly0, top), __fmul_rn(ly1, bot));
-            }
+            for (int c = 0; c < 3; ++c)
+                base[c] = ly0 * (lx0 * r0[3 * x0 + c] + lx1 * r0[3 * x1 + c]) +
+                          ly1 * (lx0 * r1[3 * x0 + c] + lx1 * r1[3 * x1 + c]);
         }
 #pragma unroll
         for (int c = 0; c < 3; ++c) {

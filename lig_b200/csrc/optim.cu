@@ -31,10 +31,13 @@ struct AdamScalars {
 // One element, in the form torch.optim.Adam evaluates it: m = lerp(m, g,
 // 1 - b1), v = v b2 + (1 - b2) g g, p -= step_size * m / (sqrt(v) / bc2 +
 // eps), with correctly rounded square root and divisions.
-__device__ __forceinline__ void adam_update(float &p, float g, float &m, float &v, float b1,
-                                            float b2, float eps, const AdamScalars &a) {
-    m = __fadd_rn(m, __fmul_rn(__fsub_rn(1.f, b1), __fsub_rn(g, m)));
-    v = __fadd_rn(__fmul_rn(v, b2), __fmul_rn(__fmul_rn(__fsub_rn(1.f, b2), g), g));
+// c1 = 1 - b1 and c2 = 1 - b2 are formed in double on the host and rounded
+// once, as torch does with its Python-float coefficients.
+__device__ __forceinline__ void adam_update(float &p, float g, float &m, float &v, float c1,
+                                            float b2, float c2, float eps,
+                                            const AdamScalars &a) {
+    m = __fadd_rn(m, __fmul_rn(c1, __fsub_rn(g, m)));
+    v = __fadd_rn(__fmul_rn(v, b2), __fmul_rn(__fmul_rn(c2, g), g));
     const float den = __fadd_rn(__fdiv_rn(__fsqrt_rn(v), a.bc2_sqrt), eps);
     p = __fsub_rn(p, __fmul_rn(a.step_size, __fdiv_rn(m, den)));
 }
@@ -58,8 +61,8 @@ __global__ void adam_prologue_kernel(const int32_t *__restrict__ status, int32_t
 
 __global__ void __launch_bounds__(256)
 adam_kernel(int64_t n, float *__restrict__ p, const float *__restrict__ g,
-            float *__restrict__ m, float *__restrict__ v, float b1, float b2, float eps,
-            const AdamScalars *__restrict__ sc) {
+            float *__restrict__ m, float *__restrict__ v, float c1, float b2, float c2,
+            float eps, const AdamScalars *__restrict__ sc) {
     const AdamScalars a = *sc;
     if (a.skip) return;
     const int64_t n4 = n / 4;
@@ -72,13 +75,13 @@ adam_kernel(int64_t n, float *__restrict__ p, const float *__restrict__ g,
         float4 pp = p4[i], gg = g4[i], mm = m4[i], vv = v4[i];
         float *pe = &pp.x, *ge = &gg.x, *me = &mm.x, *ve = &vv.x;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) adam_update(pe[k], ge[k], me[k], ve[k], b1, b2, eps, a);
+        for (int k = 0; k < 4; ++k) adam_update(pe[k], ge[k], me[k], ve[k], c1, b2, c2, eps, a);
         p4[i] = pp; m4[i] = mm; v4[i] = vv;
     }
     for (int64_t i = n4 * 4 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += stride) {
         float pi = p[i], mi = m[i], vi = v[i];
-        adam_update(pi, g[i], mi, vi, b1, b2, eps, a);
+        adam_update(pi, g[i], mi, vi, c1, b2, c2, eps, a);
         p[i] = pi; m[i] = mi; v[i] = vi;
     }
 }
@@ -118,15 +121,15 @@ __device__ __forceinline__ int elem_image(const AdamBatch &ab, int64_t e) {
 
 __global__ void __launch_bounds__(256)
 adam_batch_kernel(AdamBatch ab, float *__restrict__ p, const float *__restrict__ g,
-                  float *__restrict__ m, float *__restrict__ v, float b1, float b2, float eps,
-                  const AdamScalars *__restrict__ sc) {
+                  float *__restrict__ m, float *__restrict__ v, float c1, float b2, float c2,
+                  float eps, const AdamScalars *__restrict__ sc) {
     if (sc[0].skip) return;
     const int64_t n = 8ll * ab.n_pts;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const AdamScalars a = sc[elem_image(ab, i)];
         float pi = p[i], mi = m[i], vi = v[i];
-        adam_update(pi, g[i], mi, vi, b1, b2, eps, a);
+        adam_update(pi, g[i], mi, vi, c1, b2, c2, eps, a);
         p[i] = pi; m[i] = mi; v[i] = vi;
     }
 }
@@ -169,7 +172,8 @@ extern "C" int lig_adam_step_batch(int n_img, const int32_t *counts, float *para
         const int64_t cap = 148 * 16;
         if (blocks > cap) blocks = cap;
         adam_batch_kernel<<<(int)blocks, 256, 0, s>>>(ab, params, grads, exp_avg, exp_avg_sq,
-                                                     (float)beta1, (float)beta2, (float)eps, sc);
+                                                     (float)(1.0 - beta1), (float)beta2,
+                                                     (float)(1.0 - beta2), (float)eps, sc);
         ++launches;
     }
     note_launches(launches);
@@ -199,7 +203,8 @@ extern "C" int lig_adam_step(int64_t n, float *params, const float *grads, float
         if (blocks > cap) blocks = cap;
         if (blocks < 1) blocks = 1;
         adam_kernel<<<(int)blocks, 256, 0, s>>>(n, params, grads, exp_avg, exp_avg_sq,
-                                               (float)beta1, (float)beta2, (float)eps, sc);
+                                               (float)(1.0 - beta1), (float)beta2,
+                                               (float)(1.0 - beta2), (float)eps, sc);
         ++launches;
     }
     note_launches(launches);

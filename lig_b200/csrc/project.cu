@@ -27,11 +27,14 @@ template <typename T> struct View {
 
 // cov2d (a,b,c) from the input triple: pass-through, or the Cholesky product
 // [l11^2, l11 l21, l21^2 + l22^2] written as in csrc/forward.cu:79-83.
-template <typename T>
+// VIEW is a template parameter so that the plain projection compiles to
+// exactly the reference's arithmetic (a runtime branch changes how the
+// compiler contracts the products below, and with it the rounding).
+template <typename T, bool VIEW = false>
 __device__ __forceinline__ void input_cov(bool chol, const T *in3, int i, T &cx, T &cy, T &cz,
                                           const View<T> &v = View<T>{0, 0, 1, 1, false}) {
     T p = in3[3 * i], q = in3[3 * i + 1], r = in3[3 * i + 2];
-    if (v.on) {
+    if constexpr (VIEW) {
         if (chol) { p *= v.sx; q *= v.sy; r *= v.sy; }
         else { p *= v.sx * v.sx; q *= v.sx * v.sy; r *= v.sy * v.sy; }
     }
@@ -47,7 +50,7 @@ __device__ __forceinline__ void input_cov(bool chol, const T *in3, int i, T &cx,
 // Forward: csrc/forward.cu:13-105 semantics.  xys holds the mean only where
 // the tile area is positive (zero otherwise), conics are written whenever
 // det != 0, extents only with a positive tile area.
-template <typename T>
+template <typename T, bool VIEW>
 __global__ void project_fwd_kernel(int n, bool chol, const T *__restrict__ in3,
                                    const T *__restrict__ means, const T *__restrict__ opac,
                                    BatchGeo geo, View<T> view, T *__restrict__ xys,
@@ -58,12 +61,12 @@ __global__ void project_fwd_kernel(int n, bool chol, const T *__restrict__ in3,
     const int im = geo.image_of_gauss(i);
     const unsigned tbx = geo.tbx[im], tby = geo.tby(im), block = geo.B;
     T cx, cy, cz;
-    input_cov(chol, in3, i, cx, cy, cz, view);
+    input_cov<T, VIEW>(chol, in3, i, cx, cy, cz, view);
     T o = opac ? opac[i] : (T)1;
     T ca = 0, cb = 0, cc = 0, ex = 0, ey = 0;
     bool ok = cov2d_bounds(cx, cy, cz, o, ca, cb, cc, ex, ey);
     T mx = means[2 * i], my = means[2 * i + 1];
-    if (view.on) {
+    if constexpr (VIEW) {
         mx = (mx - view.ox) * view.sx;
         my = (my - view.oy) * view.sy;
     }
@@ -226,9 +229,14 @@ int project_fwd(int n, int chol, const void *in3, const void *means, const void 
                 const BatchGeo &geo, void *xys, void *ext, void *con, int32_t *cnt,
                 cudaStream_t s, View<T> view = View<T>{0, 0, 1, 1, false}) {
     if (n == 0) return LIG_OK;
-    project_fwd_kernel<T><<<proj_blocks(n), kProjThreads, 0, s>>>(
-        n, chol != 0, (const T *)in3, (const T *)means, (const T *)opac, geo, view, (T *)xys,
-        (T *)ext, (T *)con, cnt);
+    if (view.on)
+        project_fwd_kernel<T, true><<<proj_blocks(n), kProjThreads, 0, s>>>(
+            n, chol != 0, (const T *)in3, (const T *)means, (const T *)opac, geo, view,
+            (T *)xys, (T *)ext, (T *)con, cnt);
+    else
+        project_fwd_kernel<T, false><<<proj_blocks(n), kProjThreads, 0, s>>>(
+            n, chol != 0, (const T *)in3, (const T *)means, (const T *)opac, geo, view,
+            (T *)xys, (T *)ext, (T *)con, cnt);
     note_launches(1);
     LIG_LAUNCH_CHECK();
     return LIG_OK;

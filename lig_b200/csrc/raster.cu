@@ -339,31 +339,28 @@ __device__ __forceinline__ void block_sum_to(double v, double *dst) {
     __syncthreads();
 }
 
-// Writes one pixel's forward outputs (or, in the fused-L2 mode, its masked
-// difference and the tile's loss partial; every thread of the CTA calls it).
+// Writes one pixel's forward outputs, or in the fused-L2 mode its masked
+// difference; returns the pixel's (clamp(x) - t)^2 sum for the tile partial.
 template <typename T, bool GA>
-__device__ __forceinline__ void fwd_store(const FwdAcc<T, GA> &acc, bool inside, int pix,
-                                          T *__restrict__ img, T *__restrict__ wsum,
-                                          T *__restrict__ odx, T *__restrict__ ody,
-                                          T *__restrict__ odxy, int32_t *__restrict__ final_idx,
-                                          const L2Fwd<T> &l2, int tile) {
+__device__ __forceinline__ double fwd_write(const FwdAcc<T, GA> &acc, bool inside, int pix,
+                                            T *__restrict__ img, T *__restrict__ wsum,
+                                            T *__restrict__ odx, T *__restrict__ ody,
+                                            T *__restrict__ odxy,
+                                            int32_t *__restrict__ final_idx,
+                                            const L2Fwd<T> &l2) {
+    if (!inside) return 0.0;
+    final_idx[pix] = acc.cur;
     if (l2.target) {
         double sq = 0;
-        if (inside) {
-            final_idx[pix] = acc.cur;
-            const T x[3] = {acc.r, acc.g, acc.b};
+        const T x[3] = {acc.r, acc.g, acc.b};
 #pragma unroll
-            for (int ch = 0; ch < 3; ++ch) {
-                const T d = min(max(x[ch], (T)0), (T)1) - l2.target[3 * pix + ch];
-                sq += (double)(d * d);
-                img[3 * pix + ch] = (x[ch] >= (T)0 && x[ch] <= (T)1) ? d : (T)0;
-            }
+        for (int ch = 0; ch < 3; ++ch) {
+            const T d = min(max(x[ch], (T)0), (T)1) - l2.target[3 * pix + ch];
+            sq += (double)(d * d);
+            img[3 * pix + ch] = (x[ch] >= (T)0 && x[ch] <= (T)1) ? d : (T)0;
         }
-        block_sum_to<T>(sq, l2.tile_partial + tile);
-        return;
+        return sq;
     }
-    if (!inside) return;
-    final_idx[pix] = acc.cur;
     img[3 * pix] = acc.r;
     img[3 * pix + 1] = acc.g;
     img[3 * pix + 2] = acc.b;
@@ -376,9 +373,14 @@ __device__ __forceinline__ void fwd_store(const FwdAcc<T, GA> &acc, bool inside,
             odxy[3 * pix + ch] = acc.dxy[ch];
         }
     }
+    return 0.0;
 }
 
-template <typename T, bool GA>
+// PPL pixels per lane: 1 (8x4 regions, two Gaussians per iteration) or 2
+// (8x8 regions, lane owns (x, y) and (x, y + 4); each Gaussian's record and
+// loop overhead are shared by its two evaluations).  Per pixel the terms are
+// added in list order either way.
+template <typename T, bool GA, int PPL>
 __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int32_t *__restrict__ ids,
                                          const int2 *__restrict__ tile_bins,
                                          const Rec<T> *__restrict__ recs, T *__restrict__ img,
@@ -390,61 +392,103 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
     const unsigned FULL = 0xffffffffu;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int B = tc.B, tx0 = tc.tx0, ty0 = tc.ty0;
-    const Regions R = Regions::make(0, B);
-    int lx, ly;
-    R.pixel(w, lane, 0, lx, ly);
-    const int gx = tx0 + lx, gy = ty0 + ly;
-    const bool inside = lx < B && ly < B && gx < tc.W && gy < tc.H;
-    const int pix = tc.poff + gy * tc.W + gx;
-    const T px = (T)gx + (T)0.5, py = (T)gy + (T)0.5;
-
-    FwdAcc<T, GA> acc;
-    if (tc.empty) {  // the reference's empty-list branch (rasterize.py:80-90)
-        acc.r = acc.g = acc.b = (T)1;
-        fwd_store<T, GA>(acc, inside, pix, img, wsum, odx, ody, odxy, final_idx, l2, tile);
-        return;
+    const Regions R = Regions::make(PPL == 2 ? 1 : 0, B);
+    bool inside[PPL];
+    int pix[PPL];
+    T px[PPL], py[PPL];
+#pragma unroll
+    for (int p = 0; p < PPL; ++p) {
+        int lx, ly;
+        R.pixel(w, lane, p, lx, ly);
+        const int gx = tx0 + lx, gy = ty0 + ly;
+        inside[p] = lx < B && ly < B && gx < tc.W && gy < tc.H;
+        pix[p] = tc.poff + gy * tc.W + gx;
+        px[p] = (T)gx + (T)0.5;
+        py[p] = (T)gy + (T)0.5;
     }
 
-    const int2 range = tile_bins[tile];
-    Rec<T> pre;
-    if (range.x + tid < range.y) pre = recs[__ldg(ids + range.x + tid)];
-    for (int base = range.x; base < range.y; base += nt) {
-        const int cnt = min(nt, range.y - base);
-        __syncthreads();
-        if (tid < cnt) {
-            s_rec[tid] = pre;
-            s_bits[tid] = region_bits<T, false>(pre, R, tx0, ty0);
-        }
-        __syncthreads();
-        if (base + nt + tid < range.y) pre = recs[__ldg(ids + base + nt + tid)];
-        for (int m = 0; m * 32 < cnt; ++m) {
-            const int t = m * 32 + lane;
-            uint32_t mask = __ballot_sync(FULL, t < cnt && ((s_bits[t] >> w) & 1u));
-            while (mask) {
-                const int b1 = __ffs(mask) - 1;
-                mask &= mask - 1;
-                const Rec<T> g1 = s_rec[m * 32 + b1];
-                T dx1, dy1, a1;
-                const bool ok1 = PixelEval<T>::template alpha<GA>(g1, px, py, dx1, dy1, a1);
-                if (mask) {
-                    const int b2 = __ffs(mask) - 1;
-                    mask &= mask - 1;
-                    const Rec<T> g2 = s_rec[m * 32 + b2];
-                    T dx2, dy2, a2;
-                    const bool ok2 = PixelEval<T>::template alpha<GA>(g2, px, py, dx2, dy2, a2);
-                    if (ok1) acc.add(g1, dx1, dy1, a1, base + m * 32 + b1);
-                    if (ok2) acc.add(g2, dx2, dy2, a2, base + m * 32 + b2);
-                } else if (ok1) {
-                    acc.add(g1, dx1, dy1, a1, base + m * 32 + b1);
+    FwdAcc<T, GA> acc[PPL];
+    if (!tc.empty) {
+        const int2 range = tile_bins[tile];
+        Rec<T> pre;
+        if (range.x + tid < range.y) pre = recs[__ldg(ids + range.x + tid)];
+        for (int base = range.x; base < range.y; base += nt) {
+            const int cnt = min(nt, range.y - base);
+            __syncthreads();
+            if (tid < cnt) {
+                s_rec[tid] = pre;
+                s_bits[tid] = region_bits<T, false>(pre, R, tx0, ty0);
+            }
+            __syncthreads();
+            if (base + nt + tid < range.y) pre = recs[__ldg(ids + base + nt + tid)];
+            for (int m = 0; m * 32 < cnt; ++m) {
+                const int t = m * 32 + lane;
+                uint32_t mask = __ballot_sync(FULL, t < cnt && ((s_bits[t] >> w) & 1u));
+                if constexpr (PPL == 1) {
+                    while (mask) {
+                        const int b1 = __ffs(mask) - 1;
+                        mask &= mask - 1;
+                        const Rec<T> g1 = s_rec[m * 32 + b1];
+                        T dx1, dy1, a1;
+                        const bool ok1 =
+                            PixelEval<T>::template alpha<GA>(g1, px[0], py[0], dx1, dy1, a1);
+                        if (mask) {
+                            const int b2 = __ffs(mask) - 1;
+                            mask &= mask - 1;
+                            const Rec<T> g2 = s_rec[m * 32 + b2];
+                            T dx2, dy2, a2;
+                            const bool ok2 =
+                                PixelEval<T>::template alpha<GA>(g2, px[0], py[0], dx2, dy2, a2);
+                            if (ok1) acc[0].add(g1, dx1, dy1, a1, base + m * 32 + b1);
+                            if (ok2) acc[0].add(g2, dx2, dy2, a2, base + m * 32 + b2);
+                        } else if (ok1) {
+                            acc[0].add(g1, dx1, dy1, a1, base + m * 32 + b1);
+                        }
+                    }
+                } else {
+                    while (mask) {
+                        const int b1 = __ffs(mask) - 1;
+                        mask &= mask - 1;
+                        const Rec<T> g1 = s_rec[m * 32 + b1];
+                        T dxa, dya, aa, dxb, dyb, ab;
+                        const bool oka =
+                            PixelEval<T>::template alpha<GA>(g1, px[0], py[0], dxa, dya, aa);
+                        const bool okb =
+                            PixelEval<T>::template alpha<GA>(g1, px[1], py[1], dxb, dyb, ab);
+                        if (oka) acc[0].add(g1, dxa, dya, aa, base + m * 32 + b1);
+                        if (okb) acc[1].add(g1, dxb, dyb, ab, base + m * 32 + b1);
+                    }
                 }
             }
         }
+    } else {  // the reference's empty-list branch (rasterize.py:80-90)
+#pragma unroll
+        for (int p = 0; p < PPL; ++p) acc[p].r = acc[p].g = acc[p].b = (T)1;
     }
-    fwd_store<T, GA>(acc, inside, pix, img, wsum, odx, ody, odxy, final_idx, l2, tile);
+    double sq = 0.0;
+#pragma unroll
+    for (int p = 0; p < PPL; ++p)
+        sq += fwd_write<T, GA>(acc[p], inside[p], pix[p], img, wsum, odx, ody, odxy, final_idx, l2);
+    if (l2.target) block_sum_to<T>(sq, l2.tile_partial + tile);
 }
 
-template <typename T, bool GA>
-__global__ void __launch_bounds__(1024)
+// Launch bounds: tiles of B <= 16 launch <= 256 threads, and their
+// instantiation asks for LIG_RASTER_FWD_MINB / LIG_RASTER_BWD_MINB resident
+// CTAs per SM (the register budget follows); larger tiles use the 1024-thread
+// instantiation.
+#ifndef LIG_RASTER_FWD_MINB
+#define LIG_RASTER_FWD_MINB 4
+#endif
+#ifndef LIG_RASTER_BWD_MINB
+#define LIG_RASTER_BWD_MINB 4
+#endif
+
+#ifndef LIG_RASTER_FWD_PPL
+#define LIG_RASTER_FWD_PPL 1
+#endif
+
+template <typename T, bool GA, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB)
 raster_fwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work,
                   const int32_t *__restrict__ ids, const int2 *__restrict__ tile_bins,
                   const int32_t *__restrict__ d_total, const Rec<T> *__restrict__ recs,
@@ -459,8 +503,9 @@ raster_fwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work
     for (int tile = next_tile(work, s_slot, true); tile < n_tiles;
          tile = next_tile(work, s_slot, false)) {
         const TileCtx tc = tile_ctx(geo, cum, d_total, tile);
-        fwd_tile<T, GA>(tc, tile, ids, tile_bins, recs, img, wsum, odx, ody, odxy, final_idx,
-                        s_rec, s_bits, l2);
+        fwd_tile<T, GA, GA ? 1 : LIG_RASTER_FWD_PPL>(tc, tile, ids, tile_bins, recs, img, wsum,
+                                                     odx, ody, odxy, final_idx, s_rec, s_bits,
+                                                     l2);
     }
 }
 
@@ -756,8 +801,8 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
     }
 }
 
-template <typename T, bool GA>
-__global__ void __launch_bounds__(1024)
+template <typename T, bool GA, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB)
 raster_bwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work,
                   const int32_t *__restrict__ ids, const int2 *__restrict__ tile_bins,
                   const int32_t *__restrict__ d_total, const Rec<T> *__restrict__ recs,
@@ -809,8 +854,12 @@ int pack(int n, const void *xys, const void *con, const void *col, const void *o
 // Opt a kernel into `bytes` of dynamic shared memory, once per (kernel,
 // device, size): repeated calls cost nothing, and none is made during a
 // stream capture after the first eager call.
+#ifndef LIG_RASTER_CARVEOUT
+#define LIG_RASTER_CARVEOUT -1  // shared-memory carveout percent; -1: driver default
+#endif
+
 inline bool set_dyn_smem(const void *fn, size_t bytes) {
-    if (bytes <= 48 * 1024) return true;
+    if (bytes <= 48 * 1024 && LIG_RASTER_CARVEOUT < 0) return true;
     static std::mutex mu;
     static std::vector<std::tuple<const void *, int, size_t>> done;
     int dev = 0;
@@ -818,8 +867,13 @@ inline bool set_dyn_smem(const void *fn, size_t bytes) {
     std::lock_guard<std::mutex> lock(mu);
     for (auto &e : done)
         if (std::get<0>(e) == fn && std::get<1>(e) == dev && std::get<2>(e) >= bytes) return true;
-    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) !=
-        cudaSuccess)
+    if (bytes > 48 * 1024 &&
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) !=
+            cudaSuccess)
+        return false;
+    if (LIG_RASTER_CARVEOUT >= 0 &&
+        cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             LIG_RASTER_CARVEOUT) != cudaSuccess)
         return false;
     done.emplace_back(fn, dev, bytes);
     return true;
@@ -866,26 +920,28 @@ int raster_fwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
     int rc = pack<T>(n, xys, con, col, op, ws, ws_bytes, s);
     if (rc) return rc;
     const bool ga = dx != nullptr;
-    const int nt = 32 * Regions::make(0, geo.B).count;
+    const int kind = (!ga && LIG_RASTER_FWD_PPL == 2) ? 1 : 0;
+    const int nt = 32 * Regions::make(kind, geo.B).count;
     const size_t sm = (size_t)nt * (sizeof(Rec<T>) + sizeof(uint32_t));
-    const void *fn = ga ? (const void *)raster_fwd_kernel<T, true>
-                        : (const void *)raster_fwd_kernel<T, false>;
-    if (!set_dyn_smem(fn, sm)) return LIG_ERR_LAUNCH;
+    using K = void (*)(const BatchGeo, const int32_t *, int *, const int32_t *, const int2 *,
+                       const int32_t *, const Rec<T> *, T *, T *, T *, T *, T *, int32_t *,
+                       L2Fwd<T>);
+    const bool small = nt <= 256;
+    K fn = ga ? (small ? raster_fwd_kernel<T, true, 256, LIG_RASTER_FWD_MINB>
+                       : raster_fwd_kernel<T, true, 1024, 1>)
+              : (small ? raster_fwd_kernel<T, false, 256, LIG_RASTER_FWD_MINB>
+                       : raster_fwd_kernel<T, false, 1024, 1>);
+    if (!set_dyn_smem((const void *)fn, sm)) return LIG_ERR_LAUNCH;
     int grid = geo.total_tiles();
     if (walk.work) {
-        const int pg = persistent_grid(fn, nt, sm);
+        const int pg = persistent_grid((const void *)fn, nt, sm);
         if (pg <= 0) return LIG_ERR_LAUNCH;
         grid = grid < pg ? grid : pg;
         cudaMemsetAsync(walk.work, 0, sizeof(int), s);
     }
-    if (ga)
-        raster_fwd_kernel<T, true><<<grid, nt, sm, s>>>(
-            geo, walk.cum, walk.work, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws,
-            (T *)img, (T *)wsum, (T *)dx, (T *)dy, (T *)dxy, fin, l2);
-    else
-        raster_fwd_kernel<T, false><<<grid, nt, sm, s>>>(
-            geo, walk.cum, walk.work, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws,
-            (T *)img, (T *)wsum, nullptr, nullptr, nullptr, fin, l2);
+    fn<<<grid, nt, sm, s>>>(geo, walk.cum, walk.work, ids, (const int2 *)bins, d_total,
+                            (const Rec<T> *)ws, (T *)img, (T *)wsum, ga ? (T *)dx : nullptr,
+                            ga ? (T *)dy : nullptr, ga ? (T *)dxy : nullptr, fin, l2);
     int launches = 1;
     if (l2.target) {
         l2_tiles_final_kernel<T><<<1, 1024, 0, s>>>(geo, l2.tile_partial, l2o.loss,
@@ -923,24 +979,26 @@ int raster_bwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
     const size_t pix = ga ? sizeof(PixRec<T, true>) : sizeof(PixRec<T, false>);
     const size_t sm = (size_t)nt * pix + (size_t)nt * (sizeof(Rec<T>) + 2 * sizeof(uint32_t)) +
                       (size_t)nw * nt * sizeof(uint16_t);
-    const void *fn = ga ? (const void *)raster_bwd_kernel<T, true>
-                        : (const void *)raster_bwd_kernel<T, false>;
-    if (!set_dyn_smem(fn, sm)) return LIG_ERR_LAUNCH;
+    using K = void (*)(const BatchGeo, const int32_t *, int *, const int32_t *, const int2 *,
+                       const int32_t *, const Rec<T> *, const int32_t *, CotSrc<T>, const T *,
+                       const T *, const T *, T, T *);
+    const bool small = nt <= 256;
+    K fn = ga ? (small ? raster_bwd_kernel<T, true, 256, LIG_RASTER_BWD_MINB>
+                       : raster_bwd_kernel<T, true, 1024, 1>)
+              : (small ? raster_bwd_kernel<T, false, 256, LIG_RASTER_BWD_MINB>
+                       : raster_bwd_kernel<T, false, 1024, 1>);
+    if (!set_dyn_smem((const void *)fn, sm)) return LIG_ERR_LAUNCH;
     int grid = geo.total_tiles();
     if (walk.work) {
-        const int pg = persistent_grid(fn, nt, sm);
+        const int pg = persistent_grid((const void *)fn, nt, sm);
         if (pg <= 0) return LIG_ERR_LAUNCH;
         grid = grid < pg ? grid : pg;
         cudaMemsetAsync(walk.work, 0, sizeof(int), s);
     }
-    if (ga)
-        raster_bwd_kernel<T, true><<<grid, nt, sm, s>>>(
-            geo, walk.cum, walk.work, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws, fin,
-            cot, (const T *)v_dx, (const T *)v_dy, (const T *)v_dxy, cl, packed);
-    else
-        raster_bwd_kernel<T, false><<<grid, nt, sm, s>>>(
-            geo, walk.cum, walk.work, ids, (const int2 *)bins, d_total, (const Rec<T> *)ws, fin,
-            cot, nullptr, nullptr, nullptr, cl, packed);
+    fn<<<grid, nt, sm, s>>>(geo, walk.cum, walk.work, ids, (const int2 *)bins, d_total,
+                            (const Rec<T> *)ws, fin, cot, ga ? (const T *)v_dx : nullptr,
+                            ga ? (const T *)v_dy : nullptr, ga ? (const T *)v_dxy : nullptr, cl,
+                            packed);
     Grads<T> g{(T *)v_xy, (T *)v_abs, (T *)v_con, (T *)v_rgb, (T *)v_op};
     if (n > 0) unpack_grads_kernel<T><<<(n + 255) / 256, 256, 0, s>>>(n, packed, g);
     note_launches(n > 0 ? 2 : 1);

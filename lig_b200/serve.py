@@ -180,7 +180,10 @@ class Server:
 
     def __init__(self, budget_bytes: int = 150 * 10**9, device="cuda", block: int = 16,
                  max_fit_batch: int = 64, fit_chunk: int = 20, fit_graph: bool = True):
-        self.dev = torch.device(device)
+        dev = torch.device(device)
+        if dev.type == "cuda" and dev.index is None:
+            dev = torch.device("cuda", torch.cuda.current_device())
+        self.dev = dev
         self.block = block
         self.max_fit_batch = max_fit_batch
         self.fit_chunk = fit_chunk

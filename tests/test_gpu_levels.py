@@ -37,7 +37,9 @@ def test_compose_matches_interpolate(prev_hw, hw):
         exp = up + (torch.clamp(render, 0, 1) * (hi - lo) - 0.5 + lo)
         if last:
             exp = torch.clamp(exp, 0, 1)
-        assert (out - exp).abs().max().item() <= 2e-6
+        # a few float ulps at |values| <= 2.5: bilinear weights may contract
+        # into FMAs differently from torch's build
+        assert (out - exp).abs().max().item() <= 4e-6
     # device min/max operands give the same result as host floats
     out_t = compose(prev, render, torch.tensor(lo).cuda(), torch.tensor(hi).cuda(), True)
     assert torch.equal(out_t, compose(prev, render, lo, hi, True))

@@ -119,8 +119,12 @@ def test_raster_forward(case, ga):
     assert (img - r["img"]).abs().max().item() <= IMG_TOL
     assert (wsum - r["wsum"]).abs().max().item() <= IMG_TOL
     if ga:
+        # dx / dy / dxy are derivative images whose magnitude grows with the
+        # conic (|dxy| reaches ~1e2 for sub-pixel Gaussians): 1e-5 of the
+        # image's scale, i.e. a few float ulps of its largest values
         for a, k in zip((dx, dy, dxy), ("dx", "dy", "dxy")):
-            assert (a - r[k]).abs().max().item() <= IMG_TOL, k
+            scale = max(1.0, r[k].abs().max().item())
+            assert (a - r[k]).abs().max().item() <= IMG_TOL * scale, k
 
 
 @pytest.mark.parametrize("case", CASES, ids=_ids)
