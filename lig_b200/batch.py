@@ -196,7 +196,8 @@ class BatchedFit:
         self.fin = torch.empty(P, dtype=i32, **kw)
         self.loss = torch.zeros((), dtype=f32, **kw)
         self.per_image = torch.zeros(L.n, dtype=f32, **kw)
-        self.partials = torch.empty(max(L.tiles, 1), dtype=torch.float64, **kw)
+        self.partials = torch.empty(_lib.lib.lig_l2_tile_partials_bytes(L.tiles) // 8,
+                                    dtype=torch.float64, **kw)
         self.r_ws = torch.empty(_lib.lib.lig_raster_workspace_bytes(_lib.LIG_F32, N),
                                 dtype=torch.uint8, **kw)
         self.v_xy = torch.empty(N, 2, dtype=f32, **kw)
@@ -305,11 +306,23 @@ class BatchedFit:
         self.host_skipped.copy_(self.skipped, non_blocking=True)
 
     def _capture(self):
-        torch.cuda.current_stream(self.dev).synchronize()
+        """Capture one iteration on a side stream.  capture_begin/end rather
+        than the torch.cuda.graph context manager, which also runs the
+        Python garbage collector (holding the GIL) and empties the allocator
+        cache (a device-wide synchronisation) — both stall other threads of
+        a server.  Thread-local capture mode lets those threads keep
+        launching meanwhile."""
+        cur = torch.cuda.current_stream(self.dev)
+        side = torch.cuda.Stream(self.dev)
+        side.wait_stream(cur)
         g = torch.cuda.CUDAGraph()
-        # thread-local: other threads (e.g. a render loop) keep working
-        with torch.cuda.graph(g, capture_error_mode="thread_local"):
-            self._enqueue_step()
+        with torch.cuda.stream(side):
+            g.capture_begin(capture_error_mode="thread_local")
+            try:
+                self._enqueue_step()
+            finally:
+                g.capture_end()
+        cur.wait_stream(side)
         self.graph = g
         self.stats.recaptures += 1
 

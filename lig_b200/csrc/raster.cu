@@ -479,12 +479,15 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
 #ifndef LIG_RASTER_FWD_MINB
 #define LIG_RASTER_FWD_MINB 4
 #endif
+#ifndef LIG_RASTER_BWD_LANE_ELLIPSE
+#define LIG_RASTER_BWD_LANE_ELLIPSE 0
+#endif
 #ifndef LIG_RASTER_BWD_MINB
-#define LIG_RASTER_BWD_MINB 4
+#define LIG_RASTER_BWD_MINB 5
 #endif
 
 #ifndef LIG_RASTER_FWD_PPL
-#define LIG_RASTER_FWD_PPL 1
+#define LIG_RASTER_FWD_PPL 2
 #endif
 
 template <typename T, bool GA, int MAXT, int MINB>
@@ -509,33 +512,40 @@ raster_fwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work
     }
 }
 
-// Loss from the tile partials: image i's mean = (sum of its tiles' partials)
-// / (3 H_i W_i), summed over images.  Warp w reduces images w, w + 32, ...
-// (lane-strided, then a butterfly: fixed order), thread 0 adds the means in
-// image order.
+// Loss from the tile partials, deterministic: block i sums image i's tile
+// partials (thread-strided, then a fixed-order block reduction) into the
+// image's mean partial[T + i] = sum / (3 H_i W_i); one warp then adds the
+// means in image order.
 template <typename T>
 __global__ void __launch_bounds__(1024)
-l2_tiles_final_kernel(const BatchGeo geo, const double *__restrict__ partial,
-                      T *__restrict__ loss, T *__restrict__ per_image) {
-    __shared__ double s_mean[kMaxBatch];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int im = w; im < geo.n_img; im += 32) {
-        double t = 0;
-        for (int k = geo.tile_off[im] + lane; k < geo.tile_off[im + 1]; k += 32) t += partial[k];
+l2_tiles_image_kernel(const BatchGeo geo, double *__restrict__ partial) {
+    __shared__ double s_w[32];
+    const int im = blockIdx.x;
+    const int k0 = geo.tile_off[im], k1 = geo.tile_off[im + 1];
+    double t = 0;
+    for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) t += partial[k];
 #pragma unroll
-        for (int o = 16; o >= 1; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-        if (lane == 0) {
-            const double m = t / (3.0 * (double)geo.H[im] * (double)geo.W[im]);
-            s_mean[im] = m;
-            if (per_image) per_image[im] = (T)m;
-        }
-    }
+    for (int o = 16; o >= 1; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) s_w[w] = t;
     __syncthreads();
     if (threadIdx.x == 0) {
-        double total = 0;
-        for (int im = 0; im < geo.n_img; ++im) total += s_mean[im];
-        *loss = (T)total;
+        double u = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) u += s_w[k];
+        partial[geo.total_tiles() + im] = u / (3.0 * (double)geo.H[im] * (double)geo.W[im]);
     }
+}
+
+template <typename T>
+__global__ void l2_means_final_kernel(int n_img, const double *__restrict__ means,
+                                      T *__restrict__ loss, T *__restrict__ per_image) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double total = 0;
+    for (int im = 0; im < n_img; ++im) {
+        total += means[im];
+        if (per_image) per_image[im] = (T)means[im];
+    }
+    *loss = (T)total;
 }
 
 // ------------------------------------------------------------- backward
@@ -633,6 +643,8 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
     // fused L2: mean over this image's 3HW values (a batch sums per-image means)
     if (!cot.v_img) cot.scale = (T)(2.0 / (3.0 * (double)H * (double)W));
     const Regions R = Regions::make(GA ? 2 : 0, B);
+    T rx0 = 0, rx1 = 0, ry0 = 0, ry1 = 0;  // this warp's region (tile-local centres)
+    if (LIG_RASTER_BWD_LANE_ELLIPSE) R.rect<T>(w, rx0, rx1, ry0, ry1);
     uint16_t *my_list = s_list + w * nt;
     const PixRec<T, GA> *my_pix = s_pix + w * 32;
 
@@ -680,7 +692,7 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
         __syncthreads();
         if (tid < cnt) {
             s_rec[tid] = pre;
-            s_bits[tid] = region_bits(pre, R, tx0, ty0);
+            s_bits[tid] = region_bits<T, !LIG_RASTER_BWD_LANE_ELLIPSE>(pre, R, tx0, ty0);
             s_ids[tid] = pre_id;
         }
         __syncthreads();
@@ -692,7 +704,17 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
         int nmine = 0;
         for (int m = 0; m * 32 < cnt; ++m) {
             const int t = m * 32 + lane;
-            const bool hit = t < cnt && ((s_bits[t] >> w) & 1u);
+            bool hit = t < cnt && ((s_bits[t] >> w) & 1u);
+            if (LIG_RASTER_BWD_LANE_ELLIPSE && hit) {
+                // exact ellipse test of Gaussian t against this warp's region,
+                // one Gaussian per lane (the staging only tested the box)
+                const Rec<T> &g = s_rec[t];
+                if (g.wx >= (T)0) {
+                    const T cx = g.x - (T)tx0, cy = g.y - (T)ty0;
+                    hit = !(sigma_min_rect<T>(g.a, g.b, g.c, rx0 - cx, rx1 - cx, ry0 - cy,
+                                              ry1 - cy) > g.thr);
+                }
+            }
             const uint32_t mask = __ballot_sync(FULL, hit);
             if (hit) my_list[nmine + __popc(mask & ((1u << lane) - 1u))] = (uint16_t)t;
             nmine += __popc(mask);
@@ -944,9 +966,11 @@ int raster_fwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
                             ga ? (T *)dy : nullptr, ga ? (T *)dxy : nullptr, fin, l2);
     int launches = 1;
     if (l2.target) {
-        l2_tiles_final_kernel<T><<<1, 1024, 0, s>>>(geo, l2.tile_partial, l2o.loss,
-                                                    l2o.per_image);
-        ++launches;
+        l2_tiles_image_kernel<T><<<geo.n_img, 1024, 0, s>>>(geo, l2.tile_partial);
+        l2_means_final_kernel<T><<<1, 32, 0, s>>>(geo.n_img,
+                                                  l2.tile_partial + geo.total_tiles(),
+                                                  l2o.loss, l2o.per_image);
+        launches += 2;
     }
     note_launches(launches);
     LIG_LAUNCH_CHECK();
@@ -1241,7 +1265,8 @@ extern "C" int lig_raster_bwd_l2_batch(int dtype, int n_img, const int32_t *heig
 // and loss = sum_i mean_i((clamp(x) - target)^2) is reduced from per-tile
 // fp64 partials; lig_raster_bwd_diff then forms the loss gradient from diff.
 extern "C" size_t lig_l2_tile_partials_bytes(int num_tiles) {
-    return sizeof(double) * (size_t)(num_tiles > 0 ? num_tiles : 1);
+    // per-tile partials, then one mean per image of a batch
+    return sizeof(double) * ((size_t)(num_tiles > 0 ? num_tiles : 0) + kMaxBatch);
 }
 
 namespace lig {

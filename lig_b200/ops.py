@@ -436,7 +436,8 @@ def raster_fwd_l2(img_h, img_w, block, gaussian_ids_sorted, tile_bins, total, xy
     code = _dt(xys)
     ws, wsb = _raster_ws(code, n, dev)
     tbx, tby = tile_bounds(img_h, img_w, block)
-    part = torch.empty((tbx * tby,), dtype=torch.float64, device=dev)
+    part = torch.empty((_lib.lib.lig_l2_tile_partials_bytes(tbx * tby) // 8,), dtype=torch.float64,
+                       device=dev)
     diff = torch.empty((img_h, img_w, 3), dtype=dt, device=dev)
     fin = torch.empty((img_h, img_w), dtype=torch.int32, device=dev)
     loss = torch.empty((), dtype=dt, device=dev)

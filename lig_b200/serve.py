@@ -111,7 +111,8 @@ class Result:
     req_id: int
     kind: str
     t_submit: float
-    t_start: float = 0.0
+    t_start: float = 0.0      # dequeued / admitted
+    t_enqueued: float = 0.0   # device work enqueued (renders)
     t_done: float = 0.0
     output: object = None
     error: Optional[str] = None
@@ -294,6 +295,7 @@ class Server:
                                          (req.scale, req.scale), self.block)
                     ev = torch.cuda.Event()
                     ev.record(self.render_stream)
+                self.results[rid].t_enqueued = time.perf_counter()
                 ev.synchronize()
                 self._finish(rid, img if req.keep else None)
             except Exception as e:  # reported per request; the loop keeps serving
@@ -394,6 +396,9 @@ class WorkloadStats:
     n_fit: int = 0
     render_latency_ms: List[float] = field(default_factory=list)
     render_2048_latency_ms: List[float] = field(default_factory=list)
+    render_wait_ms: List[float] = field(default_factory=list)      # submit -> dequeue
+    render_enqueue_ms: List[float] = field(default_factory=list)   # dequeue -> enqueued
+    render_device_ms: List[float] = field(default_factory=list)    # enqueued -> done
     fit_latency_s: List[float] = field(default_factory=list)
     unfinished: int = 0
     wall_s: float = 0.0
@@ -489,6 +494,9 @@ def run_workload(server: Server, schedule, master_target: torch.Tensor, drain_s:
         if r.kind == "render":
             ms = 1e3 * r.latency
             st.render_latency_ms.append(ms)
+            st.render_wait_ms.append(1e3 * (r.t_start - r.t_submit))
+            st.render_enqueue_ms.append(1e3 * (r.t_enqueued - r.t_start))
+            st.render_device_ms.append(1e3 * (r.t_done - r.t_enqueued))
             if 1792 <= kinds[rid]["side"] <= 2304:
                 st.render_2048_latency_ms.append(ms)
         else:

@@ -67,6 +67,10 @@ def main():
         "finished": {"render": len(r), "fit": len(f)}, "unfinished": st.unfinished,
         "render_ms": {"p50": percentile(r, 50), "p99": percentile(r, 99), "n": len(r)},
         "render_2048_ms": {"p50": percentile(r2, 50), "p99": percentile(r2, 99), "n": len(r2)},
+        "render_parts_ms": {k: {"p50": percentile(v, 50), "p99": percentile(v, 99)}
+                            for k, v in (("wait", st.render_wait_ms),
+                                         ("enqueue", st.render_enqueue_ms),
+                                         ("device", st.render_device_ms))},
         "fit_s": {"p50": percentile(f, 50), "p99": percentile(f, 99), "n": len(f)},
         "throughput_per_s": {"render": len(r) / st.wall_s, "fit": len(f) / st.wall_s},
         "fit_batches": srv.fit_batches, "budget_peak_gb": srv.budget.peak / 1e9,
