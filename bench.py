@@ -48,7 +48,8 @@ N_FIT = 2_000_000
 N_TEACHER = 2_000_000
 DIAG = (0.5, 6.0)
 BLOCK = 16
-FLOP_PER_EVAL = {"lig_raster_fwd": 20.0, "lig_raster_bwd": 40.0, "lig_raster_bwd_l2": 40.0}
+FLOP_PER_EVAL = {"lig_raster_fwd": 20.0, "lig_raster_bwd": 40.0, "lig_raster_bwd_l2": 40.0,
+                 "lig_raster_fwd_l2": 20.0, "lig_raster_bwd_diff": 40.0}
 # DRAM bytes (read + write) per launch measured by an ncu capture of the same
 # kernels on the 2048^2 / 125k-Gaussian step (same density); traffic grows
 # with pixels and Gaussians, so a size-S launch is scaled by (S / 2048)^2.
@@ -158,13 +159,13 @@ def evaluations(fit) -> tuple[int, int]:
 
 
 # -------------------------------------------------------------- CPU side
-def cpu_band_sample(size, n, target_secs, steps):
+def cpu_band_sample(size, n, target_secs, steps, diag=DIAG):
     """Time the oracle (C restatement, OpenMP) on horizontal bands of the
     workload; returns (iters/s for the full image, cores, description)."""
     from lig_b200 import synthetic
     from oracle import oracle as O
     cores = os.cpu_count() or 1
-    means, chol, colors = synthetic.gaussians(n, size, size, diag=DIAG, seed=synthetic.SEED_INIT)
+    means, chol, colors = synthetic.gaussians(n, size, size, diag=diag, seed=synthetic.SEED_INIT)
     means, chol, colors = means.numpy(), chol.numpy(), colors.numpy()
     rng = np.random.default_rng(0)
 

@@ -146,6 +146,10 @@ def run(name):
     out["ref_iters_per_s"] = timed(theirs, target, iters)
     del theirs
     out["speedup"] = out["lig_iters_per_s"] / out["ref_iters_per_s"]
+    if name == "c0":  # the C restatement (oracle/, OpenMP) on this host's cores
+        import bench
+        v, cores, _, _, _ = bench.cpu_band_sample(size, n, 5.0, 3, diag=diag)
+        out.update(cpu_iters_per_s=v, cpu_cores=cores)
     if piters:
         mine, theirs = LevelFit(n, size, size, lr=1e-3, diag=diag), RefFit(n, size, size, diag)
         for _ in range(piters):
