@@ -229,6 +229,14 @@ class BatchedFit:
                 dst.copy_(src)
         self.steps[i] = int(st.step)
 
+    def export_states(self) -> List["FitState"]:
+        """Every image's state at once: three buffer copies and one read of
+        the step counts (the per-image states are views into the copies)."""
+        flat, m, v = self.flat.clone(), self.m.clone(), self.v.clone()
+        steps = self.steps.tolist()
+        return [FitState(self._segments(flat, i), self._segments(m, i), self._segments(v, i),
+                         steps[i]) for i in range(self.L.n)]
+
     def state_of(self, i: int) -> "FitState":
         """Copy of image i's parameters, Adam moments and step (device)."""
         seg = lambda buf: tuple(t.clone() for t in self._segments(buf, i))  # noqa: E731

@@ -480,17 +480,20 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
 #define LIG_RASTER_FWD_MINB 4
 #endif
 #ifndef LIG_RASTER_BWD_LANE_ELLIPSE
-#define LIG_RASTER_BWD_LANE_ELLIPSE 0
+#define LIG_RASTER_BWD_LANE_ELLIPSE 1  // ellipse culling by the warp's lanes (measured faster)
 #endif
 #ifndef LIG_RASTER_BWD_MINB
 #define LIG_RASTER_BWD_MINB 5
 #endif
 
-#ifndef LIG_RASTER_FWD_PPL
-#define LIG_RASTER_FWD_PPL 2
+// Sum forward: two pixels per lane from LIG_RASTER_PPL2_MIN_TILES tiles on
+// (fewer warps per tile; small images keep one pixel per lane so the grid
+// still fills the GPU).
+#ifndef LIG_RASTER_PPL2_MIN_TILES
+#define LIG_RASTER_PPL2_MIN_TILES 0
 #endif
 
-template <typename T, bool GA, int MAXT, int MINB>
+template <typename T, bool GA, int PPL, int MAXT, int MINB>
 __global__ void __launch_bounds__(MAXT, MINB)
 raster_fwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work,
                   const int32_t *__restrict__ ids, const int2 *__restrict__ tile_bins,
@@ -506,9 +509,8 @@ raster_fwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work
     for (int tile = next_tile(work, s_slot, true); tile < n_tiles;
          tile = next_tile(work, s_slot, false)) {
         const TileCtx tc = tile_ctx(geo, cum, d_total, tile);
-        fwd_tile<T, GA, GA ? 1 : LIG_RASTER_FWD_PPL>(tc, tile, ids, tile_bins, recs, img, wsum,
-                                                     odx, ody, odxy, final_idx, s_rec, s_bits,
-                                                     l2);
+        fwd_tile<T, GA, PPL>(tc, tile, ids, tile_bins, recs, img, wsum, odx, ody, odxy,
+                             final_idx, s_rec, s_bits, l2);
     }
 }
 
@@ -942,17 +944,19 @@ int raster_fwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
     int rc = pack<T>(n, xys, con, col, op, ws, ws_bytes, s);
     if (rc) return rc;
     const bool ga = dx != nullptr;
-    const int kind = (!ga && LIG_RASTER_FWD_PPL == 2) ? 1 : 0;
-    const int nt = 32 * Regions::make(kind, geo.B).count;
+    const bool ppl2 = !ga && geo.total_tiles() >= LIG_RASTER_PPL2_MIN_TILES;
+    const int nt = 32 * Regions::make(ppl2 ? 1 : 0, geo.B).count;
     const size_t sm = (size_t)nt * (sizeof(Rec<T>) + sizeof(uint32_t));
     using K = void (*)(const BatchGeo, const int32_t *, int *, const int32_t *, const int2 *,
                        const int32_t *, const Rec<T> *, T *, T *, T *, T *, T *, int32_t *,
                        L2Fwd<T>);
     const bool small = nt <= 256;
-    K fn = ga ? (small ? raster_fwd_kernel<T, true, 256, LIG_RASTER_FWD_MINB>
-                       : raster_fwd_kernel<T, true, 1024, 1>)
-              : (small ? raster_fwd_kernel<T, false, 256, LIG_RASTER_FWD_MINB>
-                       : raster_fwd_kernel<T, false, 1024, 1>);
+    K fn = ga ? (small ? raster_fwd_kernel<T, true, 1, 256, LIG_RASTER_FWD_MINB>
+                       : raster_fwd_kernel<T, true, 1, 1024, 1>)
+              : ppl2 ? (small ? raster_fwd_kernel<T, false, 2, 256, LIG_RASTER_FWD_MINB>
+                              : raster_fwd_kernel<T, false, 2, 1024, 1>)
+                     : (small ? raster_fwd_kernel<T, false, 1, 256, LIG_RASTER_FWD_MINB>
+                              : raster_fwd_kernel<T, false, 1, 1024, 1>);
     if (!set_dyn_smem((const void *)fn, sm)) return LIG_ERR_LAUNCH;
     int grid = geo.total_tiles();
     if (walk.work) {

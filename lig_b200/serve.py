@@ -26,6 +26,7 @@ from __future__ import annotations
 
 import collections
 import math
+import sys
 import threading
 import time
 from dataclasses import dataclass, field
@@ -222,6 +223,10 @@ class Server:
         return rid
 
     def start(self):
+        # the render thread needs the GIL back within a fraction of a
+        # millisecond while the fit thread runs Python between launches
+        self._switch = sys.getswitchinterval()
+        sys.setswitchinterval(2e-4)
         self._running = True
         self._threads = [threading.Thread(target=self._render_loop, name="lig-render",
                                           daemon=True),
@@ -254,6 +259,9 @@ class Server:
             self._cv.notify_all()
         for t in self._threads:
             t.join()
+        if getattr(self, "_switch", None) is not None:
+            sys.setswitchinterval(self._switch)
+            self._switch = None
 
     def _finish(self, rid: int, output=None, error: Optional[str] = None):
         with self._cv:
@@ -361,8 +369,8 @@ class Server:
                 try:
                     if changed or batch is None:
                         if batch is not None:  # carry running jobs over
-                            for i, j in enumerate(batch_jobs):
-                                j.state = batch.state_of(i)
+                            for j, st in zip(batch_jobs, batch.export_states()):
+                                j.state = st
                             batch = None
                         batch_jobs = list(active)
                         batch = self._build_batch(batch_jobs)
@@ -378,11 +386,11 @@ class Server:
                     j.done += k
                 finished = [j for j in batch_jobs if j.done >= j.req.iters]
                 if finished:
-                    for i, j in enumerate(batch_jobs):
-                        st = batch.state_of(i)
+                    for j, st in zip(batch_jobs, batch.export_states()):
                         if j.done >= j.req.iters:
                             self.budget.release(j.reserved)
-                            self._finish(j.req_id, st.params if j.req.keep else None)
+                            out = tuple(t.clone() for t in st.params) if j.req.keep else None
+                            self._finish(j.req_id, out)
                         else:
                             j.state = st
                     active = [j for j in active if j.done < j.req.iters]
