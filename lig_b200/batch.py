@@ -213,6 +213,7 @@ class BatchedFit:
         self.gids = None
         self.bin_ws = None
         self.graph: Optional[torch.cuda.CUDAGraph] = None
+        self._graphs: dict = {}
         self.stats = BatchStats()
         self._size_capacity(self._count_intersections())
 
@@ -270,6 +271,7 @@ class BatchedFit:
         self.bin_ws = torch.empty(nb, dtype=torch.uint8, device=self.dev)
         self.stats.capacity = cap
         self.graph = None
+        self._graphs = {}
 
     # -------------------------------------------------------- the iteration
     def _bin(self, st):
@@ -288,16 +290,18 @@ class BatchedFit:
              _p(self.rgbs), None, int(self.persistent), _p(self.work), _p(self.r_ws),
              self.r_ws.numel(), _p(self.img), _p(self.wsum), None, None, None, _p(self.fin), st)
 
-    def _enqueue_step(self):
+    def _enqueue_step(self, target: Optional[torch.Tensor] = None):
         """Forward with the loss fused in (self.img receives the masked
         difference clamp(x) - target, self.loss / self.per_image the losses),
-        the backward from that difference, the projection backward and Adam."""
+        the backward from that difference, the projection backward and Adam.
+        target: the concatenated [pixels, 3] target (default self.target)."""
         L = self.L
         st = self._stream()
+        tgt = self.target if target is None else target
         self._bin(st)
         call("lig_raster_fwd_l2_batch", _lib.LIG_F32, *L.args(), L.block, _p(self.gids),
              _p(self.bins), _p(self.total), _p(self.cum), _p(self.xys), _p(self.con),
-             _p(self.rgbs), None, _p(self.target), int(self.persistent), _p(self.work),
+             _p(self.rgbs), None, _p(tgt), int(self.persistent), _p(self.work),
              _p(self.r_ws), self.r_ws.numel(), _p(self.partials), _p(self.img), _p(self.fin),
              _p(self.loss), _p(self.per_image), st)
         call("lig_raster_bwd_diff_batch", _lib.LIG_F32, *L.args(), L.block, _p(self.gids),
@@ -313,7 +317,7 @@ class BatchedFit:
              _p(self.skipped), _p(self.adam_scratch), self.adam_scratch.numel(), st)
         self.host_skipped.copy_(self.skipped, non_blocking=True)
 
-    def _capture(self):
+    def _capture(self, target: Optional[torch.Tensor] = None):
         """Capture one iteration on a side stream.  capture_begin/end rather
         than the torch.cuda.graph context manager, which also runs the
         Python garbage collector (holding the GIL) and empties the allocator
@@ -327,12 +331,12 @@ class BatchedFit:
         with torch.cuda.stream(side):
             g.capture_begin(capture_error_mode="thread_local")
             try:
-                self._enqueue_step()
+                self._enqueue_step(target)
             finally:
                 g.capture_end()
         cur.wait_stream(side)
-        self.graph = g
         self.stats.recaptures += 1
+        return g
 
     def _recover(self):
         """A step overflowed the capacity (and was skipped): grow, recapture."""
@@ -344,16 +348,45 @@ class BatchedFit:
         self._size_capacity(self._count_intersections())
         return k
 
-    def step(self):
+    def _target_arg(self, target: Optional[torch.Tensor]) -> Optional[torch.Tensor]:
+        if target is None:
+            return None
+        t = target.reshape(-1, 3)
+        if (t.dtype != torch.float32 or t.device != self.dev or not t.is_contiguous()
+                or t.shape[0] != self.L.pixels):
+            raise ValueError("target must be a contiguous float32 CUDA tensor with the batch's "
+                             "[pixels, 3] values")
+        return t
+
+    def step(self, target: Optional[torch.Tensor] = None):
         """One iteration (render, loss, backward, Adam) for every image; no
-        host synchronisation unless a capacity overflow is being recovered."""
-        if self.use_graph and self.graph is None and self.stats.iters >= 2:
-            self._capture()
-        if self.graph is not None:
-            self.graph.replay()
+        host synchronisation unless a capacity overflow is being recovered.
+        target (optional): fit against this [pixels, 3] buffer instead of the
+        constructor's targets, read in place; one captured graph is kept per
+        target buffer (a caller alternating two upload buffers replays two
+        graphs, no copies)."""
+        t = self._target_arg(target)
+        key = 0 if t is None else t.data_ptr()
+        g = self._graphs.get(key)
+        if g is None and self.use_graph and self.stats.iters >= 2:
+            if len(self._graphs) >= 4:
+                self._graphs.clear()
+            g = self._graphs[key] = self._capture(t)
+            self.graph = g
+        if g is not None:
+            g.replay()
         else:
-            self._enqueue_step()
+            self._enqueue_step(t)
         self.stats.iters += 1
+
+    def step_checked(self, target: Optional[torch.Tensor] = None):
+        """step(), then — if an earlier step was skipped for a capacity
+        overflow (noticed without a sync through the pinned counter) — grow
+        the capacity and redo the skipped steps."""
+        self.step(target)
+        while int(self.host_skipped[0]) > 0:
+            for _ in range(self._recover()):
+                self.step(target)
 
     def fit(self, iters: int) -> BatchStats:
         """Run until `iters` Adam steps have been applied (skipped steps are

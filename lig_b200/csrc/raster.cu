@@ -514,16 +514,38 @@ raster_fwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work
     }
 }
 
-// Loss from the tile partials, deterministic: block i sums image i's tile
-// partials (thread-strided, then a fixed-order block reduction) into the
-// image's mean partial[T + i] = sum / (3 H_i W_i); one warp then adds the
-// means in image order.
-template <typename T>
-__global__ void __launch_bounds__(1024)
-l2_tiles_image_kernel(const BatchGeo geo, double *__restrict__ partial) {
-    __shared__ double s_w[32];
-    const int im = blockIdx.x;
-    const int k0 = geo.tile_off[im], k1 = geo.tile_off[im + 1];
+// Loss from the tile partials, deterministic.  Pass 1: each CTA sums a
+// chunk of kLossChunk tile partials of one image (thread-strided, then a
+// fixed-order block reduction); image i owns CTAs [chunk_off[i],
+// chunk_off[i+1]).  Pass 2: one warp per image adds its chunk sums in order
+// (lane-strided + butterfly) and divides by 3 H_i W_i; thread 0 adds the
+// image means in order.
+constexpr int kLossChunk = 4096;
+
+struct TileChunks {
+    int n_img;
+    int chunk_off[kMaxBatch + 1];
+};
+
+inline TileChunks tile_chunks(const BatchGeo &geo) {
+    TileChunks c;
+    c.n_img = geo.n_img;
+    c.chunk_off[0] = 0;
+    for (int i = 0; i < geo.n_img; ++i) {
+        const int t = geo.tile_off[i + 1] - geo.tile_off[i];
+        c.chunk_off[i + 1] = c.chunk_off[i] + (t + kLossChunk - 1) / kLossChunk;
+    }
+    return c;
+}
+
+__global__ void __launch_bounds__(256)
+l2_tiles_chunk_kernel(const BatchGeo geo, const TileChunks ch, const double *__restrict__ partial,
+                      double *__restrict__ chunk_sum) {
+    __shared__ double s_w[8];
+    const int b = blockIdx.x;
+    const int im = BatchGeo::find(ch.chunk_off, ch.n_img, b);
+    const int k0 = geo.tile_off[im] + (b - ch.chunk_off[im]) * kLossChunk;
+    const int k1 = min(k0 + kLossChunk, geo.tile_off[im + 1]);
     double t = 0;
     for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) t += partial[k];
 #pragma unroll
@@ -534,20 +556,34 @@ l2_tiles_image_kernel(const BatchGeo geo, double *__restrict__ partial) {
     if (threadIdx.x == 0) {
         double u = 0;
         for (int k = 0; k < (int)(blockDim.x >> 5); ++k) u += s_w[k];
-        partial[geo.total_tiles() + im] = u / (3.0 * (double)geo.H[im] * (double)geo.W[im]);
+        chunk_sum[b] = u;
     }
 }
 
 template <typename T>
-__global__ void l2_means_final_kernel(int n_img, const double *__restrict__ means,
-                                      T *__restrict__ loss, T *__restrict__ per_image) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double total = 0;
-    for (int im = 0; im < n_img; ++im) {
-        total += means[im];
-        if (per_image) per_image[im] = (T)means[im];
+__global__ void __launch_bounds__(1024)
+l2_chunks_final_kernel(const BatchGeo geo, const TileChunks ch,
+                       const double *__restrict__ chunk_sum, T *__restrict__ loss,
+                       T *__restrict__ per_image) {
+    __shared__ double s_mean[kMaxBatch];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int im = w; im < geo.n_img; im += 32) {
+        double t = 0;
+        for (int k = ch.chunk_off[im] + lane; k < ch.chunk_off[im + 1]; k += 32) t += chunk_sum[k];
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+        if (lane == 0) {
+            const double m = t / (3.0 * (double)geo.H[im] * (double)geo.W[im]);
+            s_mean[im] = m;
+            if (per_image) per_image[im] = (T)m;
+        }
     }
-    *loss = (T)total;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double total = 0;
+        for (int im = 0; im < geo.n_img; ++im) total += s_mean[im];
+        *loss = (T)total;
+    }
 }
 
 // ------------------------------------------------------------- backward
@@ -970,10 +1006,12 @@ int raster_fwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
                             ga ? (T *)dy : nullptr, ga ? (T *)dxy : nullptr, fin, l2);
     int launches = 1;
     if (l2.target) {
-        l2_tiles_image_kernel<T><<<geo.n_img, 1024, 0, s>>>(geo, l2.tile_partial);
-        l2_means_final_kernel<T><<<1, 32, 0, s>>>(geo.n_img,
-                                                  l2.tile_partial + geo.total_tiles(),
-                                                  l2o.loss, l2o.per_image);
+        const TileChunks ch = tile_chunks(geo);
+        double *chunk_sum = l2.tile_partial + geo.total_tiles();
+        if (ch.chunk_off[geo.n_img] > 0)
+            l2_tiles_chunk_kernel<<<ch.chunk_off[geo.n_img], 256, 0, s>>>(geo, ch, l2.tile_partial,
+                                                                         chunk_sum);
+        l2_chunks_final_kernel<T><<<1, 1024, 0, s>>>(geo, ch, chunk_sum, l2o.loss, l2o.per_image);
         launches += 2;
     }
     note_launches(launches);
@@ -1269,8 +1307,10 @@ extern "C" int lig_raster_bwd_l2_batch(int dtype, int n_img, const int32_t *heig
 // and loss = sum_i mean_i((clamp(x) - target)^2) is reduced from per-tile
 // fp64 partials; lig_raster_bwd_diff then forms the loss gradient from diff.
 extern "C" size_t lig_l2_tile_partials_bytes(int num_tiles) {
-    // per-tile partials, then one mean per image of a batch
-    return sizeof(double) * ((size_t)(num_tiles > 0 ? num_tiles : 0) + kMaxBatch);
+    // per-tile partials, then the chunk sums (at most one per kLossChunk
+    // tiles plus one per image of a batch)
+    const size_t t = (size_t)(num_tiles > 0 ? num_tiles : 0);
+    return sizeof(double) * (t + t / kLossChunk + 1 + kMaxBatch);
 }
 
 namespace lig {

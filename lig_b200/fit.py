@@ -23,13 +23,24 @@ from .gsplat2d import gradient_aware_upscale, project_gaussians_cholesky, raster
 
 
 class LevelFit:
-    """One LIG level: N Gaussians fitted to an [H, W, 3] target."""
+    """One LIG level: N Gaussians fitted to an [H, W, 3] target.
+
+    engine "graph" (default): the iteration runs as a one-image BatchedFit —
+    fused-loss forward, backward from the masked difference, projection
+    backward and the flat guarded Adam, captured as a CUDA graph (one per
+    target buffer), no autograd and no per-step host work.  engine
+    "autograd": the drop-in gsplat2d API under torch autograd with
+    torch.optim.Adam (fused_loss selects the fused render + L2 node or the
+    plain clamp + F.mse_loss chain)."""
 
     def __init__(self, n: int, H: int, W: int, device="cuda", lr: float = 1e-3, block: int = 16,
                  diag=(0.5, 6.0), seed: int = synthetic.SEED_INIT, fused_adam: bool = True,
-                 fused_loss: bool = True):
-        self.H, self.W, self.block = H, W, block
+                 fused_loss: bool = True, engine: str = "graph"):
+        if engine not in ("graph", "autograd"):
+            raise ValueError("engine must be 'graph' or 'autograd'")
+        self.H, self.W, self.block, self.lr = H, W, block, lr
         self.fused_loss = fused_loss
+        self.engine = engine if fused_loss else "autograd"
         means, chol, colors = synthetic.gaussians(n, H, W, diag=diag, seed=seed)
         self.means = torch.nn.Parameter(means.to(device))
         self.chol = torch.nn.Parameter(chol.to(device))
@@ -37,6 +48,7 @@ class LevelFit:
         self.params = [self.rgbs, self.means, self.chol]
         kw = {"fused": True} if fused_adam and torch.device(device).type == "cuda" else {}
         self.opt = torch.optim.Adam(self.params, lr=lr, **kw)
+        self._batch = None
 
     @property
     def n(self) -> int:
@@ -48,10 +60,26 @@ class LevelFit:
         return rasterize_gaussians(xys, ext, con, cnt, self.rgbs, None, self.H, self.W,
                                    self.block, compute_upscale_gradients=grad_aware)
 
+    def _graph_step(self, target_hwc: torch.Tensor) -> torch.Tensor:
+        if self._batch is None:
+            from .batch import BatchedFit
+            with torch.no_grad():
+                init = [(self.means.detach(), self.chol.detach(), self.rgbs.detach())]
+            self._batch = BatchedFit([target_hwc], [self.n], block=self.block, lr=self.lr,
+                                     init=init, graph=True)
+            b = self._batch
+            # the parameters now live in the batch's flat buffer
+            self.means, self.chol, self.rgbs = b.means, b.chol, b.rgbs
+            self.params = [self.rgbs, self.means, self.chol]
+        self._batch.step_checked(target_hwc)
+        return self._batch.loss
+
     def step(self, target_hwc: torch.Tensor) -> torch.Tensor:
         """One iteration: render, clamp, L2, backward, Adam.  Returns the loss
-        as a device tensor (no host synchronisation).  fused_loss=True runs the
-        same math through the fused render+L2 node (lig_b200.fused)."""
+        as a device tensor (no host synchronisation; with the graph engine a
+        buffer that the next step overwrites)."""
+        if self.engine == "graph":
+            return self._graph_step(target_hwc.contiguous())
         if self.fused_loss:
             loss = render_l2_loss(self.chol, self.means, self.rgbs, None, target_hwc, self.H,
                                   self.W, self.block)

@@ -205,6 +205,7 @@ class Server:
         self._threads: List[threading.Thread] = []
         self.fit_batches = 0
         self.errors: List[str] = []
+        self.fit_phases: List[tuple] = []  # (t0, t1, phase) of the fit thread
 
     # ----------------------------------------------------------- resources
     def add_set(self, set_id: str, gs: GaussianSet):
@@ -368,14 +369,18 @@ class Server:
                     continue
                 try:
                     if changed or batch is None:
+                        t0 = time.perf_counter()
                         if batch is not None:  # carry running jobs over
                             for j, st in zip(batch_jobs, batch.export_states()):
                                 j.state = st
                             batch = None
                         batch_jobs = list(active)
                         batch = self._build_batch(batch_jobs)
+                        self.fit_phases.append((t0, time.perf_counter(), "build"))
                     k = min(self.fit_chunk, min(j.req.iters - j.done for j in batch_jobs))
+                    t0 = time.perf_counter()
                     batch.fit(k)
+                    self.fit_phases.append((t0, time.perf_counter(), "iterate"))
                 except Exception as e:  # fail this batch's jobs, keep serving
                     for j in active:
                         self.budget.release(j.reserved)
@@ -386,6 +391,7 @@ class Server:
                     j.done += k
                 finished = [j for j in batch_jobs if j.done >= j.req.iters]
                 if finished:
+                    t0 = time.perf_counter()
                     for j, st in zip(batch_jobs, batch.export_states()):
                         if j.done >= j.req.iters:
                             self.budget.release(j.reserved)
@@ -395,6 +401,7 @@ class Server:
                             j.state = st
                     active = [j for j in active if j.done < j.req.iters]
                     batch, batch_jobs = None, []
+                    self.fit_phases.append((t0, time.perf_counter(), "finish"))
 
 
 # ------------------------------------------------------------------ workload
@@ -410,6 +417,7 @@ class WorkloadStats:
     fit_latency_s: List[float] = field(default_factory=list)
     unfinished: int = 0
     wall_s: float = 0.0
+    slow_render_phases: dict = field(default_factory=dict)  # fit phase overlapping a slow wait
 
 
 def percentile(xs: List[float], q: float) -> float:
@@ -509,4 +517,11 @@ def run_workload(server: Server, schedule, master_target: torch.Tensor, drain_s:
                 st.render_2048_latency_ms.append(ms)
         else:
             st.fit_latency_s.append(r.latency)
+    # which fit-thread phase overlapped the renders that waited > 20 ms
+    for rid, r in server.results.items():
+        if r.kind != "render" or r.t_done == 0.0 or r.t_start - r.t_submit <= 0.02:
+            continue
+        hit = [ph for (a, b, ph) in server.fit_phases if a < r.t_start and b > r.t_submit]
+        key = "+".join(sorted(set(hit))) or "none"
+        st.slow_render_phases[key] = st.slow_render_phases.get(key, 0) + 1
     return st

@@ -42,6 +42,7 @@ def main():
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--sets", type=int, default=64)
     ap.add_argument("--fit-chunk", type=int, default=20)
+    ap.add_argument("--no-fit-graph", action="store_true")
     a = ap.parse_args()
     t0 = time.time()
     sets = resident_sets(a.sets)
@@ -49,7 +50,8 @@ def main():
                          noise="white", noise_std=0.02)
     schedule = poisson_requests(a.duration, a.rate, a.fit_frac, sets, fit_iters=a.fit_iters,
                                 seed=5000)
-    srv = Server(budget_bytes=int(a.budget_gb * 1e9), fit_chunk=a.fit_chunk)
+    srv = Server(budget_bytes=int(a.budget_gb * 1e9), fit_chunk=a.fit_chunk,
+                 fit_graph=not a.no_fit_graph)
     for k, gs in sets.items():
         srv.add_set(k, gs)
     # warm the render path (library load, allocator) before the clock starts
@@ -73,6 +75,9 @@ def main():
                                          ("device", st.render_device_ms))},
         "fit_s": {"p50": percentile(f, 50), "p99": percentile(f, 99), "n": len(f)},
         "throughput_per_s": {"render": len(r) / st.wall_s, "fit": len(f) / st.wall_s},
+        "slow_render_fit_phases": st.slow_render_phases,
+        "fit_phase_s": {ph: round(sum(b - a for a, b, p in srv.fit_phases if p == ph), 2)
+                        for ph in ("build", "iterate", "finish")},
         "fit_batches": srv.fit_batches, "budget_peak_gb": srv.budget.peak / 1e9,
         "errors": srv.errors[:5],
     }

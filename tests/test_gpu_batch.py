@@ -270,3 +270,31 @@ def test_batched_adam_per_image_steps_match_single_adam():
                      ops._p(mq), ops._p(vq), 1e-2, 0.9, 0.999, 1e-8, None, ops._p(s1), None,
                      ops._p(sc1), st)
         assert torch.allclose(parts(p, i), q, rtol=1e-6, atol=1e-7)
+
+
+def test_levelfit_graph_engine_matches_autograd_engine():
+    """LevelFit's CUDA-graph engine (one-image BatchedFit, flat Adam) follows
+    the autograd engine (drop-in API + torch Adam); alternating two target
+    buffers replays one graph per buffer with the same results."""
+    from lig_b200.fit import LevelFit
+    H, W, n = 96, 112, 1500
+    g = torch.Generator().manual_seed(12)
+    target = torch.rand(H, W, 3, generator=g).cuda()
+    a = LevelFit(n, H, W, lr=1e-2, diag=(0.5, 4.0), engine="graph")
+    b = LevelFit(n, H, W, lr=1e-2, diag=(0.5, 4.0), engine="autograd")
+    c = LevelFit(n, H, W, lr=1e-2, diag=(0.5, 4.0), engine="graph")
+    bufs = [target.clone(), target.clone()]
+    la, lb = [], []
+    for k in range(8):
+        la.append(float(a.step(target)))
+        lb.append(float(b.step(target)))
+        c.step(bufs[k % 2])
+    assert a._batch.graph is not None and len(c._batch._graphs) == 2
+    for x, y in zip(la, lb):
+        assert abs(x - y) <= 1e-4 * abs(y)
+    for p, q in zip((a.means, a.chol, a.rgbs), (b.means, b.chol, b.rgbs)):
+        d = (p - q.detach()).abs()
+        assert float((d > 1e-4).float().mean()) < 0.01 and float(d.median()) <= 1e-6
+    for p, q in zip((a.means, a.chol, a.rgbs), (c.means, c.chol, c.rgbs)):
+        d = (p - q).abs()
+        assert float((d > 1e-4).float().mean()) < 0.01 and float(d.median()) <= 1e-6
