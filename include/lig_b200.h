@@ -162,7 +162,9 @@ int lig_raster_bwd(int dtype, int img_h, int img_w, int block_width, int num_poi
  * the gradient of mean((clamp(img, 0, 1) - target)^2) times the device scalar
  * *grad_loss, computed per pixel from img and target (both [H,W,3]) instead
  * of read from a materialised dL/dimg; wsum cotangent zero.  Otherwise as
- * lig_raster_bwd.  Replaces, in the fit loop, the clamp + F.mse_loss backward
+ * lig_raster_bwd, except that with opacities == NULL v_xy_abs is written as
+ * zeros (the fit uses neither it nor an opacity gradient, so the kernel
+ * skips both).  Replaces, in the fit loop, the clamp + F.mse_loss backward
  * of gaussianlig.py:95-103 feeding rasterize_backward_tensor
  * (csrc/bindings.cu:403-506). */
 int lig_raster_bwd_l2(int dtype, int img_h, int img_w, int block_width, int num_points,
@@ -192,7 +194,9 @@ int lig_raster_fwd_l2(int dtype, int img_h, int img_w, int block_width, int num_
                       void *diff, int32_t *final_idx, void *loss, void *stream);
 
 /* Sum backward of that loss from the forward's diff: pixel cotangent
- * diff * 2 / (3 H W) * grad_loss (equal to lig_raster_bwd_l2's). */
+ * diff * 2 / (3 H W) * grad_loss (equal to lig_raster_bwd_l2's).  As in
+ * lig_raster_bwd_l2, with opacities == NULL the fit needs neither |v_xy| nor
+ * an opacity gradient: v_xy_abs is written as zeros and not accumulated. */
 int lig_raster_bwd_diff(int dtype, int img_h, int img_w, int block_width, int num_points,
                         const int32_t *gaussian_ids_sorted, const int32_t *tile_bins,
                         const int32_t *num_intersects, const void *xys, const void *conics,

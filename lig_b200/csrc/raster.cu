@@ -657,7 +657,11 @@ struct alignas(16) PixRec {
     T vd[GA ? 9 : 1];  // vdx.rgb, vdy.rgb, vdxy.rgb
 };
 
-template <typename T, bool GA>
+// LEAN (sum backward of the fused fit loss, no opacities, no wsum
+// cotangent): only the gradients the fit needs — v_xy, v_conic, v_rgb — are
+// accumulated (no |v_xy| sums, no opacity gradient) and each (Gaussian,
+// region) pair adds them with two 16-byte atomics into an [N][8] buffer.
+template <typename T, bool GA, bool LEAN>
 __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
                                          const int32_t *__restrict__ ids,
                                          const int2 *__restrict__ tile_bins,
@@ -786,8 +790,10 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
                     v_alpha += g.r * c.vo0;
                     v_alpha += g.g * c.vo1;
                     v_alpha += g.bl * c.vo2;
-                    v_alpha += c.vw;
-                    acc[10] += vis * v_alpha;
+                    if constexpr (!LEAN) {
+                        v_alpha += c.vw;
+                        acc[10] += vis * v_alpha;
+                    }
                     const T v_sigma = -alpha * v_alpha;
                     acc[4] += (T)0.5 * v_sigma * dx * dx;
                     acc[5] += v_sigma * dx * dy;
@@ -796,8 +802,10 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
                     const T gy = v_sigma * (g.b * dx + g.c * dy);
                     acc[0] += gx;
                     acc[1] += gy;
-                    acc[2] += M::abs_(gx);
-                    acc[3] += M::abs_(gy);
+                    if constexpr (!LEAN) {
+                        acc[2] += M::abs_(gx);
+                        acc[3] += M::abs_(gy);
+                    }
                 } else {
                     // csrc/gradient_aware_rasterizer.cu:201-315
                     const T dx = c.px - g.x;
@@ -846,22 +854,37 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
                     acc[2] = M::abs_(acc[0]);
                     acc[3] = M::abs_(acc[1]);
                 }
-                T *dst = packed + (size_t)s_ids[slot] * 12;
-                if constexpr (sizeof(T) == 4) {
-                    float4 *d4 = reinterpret_cast<float4 *>(dst);
-                    atomicAdd(d4, make_float4(acc[0], acc[1], acc[2], acc[3]));
-                    atomicAdd(d4 + 1, make_float4(acc[4], acc[5], acc[6], acc[7]));
-                    atomicAdd(d4 + 2, make_float4(acc[8], acc[9], acc[10], 0.f));
-                } else {
+                if constexpr (LEAN) {
+                    // [xy, conic, rgb]
+                    T *dst = packed + (size_t)s_ids[slot] * 8;
+                    if constexpr (sizeof(T) == 4) {
+                        float4 *d4 = reinterpret_cast<float4 *>(dst);
+                        atomicAdd(d4, make_float4(acc[0], acc[1], acc[4], acc[5]));
+                        atomicAdd(d4 + 1, make_float4(acc[6], acc[7], acc[8], acc[9]));
+                    } else {
+                        const T v[8] = {acc[0], acc[1], acc[4], acc[5],
+                                        acc[6], acc[7], acc[8], acc[9]};
 #pragma unroll
-                    for (int q = 0; q < 11; ++q) atomicAdd(dst + q, acc[q]);
+                        for (int q = 0; q < 8; ++q) atomicAdd(dst + q, v[q]);
+                    }
+                } else {
+                    T *dst = packed + (size_t)s_ids[slot] * 12;
+                    if constexpr (sizeof(T) == 4) {
+                        float4 *d4 = reinterpret_cast<float4 *>(dst);
+                        atomicAdd(d4, make_float4(acc[0], acc[1], acc[2], acc[3]));
+                        atomicAdd(d4 + 1, make_float4(acc[4], acc[5], acc[6], acc[7]));
+                        atomicAdd(d4 + 2, make_float4(acc[8], acc[9], acc[10], 0.f));
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < 11; ++q) atomicAdd(dst + q, acc[q]);
+                    }
                 }
             }
         }
     }
 }
 
-template <typename T, bool GA, int MAXT, int MINB>
+template <typename T, bool GA, bool LEAN, int MAXT, int MINB>
 __global__ void __launch_bounds__(MAXT, MINB)
 raster_bwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work,
                   const int32_t *__restrict__ ids, const int2 *__restrict__ tile_bins,
@@ -874,12 +897,29 @@ raster_bwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work
     for (int tile = next_tile(work, s_slot, true); tile < n_tiles;
          tile = next_tile(work, s_slot, false)) {
         const TileCtx tc = tile_ctx(geo, cum, d_total, tile);
-        bwd_tile<T, GA>(tc, tile, ids, tile_bins, recs, final_idx, cot, v_dx, v_dy, v_dxy, clamp,
-                        packed, s_end);
+        bwd_tile<T, GA, LEAN>(tc, tile, ids, tile_bins, recs, final_idx, cot, v_dx, v_dy, v_dxy,
+                              clamp, packed, s_end);
     }
 }
 
 // Packed per-Gaussian gradients [N][12] -> the five output arrays of the ABI.
+template <typename T>
+__global__ void unpack_lean_grads_kernel(int n, const T *__restrict__ packed, Grads<T> out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const T *g = packed + (size_t)i * 8;
+    out.v_xy[2 * i] = g[0];
+    out.v_xy[2 * i + 1] = g[1];
+    out.v_abs[2 * i] = 0;
+    out.v_abs[2 * i + 1] = 0;
+    out.v_conic[3 * i] = g[2];
+    out.v_conic[3 * i + 1] = g[3];
+    out.v_conic[3 * i + 2] = g[4];
+    out.v_rgb[3 * i] = g[5];
+    out.v_rgb[3 * i + 1] = g[6];
+    out.v_rgb[3 * i + 2] = g[7];
+}
+
 template <typename T>
 __global__ void unpack_grads_kernel(int n, const T *__restrict__ packed, Grads<T> out) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1034,11 +1074,15 @@ int raster_bwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
     const int n = geo.total_points();
     const size_t goff = bwd_grad_offset<T>(n);
     if (ws_bytes < goff + sizeof(T) * 12 * (size_t)n) return LIG_ERR_WORKSPACE;
+    const bool ga = v_dx != nullptr;
+    // the fused-loss backward without opacities needs neither |v_xy| nor an
+    // opacity gradient (nor a wsum cotangent)
+    const bool lean = !ga && !cot.v_img && !cot.v_wsum && !op && !v_op;
+    const int stride = lean ? 8 : 12;
     T *packed = reinterpret_cast<T *>((char *)ws + goff);
-    cudaMemsetAsync(packed, 0, sizeof(T) * 12 * (size_t)n, s);
+    cudaMemsetAsync(packed, 0, sizeof(T) * stride * (size_t)n, s);
     int rc = pack<T>(n, xys, con, col, op, ws, goff, s);
     if (rc) return rc;
-    const bool ga = v_dx != nullptr;
     const T cl = (T)(clamp > 0 ? clamp : (ga ? 0.999 : 0.99));
     const int nt = 32 * Regions::make(ga ? 2 : 0, geo.B).count;
     const int nw = nt / 32;
@@ -1049,10 +1093,12 @@ int raster_bwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
                        const int32_t *, const Rec<T> *, const int32_t *, CotSrc<T>, const T *,
                        const T *, const T *, T, T *);
     const bool small = nt <= 256;
-    K fn = ga ? (small ? raster_bwd_kernel<T, true, 256, LIG_RASTER_BWD_MINB>
-                       : raster_bwd_kernel<T, true, 1024, 1>)
-              : (small ? raster_bwd_kernel<T, false, 256, LIG_RASTER_BWD_MINB>
-                       : raster_bwd_kernel<T, false, 1024, 1>);
+    K fn = ga ? (small ? raster_bwd_kernel<T, true, false, 256, LIG_RASTER_BWD_MINB>
+                       : raster_bwd_kernel<T, true, false, 1024, 1>)
+              : lean ? (small ? raster_bwd_kernel<T, false, true, 256, LIG_RASTER_BWD_MINB>
+                              : raster_bwd_kernel<T, false, true, 1024, 1>)
+                     : (small ? raster_bwd_kernel<T, false, false, 256, LIG_RASTER_BWD_MINB>
+                              : raster_bwd_kernel<T, false, false, 1024, 1>);
     if (!set_dyn_smem((const void *)fn, sm)) return LIG_ERR_LAUNCH;
     int grid = geo.total_tiles();
     if (walk.work) {
@@ -1066,7 +1112,8 @@ int raster_bwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
                             ga ? (const T *)v_dy : nullptr, ga ? (const T *)v_dxy : nullptr, cl,
                             packed);
     Grads<T> g{(T *)v_xy, (T *)v_abs, (T *)v_con, (T *)v_rgb, (T *)v_op};
-    if (n > 0) unpack_grads_kernel<T><<<(n + 255) / 256, 256, 0, s>>>(n, packed, g);
+    if (n > 0 && lean) unpack_lean_grads_kernel<T><<<(n + 255) / 256, 256, 0, s>>>(n, packed, g);
+    else if (n > 0) unpack_grads_kernel<T><<<(n + 255) / 256, 256, 0, s>>>(n, packed, g);
     note_launches(n > 0 ? 2 : 1);
     LIG_LAUNCH_CHECK();
     return LIG_OK;

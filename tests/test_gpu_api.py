@@ -215,3 +215,11 @@ def test_fused_l2_forward_diff_and_loss():
                              colors, None, fin2, diff, one)
     for x, y in zip(ga[:4], gb[:4]):
         assert rel_err(np_(x), np_(y)) <= 1e-5
+    # without opacities these fused backwards skip |v_xy| and the opacity
+    # gradient; the rest equals the general backward fed the same cotangent
+    assert torch.all(gb[1] == 0)
+    v_img = diff * (2.0 / (3 * H * W))
+    full = ops.raster_bwd(H, W, B, b.gaussian_ids_sorted, b.tile_bins, b.total, xys, con, colors,
+                          None, fin, v_img, None, None, None, None)
+    for i in (0, 2, 3):
+        assert rel_err(np_(gb[i]), np_(full[i])) <= 1e-5
