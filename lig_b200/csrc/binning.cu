@@ -14,6 +14,7 @@
 // order inside a tile is emission order (ascending Gaussian id), which is the
 // order of the reference's stable torch.sort.
 #include <atomic>
+#include <mutex>
 
 #include "common.cuh"
 
@@ -488,15 +489,21 @@ int run_bin(const BatchGeo &geo, const void *xys, const void *ext, const int32_t
 
     size_t dsm = downsweep_smem(p.bins);
     if (dsm > 48 * 1024) {
-        // set once per device (and never during stream capture)
-        static std::atomic<uint64_t> opted{0};
+        // opt in once per (device, size): the digit count — and with it the
+        // shared memory — depends on the tile count, so a later call may need
+        // more than an earlier one; never during a stream capture after the
+        // first eager call of that size
+        static std::mutex mu;
+        static size_t opted[128] = {};
         int dev = 0;
-        cudaGetDevice(&dev);
-        const uint64_t bit = 1ull << (dev & 63);
-        if (!(opted.load() & bit)) {
-            cudaFuncSetAttribute(radix_downsweep_kernel,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
-            opted.fetch_or(bit);
+        if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return LIG_ERR_LAUNCH;
+        std::lock_guard<std::mutex> lock(mu);
+        if (opted[dev] < dsm) {
+            if (cudaFuncSetAttribute(radix_downsweep_kernel,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)dsm) != cudaSuccess)
+                return LIG_ERR_LAUNCH;
+            opted[dev] = dsm;
         }
     }
     int hist_n = p.bins * p.nblk;

@@ -479,6 +479,9 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
 #ifndef LIG_RASTER_FWD_MINB
 #define LIG_RASTER_FWD_MINB 4
 #endif
+#ifndef LIG_RASTER_BWD_SPLIT
+#define LIG_RASTER_BWD_SPLIT 0  // split a short list's Gaussians across lanes
+#endif
 #ifndef LIG_RASTER_BWD_LANE_ELLIPSE
 #define LIG_RASTER_BWD_LANE_ELLIPSE 1  // ellipse culling by the warp's lanes (measured faster)
 #endif
@@ -763,7 +766,15 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
         }
         __syncwarp();
         for (int g0 = 0; g0 < nmine; g0 += 32) {
-            const int slot = g0 + lane < nmine ? (int)my_list[g0 + lane] : -1;
+            // lanes per Gaussian: with fewer than 17 / 9 / 5 Gaussians left,
+            // 2 / 4 / 8 lanes share one Gaussian, each taking a contiguous
+            // share of the region's 32 pixels (their sums are combined below)
+            const int left = min(32, nmine - g0);
+            const int lsplit = !LIG_RASTER_BWD_SPLIT ? 0 : left <= 4 ? 3 : left <= 8 ? 2
+                                                             : left <= 16 ? 1 : 0;
+            const int gi = lane >> lsplit, part = lane & ((1 << lsplit) - 1);
+            const int j0 = part << (5 - lsplit), j1 = j0 + (32 >> lsplit);
+            const int slot = gi < left ? (int)my_list[g0 + gi] : -1;
             const bool act = slot >= 0;
             const Rec<T> g = s_rec[act ? slot : 0];
             const int k = act ? base + slot : 0x7fffffff;
@@ -771,7 +782,7 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
 #pragma unroll
             for (int q = 0; q < 11; ++q) acc[q] = 0;
             bool touched = false;
-            for (int j = 0; j < 32; ++j) {
+            for (int j = j0; j < j1; ++j) {
                 const PixRec<T, GA> &c = my_pix[j];
                 if (k > c.fin) continue;
                 if constexpr (!GA) {
@@ -849,7 +860,15 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
                     acc[10] += vis * va;
                 }
             }
-            if (touched) {
+            for (int o = 1; o < (1 << lsplit); o <<= 1) {  // combine the lane group
+#pragma unroll
+                for (int q = 0; q < 11; ++q) {
+                    if (LEAN && (q == 2 || q == 3 || q == 10)) continue;
+                    acc[q] += __shfl_xor_sync(FULL, acc[q], o);
+                }
+                touched = __shfl_xor_sync(FULL, (int)touched, o) || touched;
+            }
+            if (touched && part == 0) {
                 if (GA) {  // |sum over the reference warp| (= this region)
                     acc[2] = M::abs_(acc[0]);
                     acc[3] = M::abs_(acc[1]);

@@ -43,6 +43,7 @@ def main():
     ap.add_argument("--sets", type=int, default=64)
     ap.add_argument("--fit-chunk", type=int, default=20)
     ap.add_argument("--no-fit-graph", action="store_true")
+    ap.add_argument("--dump", default="", help="write per-request timings (CSV) here")
     a = ap.parse_args()
     t0 = time.time()
     sets = resident_sets(a.sets)
@@ -81,6 +82,14 @@ def main():
         "fit_batches": srv.fit_batches, "budget_peak_gb": srv.budget.peak / 1e9,
         "errors": srv.errors[:5],
     }
+    if a.dump:
+        with open(a.dump, "w") as f:
+            f.write("id,kind,t_submit,t_start,t_enqueued,t_done,error\n")
+            for rid, r in sorted(srv.results.items()):
+                f.write(f"{rid},{r.kind},{r.t_submit:.6f},{r.t_start:.6f},{r.t_enqueued:.6f},"
+                        f"{r.t_done:.6f},{1 if r.error else 0}\n")
+            for a0, b0, ph in srv.fit_phases:
+                f.write(f"-1,phase:{ph},{a0:.6f},{b0:.6f},0,0,0\n")
     print(json.dumps(out), flush=True)
 
 

@@ -223,3 +223,28 @@ def test_fused_l2_forward_diff_and_loss():
                           None, fin, v_img, None, None, None, None)
     for i in (0, 2, 3):
         assert rel_err(np_(gb[i]), np_(full[i])) <= 1e-5
+
+
+def test_binning_grows_sort_shared_memory_between_calls():
+    """A process whose first binning needs 9-bit radix digits and whose next
+    one needs 10-bit digits (more shared memory in the downsweep) must opt
+    the kernel into the larger size (fresh process: the opt-in is cached)."""
+    import subprocess
+    import sys
+    code = r"""
+import torch
+from lig_b200 import ops
+from tests._scene import scene
+for (H, W, B) in ((4096, 8192, 16), (8192, 8192, 8)):
+    means, L, colors, _ = scene(2000, H, W, diag=(0.5, 3.0), seed=3)
+    xys, ext, con, cnt = ops.project_fwd(L, means, None, H, W, B, True)
+    b = ops.bin_gaussians(xys, ext, cnt, H, W, B)
+    torch.cuda.synchronize()
+    assert b.num_intersects == int(cnt.sum())
+print("ok")
+"""
+    import os
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0 and "ok" in r.stdout, r.stderr[-2000:]
