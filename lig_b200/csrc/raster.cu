@@ -480,7 +480,7 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
 #define LIG_RASTER_FWD_MINB 4
 #endif
 #ifndef LIG_RASTER_BWD_SPLIT
-#define LIG_RASTER_BWD_SPLIT 0  // split a short list's Gaussians across lanes
+#define LIG_RASTER_BWD_SPLIT 1  // split a short list's Gaussians across lanes (measured faster)
 #endif
 #ifndef LIG_RASTER_BWD_LANE_ELLIPSE
 #define LIG_RASTER_BWD_LANE_ELLIPSE 1  // ellipse culling by the warp's lanes (measured faster)
