@@ -181,7 +181,8 @@ class Server:
     fit (<= 64); fit_chunk: iterations between batch changes."""
 
     def __init__(self, budget_bytes: int = 150 * 10**9, device="cuda", block: int = 16,
-                 max_fit_batch: int = 64, fit_chunk: int = 20, fit_graph: bool = True):
+                 max_fit_batch: int = 64, fit_chunk: int = 20, fit_graph: bool = True,
+                 reserve_fit_bytes: int = 0, reserve_render_bytes: int = 0):
         dev = torch.device(device)
         if dev.type == "cuda" and dev.index is None:
             dev = torch.device("cuda", torch.cuda.current_device())
@@ -205,6 +206,10 @@ class Server:
         self._threads: List[threading.Thread] = []
         self.fit_batches = 0
         self.errors: List[str] = []
+        # device memory taken into the allocator's cache per stream at start,
+        # so the workers' allocations come from the cache: a large cudaMalloc
+        # in the fit thread holds up the render thread's launches meanwhile
+        self.reserve = {"fit": int(reserve_fit_bytes), "render": int(reserve_render_bytes)}
         self.fit_phases: List[tuple] = []  # (t0, t1, phase) of the fit thread
 
     # ----------------------------------------------------------- resources
@@ -224,6 +229,12 @@ class Server:
         return rid
 
     def start(self):
+        for kind, stream in (("fit", self.fit_stream), ("render", self.render_stream)):
+            if self.reserve[kind] > 0:
+                with torch.cuda.stream(stream):
+                    block = torch.empty(self.reserve[kind], dtype=torch.uint8, device=self.dev)
+                    del block  # stays cached for this stream
+        torch.cuda.synchronize(self.dev)
         # the render thread needs the GIL back within a fraction of a
         # millisecond while the fit thread runs Python between launches
         self._switch = sys.getswitchinterval()
@@ -339,10 +350,10 @@ class Server:
             if j.target is None:
                 t = j.req.target() if callable(j.req.target) else j.req.target
                 j.target = t.to(self.dev, torch.float32).contiguous()
-            if j.state is None:
+            if j.state is None:  # initial Gaussians drawn on the device
                 h, w = j.target.shape[:2]
-                mu, ch, co = synthetic.gaussians(j.req.n_points, h, w, seed=j.req.seed)
-                j.state = FitState((mu.to(self.dev), ch.to(self.dev), co.to(self.dev)))
+                j.state = FitState(synthetic.gaussians_on_device(j.req.n_points, h, w, self.dev,
+                                                                 seed=j.req.seed))
             init.append(j.state)
         fit = BatchedFit([j.target for j in jobs], [j.req.n_points for j in jobs],
                          block=self.block, lr=jobs[0].req.lr, init=init, graph=self.fit_graph)

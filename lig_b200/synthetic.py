@@ -29,6 +29,23 @@ def gaussians(n: int, H: int, W: int, diag=(0.5, 4.0), offdiag_std: float = 0.5,
     return means.to(dtype), chol.to(dtype), colors.to(dtype)
 
 
+def gaussians_on_device(n: int, H: int, W: int, device, diag=(0.5, 4.0),
+                        offdiag_std: float = 0.5, seed: int = SEED_TEACHER):
+    """The distribution of gaussians() drawn on the device with a device
+    generator (a different random stream from the CPU one): no host work or
+    host-to-device copies, for fit requests arriving at a running server."""
+    g = torch.Generator(device=device).manual_seed(seed)
+    kw = dict(generator=g, device=device, dtype=torch.float32)
+    means = torch.rand(n, 2, **kw) * torch.tensor([float(W), float(H)], device=device)
+    lo, hi = diag
+    l11 = lo + (hi - lo) * torch.rand(n, **kw)
+    l22 = lo + (hi - lo) * torch.rand(n, **kw)
+    l21 = offdiag_std * torch.randn(n, **kw)
+    chol = torch.stack([l11, l21, l22], 1)
+    colors = torch.rand(n, 3, **kw)
+    return means, chol, colors
+
+
 def white_noise(H: int, W: int, std: float, seed: int = SEED_NOISE) -> torch.Tensor:
     g = torch.Generator().manual_seed(seed)
     return std * torch.randn(H, W, 3, generator=g)

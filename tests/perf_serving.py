@@ -43,6 +43,8 @@ def main():
     ap.add_argument("--sets", type=int, default=64)
     ap.add_argument("--fit-chunk", type=int, default=20)
     ap.add_argument("--no-fit-graph", action="store_true")
+    ap.add_argument("--reserve-fit-gb", type=float, default=60.0)
+    ap.add_argument("--reserve-render-gb", type=float, default=8.0)
     ap.add_argument("--dump", default="", help="write per-request timings (CSV) here")
     a = ap.parse_args()
     t0 = time.time()
@@ -52,7 +54,8 @@ def main():
     schedule = poisson_requests(a.duration, a.rate, a.fit_frac, sets, fit_iters=a.fit_iters,
                                 seed=5000)
     srv = Server(budget_bytes=int(a.budget_gb * 1e9), fit_chunk=a.fit_chunk,
-                 fit_graph=not a.no_fit_graph)
+                 fit_graph=not a.no_fit_graph, reserve_fit_bytes=int(a.reserve_fit_gb * 1e9),
+                 reserve_render_bytes=int(a.reserve_render_gb * 1e9))
     for k, gs in sets.items():
         srv.add_set(k, gs)
     # warm the render path (library load, allocator) before the clock starts
