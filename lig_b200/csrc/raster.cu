@@ -90,8 +90,9 @@ __global__ void pack_kernel(int n, const T *__restrict__ xys, const T *__restric
 // ---------------------------------------------------------------- regions
 // A tile is split into R <= 32 regions of 32 pixels; warp w of the CTA owns
 // region w and each lane owns PPL pixels of it.
-//   kind 0: 8x4 blocks, PPL 1                          (forward)
-//   kind 1: 8x8 blocks, lane owns (x, y) and (x, y+4)  (sum backward)
+//   kind 0: 8x4 blocks, PPL 1               (backward; gradient-aware forward)
+//   kind 1: 8x8 blocks, lane owns (x, y + 4p), p < 2    (sum forward)
+//   kind 3: 8x16 blocks, lane owns (x, y + 4p), p < 4   (sum forward option)
 //   kind 2: the reference's warps, thread ranks 32w..32w+31 with
 //           rank = ty*B + tx, PPL 1                    (gradient-aware backward)
 struct Regions {
@@ -100,6 +101,7 @@ struct Regions {
         Regions r{kind, B, 1, 1, 1};
         if (kind == 0) { r.nbx = (B + 7) / 8; r.nby = (B + 3) / 4; }
         else if (kind == 1) { r.nbx = (B + 7) / 8; r.nby = (B + 7) / 8; }
+        else if (kind == 3) { r.nbx = (B + 7) / 8; r.nby = (B + 15) / 16; }
         else { r.nbx = 1; r.nby = (B * B + 31) / 32; }
         r.count = r.nbx * r.nby;
         return r;
@@ -108,14 +110,18 @@ struct Regions {
         if (kind == 0) {
             lx = (w % nbx) * 8 + (lane & 7);
             ly = (w / nbx) * 4 + (lane >> 3);
-        } else if (kind == 1) {
+        } else if (kind == 1 || kind == 3) {
             lx = (w % nbx) * 8 + (lane & 7);
-            ly = (w / nbx) * 8 + (lane >> 3) + 4 * p;
+            ly = (w / nbx) * block_h() + (lane >> 3) + 4 * p;
         } else {
             int r = w * 32 + lane;
             lx = r % B;
             ly = r < B * B ? r / B : B;  // B marks "no pixel"
         }
+    }
+    // rows of a block region (kinds 0, 1, 3)
+    __host__ __device__ __forceinline__ int block_h() const {
+        return kind == 0 ? 4 : (kind == 1 ? 8 : 16);
     }
     // tile-local pixel-centre rectangle of region w (conservative)
     template <typename T>
@@ -127,7 +133,7 @@ struct Regions {
             if (iy0 == iy1) { ix0 = r0 % B; ix1 = r1 % B; }
             else { ix0 = 0; ix1 = B - 1; }
         } else {
-            const int hb = kind == 0 ? 4 : 8;
+            const int hb = block_h();
             ix0 = (w % nbx) * 8; ix1 = min(ix0 + 7, B - 1);
             iy0 = (w / nbx) * hb; iy1 = min(iy0 + hb - 1, B - 1);
         }
@@ -153,7 +159,7 @@ struct Regions {
             }
             return m;
         }
-        const int hb = kind == 0 ? 4 : 8;
+        const int hb = block_h();
         T c0 = Math<T>::ceil_((x0 - (T)7.5) / (T)8), c1 = Math<T>::floor_((x1 - (T)0.5) / (T)8);
         T r0 = Math<T>::ceil_((y0 - ((T)hb - (T)0.5)) / (T)hb);
         T r1 = Math<T>::floor_((y1 - (T)0.5) / (T)hb);
@@ -392,7 +398,7 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
     const unsigned FULL = 0xffffffffu;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int B = tc.B, tx0 = tc.tx0, ty0 = tc.ty0;
-    const Regions R = Regions::make(PPL == 2 ? 1 : 0, B);
+    const Regions R = Regions::make(PPL == 1 ? 0 : (PPL == 2 ? 1 : 3), B);
     bool inside[PPL];
     int pix[PPL];
     T px[PPL], py[PPL];
@@ -450,13 +456,15 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
                         const int b1 = __ffs(mask) - 1;
                         mask &= mask - 1;
                         const Rec<T> g1 = s_rec[m * 32 + b1];
-                        T dxa, dya, aa, dxb, dyb, ab;
-                        const bool oka =
-                            PixelEval<T>::template alpha<GA>(g1, px[0], py[0], dxa, dya, aa);
-                        const bool okb =
-                            PixelEval<T>::template alpha<GA>(g1, px[1], py[1], dxb, dyb, ab);
-                        if (oka) acc[0].add(g1, dxa, dya, aa, base + m * 32 + b1);
-                        if (okb) acc[1].add(g1, dxb, dyb, ab, base + m * 32 + b1);
+                        T dxp[PPL], dyp[PPL], ap[PPL];
+                        bool okp[PPL];
+#pragma unroll
+                        for (int p = 0; p < PPL; ++p)
+                            okp[p] = PixelEval<T>::template alpha<GA>(g1, px[p], py[p], dxp[p],
+                                                                      dyp[p], ap[p]);
+#pragma unroll
+                        for (int p = 0; p < PPL; ++p)
+                            if (okp[p]) acc[p].add(g1, dxp[p], dyp[p], ap[p], base + m * 32 + b1);
                     }
                 }
             }
@@ -489,11 +497,14 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
 #define LIG_RASTER_BWD_MINB 5
 #endif
 
-// Sum forward: two pixels per lane from LIG_RASTER_PPL2_MIN_TILES tiles on
-// (fewer warps per tile; small images keep one pixel per lane so the grid
-// still fills the GPU).
+// Sum forward: LIG_RASTER_FWD_PPL (2 or 4) pixels per lane from
+// LIG_RASTER_PPL2_MIN_TILES tiles on (fewer warps per tile; below it one
+// pixel per lane keeps more warps per tile).
 #ifndef LIG_RASTER_PPL2_MIN_TILES
 #define LIG_RASTER_PPL2_MIN_TILES 0
+#endif
+#ifndef LIG_RASTER_FWD_PPL
+#define LIG_RASTER_FWD_PPL 2
 #endif
 
 template <typename T, bool GA, int PPL, int MAXT, int MINB>
@@ -767,13 +778,15 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
         __syncwarp();
         for (int g0 = 0; g0 < nmine; g0 += 32) {
             // lanes per Gaussian: with fewer than 17 / 9 / 5 Gaussians left,
-            // 2 / 4 / 8 lanes share one Gaussian, each taking a contiguous
-            // share of the region's 32 pixels (their sums are combined below)
+            // 2 / 4 / 8 lanes share one Gaussian, lane part p taking pixels
+            // p, p + 2^lsplit, ... of the region (interleaved, so the group's
+            // pixel records sit in different shared-memory banks); their
+            // sums are combined below
             const int left = min(32, nmine - g0);
             const int lsplit = !LIG_RASTER_BWD_SPLIT ? 0 : left <= 4 ? 3 : left <= 8 ? 2
                                                              : left <= 16 ? 1 : 0;
             const int gi = lane >> lsplit, part = lane & ((1 << lsplit) - 1);
-            const int j0 = part << (5 - lsplit), j1 = j0 + (32 >> lsplit);
+            const int jstep = 1 << lsplit;
             const int slot = gi < left ? (int)my_list[g0 + gi] : -1;
             const bool act = slot >= 0;
             const Rec<T> g = s_rec[act ? slot : 0];
@@ -782,7 +795,7 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
 #pragma unroll
             for (int q = 0; q < 11; ++q) acc[q] = 0;
             bool touched = false;
-            for (int j = j0; j < j1; ++j) {
+            for (int j = part; j < 32; j += jstep) {
                 const PixRec<T, GA> &c = my_pix[j];
                 if (k > c.fin) continue;
                 if constexpr (!GA) {
@@ -1040,7 +1053,8 @@ int raster_fwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
     if (rc) return rc;
     const bool ga = dx != nullptr;
     const bool ppl2 = !ga && geo.total_tiles() >= LIG_RASTER_PPL2_MIN_TILES;
-    const int nt = 32 * Regions::make(ppl2 ? 1 : 0, geo.B).count;
+    constexpr int PM = LIG_RASTER_FWD_PPL;  // pixels per lane of the multi-pixel forward
+    const int nt = 32 * Regions::make(ppl2 ? (PM == 2 ? 1 : 3) : 0, geo.B).count;
     const size_t sm = (size_t)nt * (sizeof(Rec<T>) + sizeof(uint32_t));
     using K = void (*)(const BatchGeo, const int32_t *, int *, const int32_t *, const int2 *,
                        const int32_t *, const Rec<T> *, T *, T *, T *, T *, T *, int32_t *,
@@ -1048,8 +1062,8 @@ int raster_fwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
     const bool small = nt <= 256;
     K fn = ga ? (small ? raster_fwd_kernel<T, true, 1, 256, LIG_RASTER_FWD_MINB>
                        : raster_fwd_kernel<T, true, 1, 1024, 1>)
-              : ppl2 ? (small ? raster_fwd_kernel<T, false, 2, 256, LIG_RASTER_FWD_MINB>
-                              : raster_fwd_kernel<T, false, 2, 1024, 1>)
+              : ppl2 ? (small ? raster_fwd_kernel<T, false, PM, 256, LIG_RASTER_FWD_MINB>
+                              : raster_fwd_kernel<T, false, PM, 1024, 1>)
                      : (small ? raster_fwd_kernel<T, false, 1, 256, LIG_RASTER_FWD_MINB>
                               : raster_fwd_kernel<T, false, 1, 1024, 1>);
     if (!set_dyn_smem((const void *)fn, sm)) return LIG_ERR_LAUNCH;
