@@ -486,6 +486,21 @@ def poisson_requests(duration_s: float, rate: float, fit_frac: float, sets: Dict
                                       "origin": (ox, oy)}))
 
 
+def warm_up(server: Server, sides=(256, 1024, 2048, 4096), scales=(0.25, 1.0, 2.0)):
+    """Render a few views of each resident set's kind at several output sizes
+    and scales on the render stream, so the first requests do not pay for
+    first-use costs (kernel loading, tile-count-dependent sort set-up,
+    allocator growth)."""
+    gs = next(iter(server.sets.values()), None)
+    if gs is None:
+        return
+    with torch.cuda.stream(server.render_stream):
+        for side in sides:
+            for s in scales:
+                render_view(gs, side, side, (0.0, 0.0), (s, s), server.block)
+    torch.cuda.synchronize(server.dev)
+
+
 def run_workload(server: Server, schedule, master_target: torch.Tensor, drain_s: float = 60.0,
                  fit_lr: float = 1e-3) -> WorkloadStats:
     """Submit `schedule` (from poisson_requests) at its arrival times, wait up
@@ -494,8 +509,9 @@ def run_workload(server: Server, schedule, master_target: torch.Tensor, drain_s:
     when the fit is admitted."""
     st = WorkloadStats()
     kinds = {}
+    if not server._threads:
+        server.start()  # before the clock: start-up reserves device memory
     t0 = time.perf_counter()
-    server.start()
     for t, kind, p in schedule:
         delay = t0 + t - time.perf_counter()
         if delay > 0:
