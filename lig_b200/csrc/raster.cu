@@ -837,14 +837,24 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
                         acc[10] += vis * v_alpha;
                     }
                     const T v_sigma = -alpha * v_alpha;
-                    acc[4] += (T)0.5 * v_sigma * dx * dx;
-                    acc[5] += v_sigma * dx * dy;
-                    acc[6] += (T)0.5 * v_sigma * dy * dy;
-                    const T gx = v_sigma * (g.a * dx + g.b * dy);
-                    const T gy = v_sigma * (g.b * dx + g.c * dy);
-                    acc[0] += gx;
-                    acc[1] += gy;
-                    if constexpr (!LEAN) {
+                    if constexpr (LEAN) {
+                        // the gradients are linear in five per-pixel sums
+                        // (Sx, Sy, Sxx, Sxy, Syy of v_sigma dx^i dy^j); the
+                        // conic is applied once per Gaussian after the loop
+                        const T tx = v_sigma * dx, ty = v_sigma * dy;
+                        acc[0] += tx;
+                        acc[1] += ty;
+                        acc[4] += tx * dx;
+                        acc[5] += tx * dy;
+                        acc[6] += ty * dy;
+                    } else {
+                        acc[4] += (T)0.5 * v_sigma * dx * dx;
+                        acc[5] += v_sigma * dx * dy;
+                        acc[6] += (T)0.5 * v_sigma * dy * dy;
+                        const T gx = v_sigma * (g.a * dx + g.b * dy);
+                        const T gy = v_sigma * (g.b * dx + g.c * dy);
+                        acc[0] += gx;
+                        acc[1] += gy;
                         acc[2] += M::abs_(gx);
                         acc[3] += M::abs_(gy);
                     }
@@ -900,6 +910,14 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
                 touched = __shfl_xor_sync(FULL, (int)touched, o) || touched;
             }
             if (touched && part == 0) {
+                if constexpr (LEAN && !GA) {
+                    // v_xy = (a Sx + b Sy, b Sx + c Sy); v_conic = (Sxx/2, Sxy, Syy/2)
+                    const T sx = acc[0], sy = acc[1];
+                    acc[0] = g.a * sx + g.b * sy;
+                    acc[1] = g.b * sx + g.c * sy;
+                    acc[4] *= (T)0.5;
+                    acc[6] *= (T)0.5;
+                }
                 if (GA) {  // |sum over the reference warp| (= this region)
                     acc[2] = M::abs_(acc[0]);
                     acc[3] = M::abs_(acc[1]);
