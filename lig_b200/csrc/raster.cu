@@ -1,29 +1,34 @@
 // Weighted-sum rasterizer, forward and backward, plain and gradient-aware.
 //
-// Work decomposition (B200): one CTA per tile; the tile is split into <= 32
-// regions of 32 pixels and warp w owns region w (8x4 pixels in the forward,
-// 8x8 with two pixels per lane in the sum backward, the reference's warp in
-// the gradient-aware backward, whose v_xy_abs is |sum over that warp| per
-// Gaussian, csrc/gradient_aware_rasterizer.cu:317-341).
+// Work decomposition (B200): one CTA per tile (or per work item of a
+// batch's flattened (image, tile) list); the tile is split into <= 32
+// regions of 32 lanes and warp w owns region w: 8x8 pixels with two pixels
+// per lane in the sum forward, 8x4 pixels in the gradient-aware forward and
+// the sum backward, the reference's warp in the gradient-aware backward,
+// whose v_xy_abs is |sum over that warp| per Gaussian
+// (csrc/gradient_aware_rasterizer.cu:317-341).
 //
 // Gaussian data: a pack kernel writes one 16-byte-aligned 48-byte record per
-// Gaussian (mean, conic, opacity, colour, cull half-widths).  The tile's
-// sorted id list is consumed in batches of blockDim Gaussians: each thread
-// parks one record in shared memory (fetched into registers while the
-// previous batch was processed) together with that Gaussian's region mask.
+// Gaussian (mean, conic, opacity, colour, cull half-widths, sigma
+// threshold).  The tile's sorted id list is consumed in batches of blockDim
+// Gaussians: each thread parks one record in shared memory (fetched into
+// registers while the previous batch was processed) together with that
+// Gaussian's region mask.
 //
 // Culling: a warp runs only the Gaussians whose mask has its region bit
-// (one ballot per 32 Gaussians, then the set bits in ascending order, i.e.
-// list order).  The mask comes from a conservative box around the
-// Gaussian's alpha >= 1/255 ellipse, built with margin (see pack_kernel), so
-// every skipped pixel would have failed the reference's own `alpha < 1/255`
-// test (csrc/forward.cu:258): results are unchanged.
+// (forward: one ballot per 32 Gaussians, then the set bits in ascending, i.e.
+// list, order; backward: a compacted per-warp list).  The mask comes from a
+// conservative box around the Gaussian's alpha >= 1/255 ellipse, built with
+// margin (see pack_kernel), refined in the backward by an exact
+// ellipse-over-rectangle test, so every skipped pixel would have failed the
+// reference's own `alpha < 1/255` test (csrc/forward.cu:258): results are
+// unchanged.
 //
-// Per-pixel arithmetic is written exactly as the reference writes it
-// (csrc/forward.cu:250-269, csrc/backward.cu:102-150,
-// csrc/gradient_aware_rasterizer.cu:201-315, :434-482) so that the float
-// roundings, and with them the alpha-threshold decisions, are the same, and
-// each pixel adds its terms in list order.
+// Per-pixel arithmetic follows the reference (csrc/forward.cu:250-269,
+// csrc/backward.cu:102-150, csrc/gradient_aware_rasterizer.cu:201-315,
+// :434-482), sigma with explicit roundings in its compiled form (sigma_ref),
+// so that the alpha-threshold decisions are the same, and each pixel adds its
+// terms in list order.
 #include <mutex>
 #include <tuple>
 #include <vector>
