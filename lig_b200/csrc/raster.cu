@@ -625,18 +625,8 @@ l2_chunks_final_kernel(const BatchGeo geo, const TileChunks ch,
 
 // ------------------------------------------------------------- backward
 template <typename T>
-struct Grads {
+struct Grads {  // the ABI's per-Gaussian gradient arrays (v_opac may be null)
     T *v_xy, *v_abs, *v_conic, *v_rgb, *v_opac;
-    // value index k: 0-1 v_xy, 2-3 v_xy_abs, 4-6 v_conic, 7-9 v_rgb, 10 v_opacity
-    __device__ __forceinline__ void add(int k, int g, T val) const {
-        T *p = nullptr;
-        if (k < 2) p = v_xy + 2 * g + k;
-        else if (k < 4) p = v_abs + 2 * g + (k - 2);
-        else if (k < 7) p = v_conic + 3 * g + (k - 4);
-        else if (k < 10) p = v_rgb + 3 * g + (k - 7);
-        else if (k == 10 && v_opac) p = v_opac + g;
-        if (p) atomicAdd(p, val);
-    }
 };
 
 // Backward, transposed: one CTA per tile, warp w owns region w (an 8x4 block in
@@ -644,13 +634,16 @@ struct Grads {
 // v_xy_abs is |sum over that warp| per Gaussian,
 // csrc/gradient_aware_rasterizer.cu:317-341).  The tile's pixel cotangents,
 // pixel centres and final indices are staged in shared memory once, region
-// by region.  Per batch each warp compacts the batch slots whose region mask
-// has its bit; lanes then take one such Gaussian each and loop over the
-// region's 32 pixels (pixel data read by broadcast), so every lane
-// accumulates its own Gaussian's gradient terms in registers — no cross-lane
-// reduction — and adds them to the packed [N][12] gradient buffer with three
-// 16-byte atomics per (Gaussian, region).  Entries past every pixel's final
-// index are skipped.
+// by region.  Per batch each warp compacts the batch slots whose region box it
+// meets (exact ellipse test by the lanes); lanes then take one such Gaussian
+// each — or, for a short list, 2 / 4 / 8 lanes share one and take interleaved
+// pixels — and loop over the region's pixels (pixel data read by broadcast),
+// accumulating the Gaussian's gradient terms in registers; a lane group is
+// combined with shuffles, and the terms go to the packed per-Gaussian buffer
+// with 16-byte atomics per (Gaussian, region) — [N][12], three atomics, in
+// general; [N][8], two, in the lean fused-loss variant.  Entries past every
+// pixel's final index are skipped.
+//
 // Pixel cotangent source of the backward: explicit dL/dimg (+ optional
 // dL/dwsum), or — fused L2 — computed on the fly from the render and the target
 // as the gradient of mean((clamp(img, 0, 1) - target)^2): the value torch's
