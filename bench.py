@@ -4,18 +4,20 @@ Workload (one "step"): one fit iteration of LIG's full-resolution level —
 2M Cholesky Gaussians (means U[0,8192)^2, diagonals U[0.5,6], off-diagonal
 N(0,0.5), colours U(0,1)) on an 8192x8192 RGB fp32 target (a render of 2M
 seeded teacher Gaussians plus 1/f^2 noise of std 0.03, clipped): project ->
-bin -> raster forward -> clamp -> L2 -> raster backward -> projection
-backward -> Adam, through the drop-in gsplat2d API.  Synthetic data stands
+bin -> raster forward with the clamped L2 loss fused in -> raster backward
+-> projection backward -> Adam, as lig_b200.fit.LevelFit.step runs it (its
+CUDA-graph engine: one graph replay per iteration).  Synthetic data stands
 in for the DIV2K/STimage images (not available offline).
 
   value  device-timed iterations/s, target resident in HBM (inputs > L2).
-  e2e    same loop through the public API with the step's input (the target
+  e2e    same loop through LevelFit.step with the step's input (the target
          image) copied host->device from pinned memory every step (double
          buffered on a copy stream, overlapping the previous step) and the
          loss copied back to pinned host memory every step.
   roofline  the dominant kernel's algorithmic rate (reference-defined
          Gaussian-pixel evaluations x FLOP per evaluation) / measured FP32
-         FMA peak of this device.
+         FMA peak of this device; per-kernel times come from three eager
+         runs of the graph's kernels just before the timed loop.
   cpu_baseline  the C restatement of the reference algorithm (oracle/) on
          this host's cores, on a horizontal band of the same workload.
 
