@@ -4,9 +4,11 @@ two-level pipeline of train.py:93-158.
 A level fits Cholesky-parameterised Gaussians (means, [l11, l21, l22], rgb) to
 an HWC target with L2 on the clamped render and Adam, the loop of
 gaussianlig.Gaussian2D.train_iter (gaussianlig.py:99-111) with the
-parameterisation of the fit configurations.  All rendering goes through the
-drop-in gsplat2d API (project_gaussians_cholesky + rasterize_gaussians
-[+ gradient_aware_upscale]); nothing here reimplements the kernels.
+parameterisation of the fit configurations.  The iteration runs either as a
+captured CUDA graph of the library's fused entry points (LevelFit's default
+engine, through lig_b200.batch) or through the drop-in gsplat2d API under
+autograd; renders between levels use the drop-in API
+(project_gaussians_cholesky + rasterize_gaussians + gradient_aware_upscale).
 """
 from __future__ import annotations
 
