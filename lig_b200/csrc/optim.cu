@@ -167,7 +167,17 @@ extern "C" int lig_adam_step_batch(int n_img, const int32_t *counts, float *para
     adam_batch_prologue_kernel<<<1, kMaxBatch, 0, s>>>(ab, status, steps, skipped, lr, beta1,
                                                        beta2, sc);
     int launches = 1;
-    if (tot > 0) {
+    if (tot > 0 && n_img == 1 && !((uintptr_t)params & 15) && !((uintptr_t)grads & 15) &&
+        !((uintptr_t)exp_avg & 15) && !((uintptr_t)exp_avg_sq & 15)) {
+        // one image: the float4 kernel with the image's scalars
+        int64_t blocks = (2 * tot + 255) / 256;
+        const int64_t cap = 148 * 16;
+        if (blocks > cap) blocks = cap;
+        adam_kernel<<<(int)blocks, 256, 0, s>>>(8 * tot, params, grads, exp_avg, exp_avg_sq,
+                                               (float)(1.0 - beta1), (float)beta2,
+                                               (float)(1.0 - beta2), (float)eps, sc);
+        ++launches;
+    } else if (tot > 0) {
         int64_t blocks = (8 * tot + 255) / 256;
         const int64_t cap = 148 * 16;
         if (blocks > cap) blocks = cap;
