@@ -513,6 +513,9 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
 #ifndef LIG_RASTER_FWD_MINB
 #define LIG_RASTER_FWD_MINB 4
 #endif
+#ifndef LIG_RASTER_BWD_PAIR
+#define LIG_RASTER_BWD_PAIR 0  // lean backward: two pixels per loop iteration
+#endif
 #ifndef LIG_RASTER_BWD_SPLIT
 #define LIG_RASTER_BWD_SPLIT 1  // split a short list's Gaussians across lanes (measured faster)
 #endif
@@ -811,6 +814,41 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
 #pragma unroll
             for (int q = 0; q < 11; ++q) acc[q] = 0;
             bool touched = false;
+            if constexpr (LEAN && !GA && LIG_RASTER_BWD_PAIR) {
+                // two of the lane's pixels per iteration: their sigma / alpha
+                // chains overlap; accumulation stays in pixel order
+                auto body = [&](const PixRec<T, GA> &c, T alpha, T dx, T dy) {
+                    touched = true;
+                    acc[7] += alpha * c.vo0;
+                    acc[8] += alpha * c.vo1;
+                    acc[9] += alpha * c.vo2;
+                    T v_alpha = 0;
+                    v_alpha += g.r * c.vo0;
+                    v_alpha += g.g * c.vo1;
+                    v_alpha += g.bl * c.vo2;
+                    const T v_sigma = -alpha * v_alpha;
+                    const T tx = v_sigma * dx, ty = v_sigma * dy;
+                    acc[0] += tx;
+                    acc[1] += ty;
+                    acc[4] += tx * dx;
+                    acc[5] += tx * dy;
+                    acc[6] += ty * dy;
+                };
+                for (int j = part; j < 32; j += 2 * jstep) {
+                    const PixRec<T, GA> &c0 = my_pix[j];
+                    const PixRec<T, GA> &c1 = my_pix[j + jstep];
+                    const T dx0 = g.x - c0.px, dy0 = g.y - c0.py;
+                    const T dx1 = g.x - c1.px, dy1 = g.y - c1.py;
+                    const T s0 = sigma_ref<T>(g.a, g.b, g.c, dx0, dy0);
+                    const T s1 = sigma_ref<T>(g.a, g.b, g.c, dx1, dy1);
+                    const T a0 = M::min_(clamp, g.o * M::exp_(-s0));
+                    const T a1 = M::min_(clamp, g.o * M::exp_(-s1));
+                    const bool ok0 = k <= c0.fin && !(s0 < (T)0 || a0 < (T)1 / (T)255);
+                    const bool ok1 = k <= c1.fin && !(s1 < (T)0 || a1 < (T)1 / (T)255);
+                    if (ok0) body(c0, a0, dx0, dy0);
+                    if (ok1) body(c1, a1, dx1, dy1);
+                }
+            } else
             for (int j = part; j < 32; j += jstep) {
                 const PixRec<T, GA> &c = my_pix[j];
                 if (k > c.fin) continue;
