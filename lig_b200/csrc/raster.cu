@@ -35,10 +35,6 @@
 
 #include "common.cuh"
 
-#ifndef LIG_RASTER_FWD_PAIR
-#define LIG_RASTER_FWD_PAIR 0  // sum forward: two Gaussians per loop iteration
-#endif
-
 namespace lig {
 
 template <typename T> struct alignas(16) Rec {
@@ -493,23 +489,6 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
                             PixelEval<T>::template alpha<GA>(g1, px[0], py[0], dxa, dya, aa);
                         const bool okb =
                             PixelEval<T>::template alpha<GA>(g1, px[1], py[1], dxb, dyb, ab);
-                        if (LIG_RASTER_FWD_PAIR && mask) {
-                            // a second Gaussian: four alpha chains overlap;
-                            // each pixel still adds g1 before g2 (list order)
-                            const int b2 = __ffs(mask) - 1;
-                            mask &= mask - 1;
-                            const Rec<T> g2 = s_rec[m * 32 + b2];
-                            T dxc, dyc, ac, dxd, dyd, ad;
-                            const bool okc =
-                                PixelEval<T>::template alpha<GA>(g2, px[0], py[0], dxc, dyc, ac);
-                            const bool okd =
-                                PixelEval<T>::template alpha<GA>(g2, px[1], py[1], dxd, dyd, ad);
-                            if (oka) acc[0].add(g1, dxa, dya, aa, base + m * 32 + b1);
-                            if (okb) acc[1].add(g1, dxb, dyb, ab, base + m * 32 + b1);
-                            if (okc) acc[0].add(g2, dxc, dyc, ac, base + m * 32 + b2);
-                            if (okd) acc[1].add(g2, dxd, dyd, ad, base + m * 32 + b2);
-                            continue;
-                        }
                         if (oka) acc[0].add(g1, dxa, dya, aa, base + m * 32 + b1);
                         if (okb) acc[1].add(g1, dxb, dyb, ab, base + m * 32 + b1);
                     }
