@@ -97,6 +97,7 @@ __global__ void pack_kernel(int n, const T *__restrict__ xys, const T *__restric
 // region w and each lane owns PPL pixels of it.
 //   kind 0: 8x4 blocks, PPL 1               (backward; gradient-aware forward)
 //   kind 1: 8x8 blocks, lane owns (x, y) and (x, y + 4)  (sum forward)
+//   kind 3: 8x16 blocks, lane owns (x, y + 4p), p < 4   (sum forward, large images)
 //   kind 2: the reference's warps, thread ranks 32w..32w+31 with
 //           rank = ty*B + tx, PPL 1                    (gradient-aware backward)
 struct Regions {
@@ -105,6 +106,7 @@ struct Regions {
         Regions r{kind, B, 1, 1, 1};
         if (kind == 0) { r.nbx = (B + 7) / 8; r.nby = (B + 3) / 4; }
         else if (kind == 1) { r.nbx = (B + 7) / 8; r.nby = (B + 7) / 8; }
+        else if (kind == 3) { r.nbx = (B + 7) / 8; r.nby = (B + 15) / 16; }
         else { r.nbx = 1; r.nby = (B * B + 31) / 32; }
         r.count = r.nbx * r.nby;
         return r;
@@ -113,7 +115,7 @@ struct Regions {
         if (kind == 0) {
             lx = (w % nbx) * 8 + (lane & 7);
             ly = (w / nbx) * 4 + (lane >> 3);
-        } else if (kind == 1) {
+        } else if (kind == 1 || kind == 3) {
             lx = (w % nbx) * 8 + (lane & 7);
             ly = (w / nbx) * block_h() + (lane >> 3) + 4 * p;
         } else {
@@ -122,8 +124,10 @@ struct Regions {
             ly = r < B * B ? r / B : B;  // B marks "no pixel"
         }
     }
-    // rows of a block region (kinds 0, 1)
-    __host__ __device__ __forceinline__ int block_h() const { return kind == 0 ? 4 : 8; }
+    // rows of a block region (kinds 0, 1, 3)
+    __host__ __device__ __forceinline__ int block_h() const {
+        return kind == 0 ? 4 : (kind == 1 ? 8 : 16);
+    }
     // tile-local pixel-centre rectangle of region w (conservative)
     template <typename T>
     __device__ __forceinline__ void rect(int w, T &x0, T &x1, T &y0, T &y1) const {
@@ -421,8 +425,8 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
     const unsigned FULL = 0xffffffffu;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int B = tc.B, tx0 = tc.tx0, ty0 = tc.ty0;
-    static_assert(PPL == 1 || PPL == 2, "one or two pixels per lane");
-    const Regions R = Regions::make(PPL == 1 ? 0 : 1, B);
+    static_assert(PPL == 1 || PPL == 2 || PPL == 4, "one, two or four pixels per lane");
+    const Regions R = Regions::make(PPL == 1 ? 0 : (PPL == 2 ? 1 : 3), B);
     bool inside[PPL];
     int pix[PPL];
     T px[PPL], py[PPL];
@@ -474,6 +478,21 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
                         } else if (ok1) {
                             acc[0].add(g1, dx1, dy1, a1, base + m * 32 + b1);
                         }
+                    }
+                } else if constexpr (PPL == 4) {
+                    while (mask) {
+                        const int b1 = __ffs(mask) - 1;
+                        mask &= mask - 1;
+                        const Rec<T> g1 = s_rec[m * 32 + b1];
+                        T dxp[4], dyp[4], ap[4];
+                        bool okp[4];
+#pragma unroll
+                        for (int p = 0; p < 4; ++p)
+                            okp[p] = PixelEval<T>::template alpha<GA>(g1, px[p], py[p], dxp[p],
+                                                                      dyp[p], ap[p]);
+#pragma unroll
+                        for (int p = 0; p < 4; ++p)
+                            if (okp[p]) acc[p].add(g1, dxp[p], dyp[p], ap[p], base + m * 32 + b1);
                     }
                 } else {
                     // written out for two pixels: this exact form compiles to
@@ -529,11 +548,14 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
 #define LIG_RASTER_BWD_MINB 5
 #endif
 
-// Sum forward: two pixels per lane from LIG_RASTER_PPL2_MIN_TILES tiles on
-// (fewer warps per tile; below it one pixel per lane keeps more warps per
-// tile).
+// Sum forward: two pixels per lane from LIG_RASTER_PPL2_MIN_TILES tiles on,
+// four from LIG_RASTER_PPL4_MIN_TILES on (fewer warps per tile, so small
+// images keep more pixels in flight with fewer pixels per lane).
 #ifndef LIG_RASTER_PPL2_MIN_TILES
 #define LIG_RASTER_PPL2_MIN_TILES 0
+#endif
+#ifndef LIG_RASTER_PPL4_MIN_TILES
+#define LIG_RASTER_PPL4_MIN_TILES 2000000000
 #endif
 
 template <typename T, bool GA, int PPL, int MAXT, int MINB>
@@ -1127,8 +1149,9 @@ int raster_fwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
     int rc = pack<T>(n, xys, con, col, op, ws, ws_bytes, s);
     if (rc) return rc;
     const bool ga = dx != nullptr;
-    const bool ppl2 = !ga && geo.total_tiles() >= LIG_RASTER_PPL2_MIN_TILES;
-    const int nt = 32 * Regions::make(ppl2 ? 1 : 0, geo.B).count;
+    const bool ppl4 = !ga && geo.total_tiles() >= LIG_RASTER_PPL4_MIN_TILES;
+    const bool ppl2 = !ga && !ppl4 && geo.total_tiles() >= LIG_RASTER_PPL2_MIN_TILES;
+    const int nt = 32 * Regions::make(ppl4 ? 3 : (ppl2 ? 1 : 0), geo.B).count;
     const size_t sm = (size_t)nt * (sizeof(Rec<T>) + sizeof(uint32_t));
     using K = void (*)(const BatchGeo, const int32_t *, int *, const int32_t *, const int2 *,
                        const int32_t *, const Rec<T> *, T *, T *, T *, T *, T *, int32_t *,
@@ -1136,6 +1159,8 @@ int raster_fwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
     const bool small = nt <= 256;
     K fn = ga ? (small ? raster_fwd_kernel<T, true, 1, 256, LIG_RASTER_FWD_MINB>
                        : raster_fwd_kernel<T, true, 1, 1024, 1>)
+              : ppl4 ? (small ? raster_fwd_kernel<T, false, 4, 256, LIG_RASTER_FWD_MINB>
+                              : raster_fwd_kernel<T, false, 4, 1024, 1>)
               : ppl2 ? (small ? raster_fwd_kernel<T, false, 2, 256, LIG_RASTER_FWD_MINB>
                               : raster_fwd_kernel<T, false, 2, 1024, 1>)
                      : (small ? raster_fwd_kernel<T, false, 1, 256, LIG_RASTER_FWD_MINB>
