@@ -66,7 +66,7 @@ CLOCK_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.a
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["lig", "reference"], default="lig")
     ap.add_argument("--size", type=int, default=H, help="image side (default 8192)")
@@ -101,7 +101,24 @@ class ClockSampler:
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+        # wait for the sampler's first line, so that sampling is live when the
+        # timed region starts; lines written before it are not counted
+        self.n_pre = 0
+        t_end = time.time() + 5.0
+        while self.proc is not None and time.time() < t_end:
+            n = self._count()
+            if n > 0:
+                self.n_pre = n
+                break
+            time.sleep(0.02)
         return self
+
+    def _count(self) -> int:
+        try:
+            with open(self.path) as f:
+                return sum(1 for line in f if line.count(",") >= 8)
+        except OSError:
+            return 0
 
     def __exit__(self, *exc):
         if self.proc is not None:
@@ -121,6 +138,8 @@ class ClockSampler:
                     rows.append(parts)
         finally:
             os.unlink(self.path)
+        if len(rows) > self.n_pre:
+            rows = rows[self.n_pre:]  # samples taken during the timed region
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
         sm = [float(r[1]) for r in rows]
