@@ -25,6 +25,7 @@ CASES = [
     (400, 70, 50, 12, (0.5, 3.0), (0.2, 0.95)),
     (300, 40, 33, 5, (0.3, 2.0), None),
     (2500, 256, 256, 16, (0.5, 8.0), (0.0, 1.0)),  # includes opacity < 1/255: phantom slots
+    (20000, 1040, 1100, 16, (0.5, 4.0), None),  # >= 4096 tiles: four pixels per lane forward
 ]
 
 
