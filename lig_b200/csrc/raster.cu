@@ -53,7 +53,9 @@ template <typename T> struct alignas(16) Rec {
 // the rounding of sigma and __expf, so skipping it changes nothing.  No culling (w < 0) for non-finite inputs, non-positive
 // opacity, non-positive-definite or nearly degenerate conics (b^2 > 0.999 ac),
 // where the reference's per-pixel tests must run everywhere in the tile.
-template <typename T>
+// HALF: the record carries a/2 and c/2 in place of a and c (the fused-loss
+// forward, see sigma_half); the cull data are computed from the full conic.
+template <typename T, bool HALF>
 __global__ void pack_kernel(int n, const T *__restrict__ xys, const T *__restrict__ conics,
                             const T *__restrict__ colors, const T *__restrict__ opac,
                             Rec<T> *__restrict__ recs) {
@@ -89,6 +91,10 @@ __global__ void pack_kernel(int n, const T *__restrict__ xys, const T *__restric
     }
     r.wx = wx;
     r.wy = wy;
+    if (HALF) {
+        r.a *= (T)0.5;
+        r.c *= (T)0.5;
+    }
     recs[i] = r;
 }
 
@@ -206,9 +212,9 @@ __device__ __forceinline__ T sigma_min_rect(T a, T b, T c, T dx0, T dx1, T dy0, 
 // it, reaches sigma <= thr (see pack_kernel: every pixel with sigma > thr
 // fails the reference's own alpha >= 1/255 test).  Records without culling
 // data (wx < 0) touch every region.
-// ELLIPSE = false stops at the box test: cheaper to build, used where the
-// per-pair work is small (forward).
-template <typename T, bool ELLIPSE = true>
+// ELLIPSE = false stops at the box test.  HALF: the record carries the
+// halved conic (fused-loss forward).
+template <typename T, bool ELLIPSE = true, bool HALF = false>
 __device__ __forceinline__ uint32_t region_bits(const Rec<T> &g, const Regions &R, int tx0,
                                                 int ty0) {
     if (!(g.wx >= (T)0)) return R.all();
@@ -221,7 +227,8 @@ __device__ __forceinline__ uint32_t region_bits(const Rec<T> &g, const Regions &
         m &= m - 1;
         T x0, x1, y0, y1;
         R.rect<T>(w, x0, x1, y0, y1);
-        if (sigma_min_rect<T>(g.a, g.b, g.c, x0 - cx, x1 - cx, y0 - cy, y1 - cy) > g.thr)
+        const T a = HALF ? (T)2 * g.a : g.a, c = HALF ? (T)2 * g.c : g.c;
+        if (sigma_min_rect<T>(a, g.b, c, x0 - cx, x1 - cx, y0 - cy, y1 - cy) > g.thr)
             keep &= ~(1u << w);
     }
     return keep;
@@ -274,6 +281,12 @@ __device__ __forceinline__ int next_tile(int *work, int &s_slot, bool first) {
 }
 
 // --------------------------------------------------------------- forward
+#ifndef LIG_RASTER_FWD_ELLIPSE
+#define LIG_RASTER_FWD_ELLIPSE 1  // sum forward: exact ellipse test per region
+#endif
+#ifndef LIG_RASTER_FWD_FUSED
+#define LIG_RASTER_FWD_FUSED 1  // specialised fused-loss forward (no opacities)
+#endif
 // One CTA per tile, warp w = region w (8x4 pixels), one pixel per lane.
 // Batches of blockDim Gaussians (list order) are staged in shared memory, one
 // record per thread, with the next batch's record fetched into registers
@@ -290,6 +303,15 @@ __device__ __forceinline__ int next_tile(int *work, int &s_slot, bool first) {
 // inputs.  Written explicitly so that the surrounding code (several pixels
 // per lane sharing products) cannot change the contraction, and with it the
 // alpha >= 1/255 decisions.
+// Rounded product / fused multiply-add, spelled out so that the compiler
+// cannot contract or reassociate them.
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) {
+    return __fma_rn(a, b, c);
+}
+
 template <typename T>
 __device__ __forceinline__ T sigma_ref(T a, T b, T c, T dx, T dy);
 template <>
@@ -302,6 +324,16 @@ __device__ __forceinline__ double sigma_ref<double>(double a, double b, double c
                                                     double dy) {
     const double ta = __dmul_rn(a, dx), tc = __dmul_rn(c, dy), tb = __dmul_rn(b, dx);
     return __fma_rn(tb, dy, __dmul_rn(0.5, __fma_rn(ta, dx, __dmul_rn(tc, dy))));
+}
+
+// sigma_ref from the halved conic (ha = a/2, hc = c/2):
+//   fma(b dx, dy, fma(ha dx, dx, (hc dy) dy)) == fma(b dx, dy, 0.5 fma(a dx, dx, (c dy) dy))
+// bit for bit — halving is exact and commutes with rounding (away from the
+// subnormal range, where every term is far below any alpha decision) — with
+// one product fewer.
+template <typename T>
+__device__ __forceinline__ T sigma_half(T ha, T b, T hc, T dx, T dy) {
+    return fma_rn(mul_rn(b, dx), dy, fma_rn(mul_rn(ha, dx), dx, mul_rn(mul_rn(hc, dy), dy)));
 }
 
 template <typename T>
@@ -318,6 +350,14 @@ struct PixelEval {
         a = M::min_((T)0.999, g.o * M::exp_(-sigma));
         return !(sigma < (T)0 || a < (T)1 / (T)255);
     }
+    // the fused-loss forward: halved conic in the record, no opacities (o = 1,
+    // so o * exp(-sigma) is exp(-sigma) exactly)
+    static __device__ __forceinline__ bool alpha_fused(const Rec<T> &g, T px, T py, T &a) {
+        using M = Math<T>;
+        const T sigma = sigma_half<T>(g.a, g.b, g.c, g.x - px, g.y - py);
+        a = M::min_((T)0.999, M::exp_(-sigma));
+        return !(sigma < (T)0 || a < (T)1 / (T)255);
+    }
 };
 
 template <typename T, bool GA>
@@ -325,6 +365,13 @@ struct FwdAcc {
     T r = 0, g = 0, b = 0, w = 0;
     T dx[GA ? 3 : 1] = {}, dy[GA ? 3 : 1] = {}, dxy[GA ? 3 : 1] = {};
     int cur = 0;
+    // fused-loss forward: colour and final index only (no wsum, not GA)
+    __device__ __forceinline__ void add_fused(const Rec<T> &q, T a, int idx) {
+        r += q.r * a;
+        g += q.g * a;
+        b += q.bl * a;
+        cur = idx;
+    }
     __device__ __forceinline__ void add(const Rec<T> &q, T dxp, T dyp, T a, int idx) {
         // csrc/forward.cu:264-269, csrc/gradient_aware_rasterizer.cu:451-482
         r += q.r * a;
@@ -409,11 +456,14 @@ __device__ __forceinline__ double fwd_write(const FwdAcc<T, GA> &acc, bool insid
     return 0.0;
 }
 
-// PPL pixels per lane: 1 (8x4 regions, two Gaussians per iteration) or 2
-// (8x8 regions, lane owns (x, y) and (x, y + 4); each Gaussian's record and
-// loop overhead are shared by its two evaluations).  Per pixel the terms are
+// PPL pixels per lane: 1 (8x4 regions, two Gaussians per iteration), 2 (8x8
+// regions, lane owns (x, y) and (x, y + 4)) or 4 (8x16, (x, y + 4p)); each
+// Gaussian's record and loop overhead are shared by the lane's evaluations,
+// whose independent sigma / exp chains overlap.  Per pixel the terms are
 // added in list order either way.
-template <typename T, bool GA, int PPL>
+// FL: the fused-loss forward without opacities (records carry the halved
+// conic; no wsum): per pixel the same alphas and colour sums, fewer operations.
+template <typename T, bool GA, int PPL, bool FL>
 __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int32_t *__restrict__ ids,
                                          const int2 *__restrict__ tile_bins,
                                          const Rec<T> *__restrict__ recs, T *__restrict__ img,
@@ -427,6 +477,9 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
     const int B = tc.B, tx0 = tc.tx0, ty0 = tc.ty0;
     static_assert(PPL == 1 || PPL == 2 || PPL == 4, "one, two or four pixels per lane");
     const Regions R = Regions::make(PPL == 1 ? 0 : (PPL == 2 ? 1 : 3), B);
+    // sum forward: a warp lists only the Gaussians whose alpha >= 1/255
+    // ellipse meets its region (one test per Gaussian and region, staged)
+    constexpr bool ELL = !GA && LIG_RASTER_FWD_ELLIPSE;
     bool inside[PPL];
     int pix[PPL];
     T px[PPL], py[PPL];
@@ -451,14 +504,56 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
             __syncthreads();
             if (tid < cnt) {
                 s_rec[tid] = pre;
-                s_bits[tid] = region_bits<T, false>(pre, R, tx0, ty0);
+                s_bits[tid] = region_bits<T, ELL, FL>(pre, R, tx0, ty0);
             }
             __syncthreads();
             if (base + nt + tid < range.y) pre = recs[__ldg(ids + base + nt + tid)];
             for (int m = 0; m * 32 < cnt; ++m) {
                 const int t = m * 32 + lane;
                 uint32_t mask = __ballot_sync(FULL, t < cnt && ((s_bits[t] >> w) & 1u));
-                if constexpr (PPL == 1) {
+                if constexpr (FL && PPL == 1) {
+                    while (mask) {
+                        const int b1 = __ffs(mask) - 1;
+                        mask &= mask - 1;
+                        const Rec<T> g1 = s_rec[m * 32 + b1];
+                        T a1;
+                        const bool ok1 = PixelEval<T>::alpha_fused(g1, px[0], py[0], a1);
+                        if (mask) {
+                            const int b2 = __ffs(mask) - 1;
+                            mask &= mask - 1;
+                            const Rec<T> g2 = s_rec[m * 32 + b2];
+                            T a2;
+                            const bool ok2 = PixelEval<T>::alpha_fused(g2, px[0], py[0], a2);
+                            if (ok1) acc[0].add_fused(g1, a1, base + m * 32 + b1);
+                            if (ok2) acc[0].add_fused(g2, a2, base + m * 32 + b2);
+                        } else if (ok1) {
+                            acc[0].add_fused(g1, a1, base + m * 32 + b1);
+                        }
+                    }
+                } else if constexpr (FL) {
+                    // a lane's pixels share their column: dx, (a/2) dx and
+                    // b dx once per Gaussian (sigma_half's products)
+                    using M = Math<T>;
+                    while (mask) {
+                        const int b1 = __ffs(mask) - 1;
+                        mask &= mask - 1;
+                        const Rec<T> g1 = s_rec[m * 32 + b1];
+                        const T dx = g1.x - px[0];
+                        const T hadx = mul_rn(g1.a, dx), bdx = mul_rn(g1.b, dx);
+                        T ap[PPL];
+                        bool okp[PPL];
+#pragma unroll
+                        for (int p = 0; p < PPL; ++p) {
+                            const T dy = g1.y - py[p];
+                            const T sg = fma_rn(bdx, dy, fma_rn(hadx, dx, mul_rn(mul_rn(g1.c, dy), dy)));
+                            ap[p] = M::min_((T)0.999, M::exp_(-sg));
+                            okp[p] = !(sg < (T)0 || ap[p] < (T)1 / (T)255);
+                        }
+#pragma unroll
+                        for (int p = 0; p < PPL; ++p)
+                            if (okp[p]) acc[p].add_fused(g1, ap[p], base + m * 32 + b1);
+                    }
+                } else if constexpr (PPL == 1) {
                     while (mask) {
                         const int b1 = __ffs(mask) - 1;
                         mask &= mask - 1;
@@ -479,37 +574,20 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
                             acc[0].add(g1, dx1, dy1, a1, base + m * 32 + b1);
                         }
                     }
-                } else if constexpr (PPL == 4) {
+                } else {
                     while (mask) {
                         const int b1 = __ffs(mask) - 1;
                         mask &= mask - 1;
                         const Rec<T> g1 = s_rec[m * 32 + b1];
-                        T dxp[4], dyp[4], ap[4];
-                        bool okp[4];
+                        T dxp[PPL], dyp[PPL], ap[PPL];
+                        bool okp[PPL];
 #pragma unroll
-                        for (int p = 0; p < 4; ++p)
+                        for (int p = 0; p < PPL; ++p)
                             okp[p] = PixelEval<T>::template alpha<GA>(g1, px[p], py[p], dxp[p],
                                                                       dyp[p], ap[p]);
 #pragma unroll
-                        for (int p = 0; p < 4; ++p)
+                        for (int p = 0; p < PPL; ++p)
                             if (okp[p]) acc[p].add(g1, dxp[p], dyp[p], ap[p], base + m * 32 + b1);
-                    }
-                } else {
-                    // written out for two pixels: this exact form compiles to
-                    // the reference's rounding of sigma for each pixel (a loop
-                    // over the lane's pixels let the compiler share products
-                    // between them and contract differently)
-                    while (mask) {
-                        const int b1 = __ffs(mask) - 1;
-                        mask &= mask - 1;
-                        const Rec<T> g1 = s_rec[m * 32 + b1];
-                        T dxa, dya, aa, dxb, dyb, ab;
-                        const bool oka =
-                            PixelEval<T>::template alpha<GA>(g1, px[0], py[0], dxa, dya, aa);
-                        const bool okb =
-                            PixelEval<T>::template alpha<GA>(g1, px[1], py[1], dxb, dyb, ab);
-                        if (oka) acc[0].add(g1, dxa, dya, aa, base + m * 32 + b1);
-                        if (okb) acc[1].add(g1, dxb, dyb, ab, base + m * 32 + b1);
                     }
                 }
             }
@@ -558,7 +636,7 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
 #define LIG_RASTER_PPL4_MIN_TILES 4096  // measured: faster from 2048^2 up, not at 512^2
 #endif
 
-template <typename T, bool GA, int PPL, int MAXT, int MINB>
+template <typename T, bool GA, int PPL, int MAXT, int MINB, bool FL = false>
 __global__ void __launch_bounds__(MAXT, MINB)
 raster_fwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work,
                   const int32_t *__restrict__ ids, const int2 *__restrict__ tile_bins,
@@ -574,8 +652,8 @@ raster_fwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work
     for (int tile = next_tile(work, s_slot, true); tile < n_tiles;
          tile = next_tile(work, s_slot, false)) {
         const TileCtx tc = tile_ctx(geo, cum, d_total, tile);
-        fwd_tile<T, GA, PPL>(tc, tile, ids, tile_bins, recs, img, wsum, odx, ody, odxy,
-                             final_idx, s_rec, s_bits, l2);
+        fwd_tile<T, GA, PPL, FL>(tc, tile, ids, tile_bins, recs, img, wsum, odx, ody, odxy,
+                                 final_idx, s_rec, s_bits, l2);
     }
 }
 
@@ -710,10 +788,74 @@ struct CotSrc {
 
 template <typename T, bool GA>
 struct alignas(16) PixRec {
-    T px, py, vw, vo0, vo1, vo2;
+    T vo0, vo1, vo2, vw;  // first: one 16-byte load in the lean loop
+    T px, py;
     int fin;
     T vd[GA ? 9 : 1];  // vdx.rgb, vdy.rgb, vdxy.rgb
 };
+
+#ifndef LIG_RASTER_BWD_COLS
+#define LIG_RASTER_BWD_COLS 1  // lean backward: column-major region walk
+#endif
+
+// Lean backward of one Gaussian over the pixels of one 8x4 region that this
+// lane takes: columns part, part + 2^LS, ... (8 >> LS of them) in each of the
+// four rows, column by column.  The separable pieces of sigma are shared:
+// per row dy and (c/2 dy) dy, per column dx, (a/2) dx and b dx, so that
+//   sigma = fma(b dx, dy, fma((a/2) dx, dx, ((c/2) dy) dy))
+// which equals sigma_ref's fma(b dx, dy, 0.5 fma(a dx, dx, (c dy) dy)) bit for
+// bit (halving is exact and commutes with rounding away from the subnormal
+// range) with one product fewer.  No opacities on this path (o = 1, so
+// alpha = min(clamp, exp(-sigma)) is the reference's o * exp(-sigma) clamped).
+// No final-index test either: a Gaussian after a pixel's final index fails
+// that pixel's alpha test here exactly as it did in the forward.  A skipped
+// pair adds zeros.  The moment sums of v_sigma dx^i dy^j (v_sigma =
+// -alpha v_alpha) use dx constant along a column: Sx, Sxx and Sxy take one
+// term per column.  Leaves Sx, Sy, Sxx, Sxy, Syy in acc[0, 1, 4, 5, 6] and the
+// colour sums in acc[7..9].
+template <typename T, int LS>
+__device__ __forceinline__ void lean_region(const Rec<T> &g, T clamp,
+                                            const PixRec<T, false> *__restrict__ pix, int part,
+                                            T px0, T py0, T (&acc)[11]) {
+    using M = Math<T>;
+    constexpr int NC = 8 >> LS, JS = 1 << LS;
+    const T ha = (T)0.5 * g.a, hc = (T)0.5 * g.c;
+    T dy[4], cdd[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        dy[r] = g.y - (py0 + (T)r);
+        cdd[r] = mul_rn(mul_rn(hc, dy[r]), dy[r]);
+    }
+    T sx = 0, sy = 0, sxx = 0, sxy = 0, syy = 0, c0 = 0, c1 = 0, c2 = 0;
+#pragma unroll
+    for (int k = 0; k < NC; ++k) {
+        const T dx = g.x - (px0 + (T)(k * JS));
+        const T hadx = mul_rn(ha, dx), bdx = mul_rn(g.b, dx);
+        T wc = 0, yc = 0;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const PixRec<T, false> &c = pix[r * 8 + part + k * JS];
+            const T s = fma_rn(bdx, dy[r], fma_rn(hadx, dx, cdd[r]));
+            const T al = M::min_(clamp, M::exp_(-s));
+            const T a = (s < (T)0 || al < (T)1 / (T)255) ? (T)0 : al;
+            c0 += a * c.vo0;
+            c1 += a * c.vo1;
+            c2 += a * c.vo2;
+            const T wv = a * (g.r * c.vo0 + g.g * c.vo1 + g.bl * c.vo2);  // -v_sigma
+            wc += wv;
+            const T ty = wv * dy[r];
+            yc += ty;
+            syy += ty * dy[r];
+        }
+        const T tx = wc * dx;
+        sx += tx;
+        sxx += tx * dx;
+        sy += yc;
+        sxy += yc * dx;
+    }
+    acc[0] = -sx; acc[1] = -sy; acc[4] = -sxx; acc[5] = -sxy; acc[6] = -syy;
+    acc[7] = c0; acc[8] = c1; acc[9] = c2;
+}
 
 // LEAN (sum backward of the fused fit loss, no opacities, no wsum
 // cotangent): only the gradients the fit needs — v_xy, v_conic, v_rgb — are
@@ -839,7 +981,21 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
 #pragma unroll
             for (int q = 0; q < 11; ++q) acc[q] = 0;
             bool touched = false;
-            if constexpr (LEAN && !GA && LIG_RASTER_BWD_PAIR) {
+            if constexpr (LEAN && !GA && LIG_RASTER_BWD_COLS) {
+                // every listed (Gaussian, region) pair met the region's
+                // ellipse test; an untouched one adds zeros
+                touched = act;
+                const T px0 = (T)(tx0 + (w % R.nbx) * 8 + part) + (T)0.5;
+                const T py0 = (T)(ty0 + (w / R.nbx) * 4) + (T)0.5;
+                if (act) {
+                    switch (lsplit) {
+                    case 0: lean_region<T, 0>(g, clamp, my_pix, part, px0, py0, acc); break;
+                    case 1: lean_region<T, 1>(g, clamp, my_pix, part, px0, py0, acc); break;
+                    case 2: lean_region<T, 2>(g, clamp, my_pix, part, px0, py0, acc); break;
+                    default: lean_region<T, 3>(g, clamp, my_pix, part, px0, py0, acc); break;
+                    }
+                }
+            } else if constexpr (LEAN && !GA && LIG_RASTER_BWD_PAIR) {
                 // two of the lane's pixels per iteration: their sigma / alpha
                 // chains overlap; accumulation stays in pixel order
                 auto body = [&](const PixRec<T, GA> &c, T alpha, T dx, T dy) {
@@ -1070,11 +1226,13 @@ __global__ void unpack_grads_kernel(int n, const T *__restrict__ packed, Grads<T
 // ------------------------------------------------------------------ host
 template <typename T>
 int pack(int n, const void *xys, const void *con, const void *col, const void *op, void *ws,
-         size_t ws_bytes, cudaStream_t s) {
+         size_t ws_bytes, cudaStream_t s, bool half = false) {
     if (ws_bytes < sizeof(Rec<T>) * (size_t)n) return LIG_ERR_WORKSPACE;
-    if (n > 0)
-        pack_kernel<T><<<(n + 255) / 256, 256, 0, s>>>(n, (const T *)xys, (const T *)con,
-                                                      (const T *)col, (const T *)op, (Rec<T> *)ws);
+    if (n > 0) {
+        auto k = half ? pack_kernel<T, true> : pack_kernel<T, false>;
+        k<<<(n + 255) / 256, 256, 0, s>>>(n, (const T *)xys, (const T *)con, (const T *)col,
+                                          (const T *)op, (Rec<T> *)ws);
+    }
     note_launches(n > 0 ? 1 : 0);
     LIG_LAUNCH_CHECK();
     return LIG_OK;
@@ -1146,9 +1304,11 @@ int raster_fwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
                void *dy, void *dxy, int32_t *fin, cudaStream_t s,
                L2Fwd<T> l2 = L2Fwd<T>{nullptr, nullptr}, L2Out<T> l2o = L2Out<T>{}) {
     const int n = geo.total_points();
-    int rc = pack<T>(n, xys, con, col, op, ws, ws_bytes, s);
-    if (rc) return rc;
     const bool ga = dx != nullptr;
+    // fused loss without opacities: the specialised forward (halved conic)
+    const bool fl = !ga && l2.target && !op && LIG_RASTER_FWD_FUSED;
+    int rc = pack<T>(n, xys, con, col, op, ws, ws_bytes, s, fl);
+    if (rc) return rc;
     const bool ppl4 = !ga && geo.total_tiles() >= LIG_RASTER_PPL4_MIN_TILES;
     const bool ppl2 = !ga && !ppl4 && geo.total_tiles() >= LIG_RASTER_PPL2_MIN_TILES;
     const int nt = 32 * Regions::make(ppl4 ? 3 : (ppl2 ? 1 : 0), geo.B).count;
@@ -1157,8 +1317,15 @@ int raster_fwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
                        const int32_t *, const Rec<T> *, T *, T *, T *, T *, T *, int32_t *,
                        L2Fwd<T>);
     const bool small = nt <= 256;
-    K fn = ga ? (small ? raster_fwd_kernel<T, true, 1, 256, LIG_RASTER_FWD_MINB>
+    constexpr int FM = LIG_RASTER_FWD_MINB;
+    K fn = ga ? (small ? raster_fwd_kernel<T, true, 1, 256, FM>
                        : raster_fwd_kernel<T, true, 1, 1024, 1>)
+         : fl ? (ppl4 ? (small ? raster_fwd_kernel<T, false, 4, 256, FM, true>
+                               : raster_fwd_kernel<T, false, 4, 1024, 1, true>)
+                 : ppl2 ? (small ? raster_fwd_kernel<T, false, 2, 256, FM, true>
+                                 : raster_fwd_kernel<T, false, 2, 1024, 1, true>)
+                        : (small ? raster_fwd_kernel<T, false, 1, 256, FM, true>
+                                 : raster_fwd_kernel<T, false, 1, 1024, 1, true>))
               : ppl4 ? (small ? raster_fwd_kernel<T, false, 4, 256, LIG_RASTER_FWD_MINB>
                               : raster_fwd_kernel<T, false, 4, 1024, 1>)
               : ppl2 ? (small ? raster_fwd_kernel<T, false, 2, 256, LIG_RASTER_FWD_MINB>

@@ -188,12 +188,15 @@ def test_fused_render_l2_matches_unfused_chain():
         assert rel_err(np_(a.grad), np_(b.grad)) <= 1e-5
 
 
-def test_fused_l2_forward_diff_and_loss():
+@pytest.mark.parametrize("H,W,B,n", [(150, 170, 16, 3000),
+                                     (1040, 1100, 16, 20000),  # >= 4096 tiles: four pixels per lane
+                                     (97, 203, 12, 2500),
+                                     (130, 90, 32, 2000)])
+def test_fused_l2_forward_diff_and_loss(H, W, B, n):
     """lig_raster_fwd_l2: diff = mask * (clamp(x) - t) bit-exact against the
     plain forward's image, loss against the separate loss kernel (different
     summation order: 1e-6 relative), final_idx identical; and the backward
     from diff equals the backward from (image, target)."""
-    H, W, B, n = 150, 170, 16, 3000
     means, L, colors, _ = scene(n, H, W, diag=(0.5, 5.0), seed=6)
     g = torch.Generator().manual_seed(10)
     target = torch.rand(H, W, 3, generator=g).cuda()
