@@ -234,6 +234,20 @@ __device__ __forceinline__ uint32_t region_bits(const Rec<T> &g, const Regions &
     return keep;
 }
 
+// One region's test of region_bits: does the Gaussian reach region w?
+template <typename T, bool ELLIPSE, bool HALF>
+__device__ __forceinline__ bool region_hit(const Rec<T> &g, const Regions &R, int w, int tx0,
+                                           int ty0) {
+    if (!(g.wx >= (T)0)) return true;
+    T x0, x1, y0, y1;
+    R.rect<T>(w, x0, x1, y0, y1);
+    const T cx = g.x - (T)tx0, cy = g.y - (T)ty0;
+    if (cx + g.wx < x0 || cx - g.wx > x1 || cy + g.wy < y0 || cy - g.wy > y1) return false;
+    if (!ELLIPSE) return true;
+    const T a = HALF ? (T)2 * g.a : g.a, c = HALF ? (T)2 * g.c : g.c;
+    return !(sigma_min_rect<T>(a, g.b, c, x0 - cx, x1 - cx, y0 - cy, y1 - cy) > g.thr);
+}
+
 // ------------------------------------------------------------ tile setup
 // Work item -> image and tile origin.  Work items index the flattened
 // (image, tile) list of a BatchGeo; a single image is a batch of one.
@@ -281,6 +295,9 @@ __device__ __forceinline__ int next_tile(int *work, int &s_slot, bool first) {
 }
 
 // --------------------------------------------------------------- forward
+#ifndef LIG_RASTER_FWD_WARPS
+#define LIG_RASTER_FWD_WARPS 1  // sum forward: warps stream the tile list independently
+#endif
 #ifndef LIG_RASTER_FWD_ELLIPSE
 #define LIG_RASTER_FWD_ELLIPSE 1  // sum forward: exact ellipse test per region
 #endif
@@ -471,7 +488,6 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
                                          T *__restrict__ ody, T *__restrict__ odxy,
                                          int32_t *__restrict__ final_idx, Rec<T> *s_rec,
                                          uint32_t *s_bits, const L2Fwd<T> &l2) {
-    const int nt = blockDim.x;
     const unsigned FULL = 0xffffffffu;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int B = tc.B, tx0 = tc.tx0, ty0 = tc.ty0;
@@ -495,100 +511,124 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
     }
 
     FwdAcc<T, GA> acc[PPL];
+    // walk the Gaussians of `mask` (bits of the 32 records at rb, list
+    // indices ib + bit) in list order
+    auto walk = [&](uint32_t mask, const Rec<T> *rb, int ib) {
+        if constexpr (FL && PPL == 1) {
+            while (mask) {
+                const int b1 = __ffs(mask) - 1;
+                mask &= mask - 1;
+                const Rec<T> g1 = rb[b1];
+                T a1;
+                const bool ok1 = PixelEval<T>::alpha_fused(g1, px[0], py[0], a1);
+                if (mask) {
+                    const int b2 = __ffs(mask) - 1;
+                    mask &= mask - 1;
+                    const Rec<T> g2 = rb[b2];
+                    T a2;
+                    const bool ok2 = PixelEval<T>::alpha_fused(g2, px[0], py[0], a2);
+                    if (ok1) acc[0].add_fused(g1, a1, ib + b1);
+                    if (ok2) acc[0].add_fused(g2, a2, ib + b2);
+                } else if (ok1) {
+                    acc[0].add_fused(g1, a1, ib + b1);
+                }
+            }
+        } else if constexpr (FL) {
+            // a lane's pixels share their column: dx, (a/2) dx and
+            // b dx once per Gaussian (sigma_half's products)
+            using M = Math<T>;
+            while (mask) {
+                const int b1 = __ffs(mask) - 1;
+                mask &= mask - 1;
+                const Rec<T> g1 = rb[b1];
+                const T dx = g1.x - px[0];
+                const T hadx = mul_rn(g1.a, dx), bdx = mul_rn(g1.b, dx);
+                T ap[PPL];
+                bool okp[PPL];
+#pragma unroll
+                for (int p = 0; p < PPL; ++p) {
+                    const T dy = g1.y - py[p];
+                    const T sg = fma_rn(bdx, dy, fma_rn(hadx, dx, mul_rn(mul_rn(g1.c, dy), dy)));
+                    ap[p] = M::min_((T)0.999, M::exp_(-sg));
+                    okp[p] = !(sg < (T)0 || ap[p] < (T)1 / (T)255);
+                }
+#pragma unroll
+                for (int p = 0; p < PPL; ++p)
+                    if (okp[p]) acc[p].add_fused(g1, ap[p], ib + b1);
+            }
+        } else if constexpr (PPL == 1) {
+            while (mask) {
+                const int b1 = __ffs(mask) - 1;
+                mask &= mask - 1;
+                const Rec<T> g1 = rb[b1];
+                T dx1, dy1, a1;
+                const bool ok1 =
+                    PixelEval<T>::template alpha<GA>(g1, px[0], py[0], dx1, dy1, a1);
+                if (mask) {
+                    const int b2 = __ffs(mask) - 1;
+                    mask &= mask - 1;
+                    const Rec<T> g2 = rb[b2];
+                    T dx2, dy2, a2;
+                    const bool ok2 =
+                        PixelEval<T>::template alpha<GA>(g2, px[0], py[0], dx2, dy2, a2);
+                    if (ok1) acc[0].add(g1, dx1, dy1, a1, ib + b1);
+                    if (ok2) acc[0].add(g2, dx2, dy2, a2, ib + b2);
+                } else if (ok1) {
+                    acc[0].add(g1, dx1, dy1, a1, ib + b1);
+                }
+            }
+        } else {
+            while (mask) {
+                const int b1 = __ffs(mask) - 1;
+                mask &= mask - 1;
+                const Rec<T> g1 = rb[b1];
+                T dxp[PPL], dyp[PPL], ap[PPL];
+                bool okp[PPL];
+#pragma unroll
+                for (int p = 0; p < PPL; ++p)
+                    okp[p] = PixelEval<T>::template alpha<GA>(g1, px[p], py[p], dxp[p],
+                                                              dyp[p], ap[p]);
+#pragma unroll
+                for (int p = 0; p < PPL; ++p)
+                    if (okp[p]) acc[p].add(g1, dxp[p], dyp[p], ap[p], ib + b1);
+            }
+        }
+    };
     if (!tc.empty) {
         const int2 range = tile_bins[tile];
-        Rec<T> pre;
-        if (range.x + tid < range.y) pre = recs[__ldg(ids + range.x + tid)];
-        for (int base = range.x; base < range.y; base += nt) {
-            const int cnt = min(nt, range.y - base);
-            __syncthreads();
-            if (tid < cnt) {
-                s_rec[tid] = pre;
-                s_bits[tid] = region_bits<T, ELL, FL>(pre, R, tx0, ty0);
+        if constexpr (LIG_RASTER_FWD_WARPS) {
+            // each warp streams the tile's list in chunks of 32 on its own
+            // (its region's test only, no block barriers: warps whose
+            // regions have short lists do not wait for the others)
+            Rec<T> *w_rec = s_rec + w * 32;
+            Rec<T> pre;
+            if (range.x + lane < range.y) pre = recs[__ldg(ids + range.x + lane)];
+            for (int base = range.x; base < range.y; base += 32) {
+                const bool hit =
+                    base + lane < range.y && region_hit<T, ELL, FL>(pre, R, w, tx0, ty0);
+                __syncwarp();
+                w_rec[lane] = pre;
+                __syncwarp();
+                if (base + 32 + lane < range.y) pre = recs[__ldg(ids + base + 32 + lane)];
+                walk(__ballot_sync(FULL, hit), w_rec, base);
             }
-            __syncthreads();
-            if (base + nt + tid < range.y) pre = recs[__ldg(ids + base + nt + tid)];
-            for (int m = 0; m * 32 < cnt; ++m) {
-                const int t = m * 32 + lane;
-                uint32_t mask = __ballot_sync(FULL, t < cnt && ((s_bits[t] >> w) & 1u));
-                if constexpr (FL && PPL == 1) {
-                    while (mask) {
-                        const int b1 = __ffs(mask) - 1;
-                        mask &= mask - 1;
-                        const Rec<T> g1 = s_rec[m * 32 + b1];
-                        T a1;
-                        const bool ok1 = PixelEval<T>::alpha_fused(g1, px[0], py[0], a1);
-                        if (mask) {
-                            const int b2 = __ffs(mask) - 1;
-                            mask &= mask - 1;
-                            const Rec<T> g2 = s_rec[m * 32 + b2];
-                            T a2;
-                            const bool ok2 = PixelEval<T>::alpha_fused(g2, px[0], py[0], a2);
-                            if (ok1) acc[0].add_fused(g1, a1, base + m * 32 + b1);
-                            if (ok2) acc[0].add_fused(g2, a2, base + m * 32 + b2);
-                        } else if (ok1) {
-                            acc[0].add_fused(g1, a1, base + m * 32 + b1);
-                        }
-                    }
-                } else if constexpr (FL) {
-                    // a lane's pixels share their column: dx, (a/2) dx and
-                    // b dx once per Gaussian (sigma_half's products)
-                    using M = Math<T>;
-                    while (mask) {
-                        const int b1 = __ffs(mask) - 1;
-                        mask &= mask - 1;
-                        const Rec<T> g1 = s_rec[m * 32 + b1];
-                        const T dx = g1.x - px[0];
-                        const T hadx = mul_rn(g1.a, dx), bdx = mul_rn(g1.b, dx);
-                        T ap[PPL];
-                        bool okp[PPL];
-#pragma unroll
-                        for (int p = 0; p < PPL; ++p) {
-                            const T dy = g1.y - py[p];
-                            const T sg = fma_rn(bdx, dy, fma_rn(hadx, dx, mul_rn(mul_rn(g1.c, dy), dy)));
-                            ap[p] = M::min_((T)0.999, M::exp_(-sg));
-                            okp[p] = !(sg < (T)0 || ap[p] < (T)1 / (T)255);
-                        }
-#pragma unroll
-                        for (int p = 0; p < PPL; ++p)
-                            if (okp[p]) acc[p].add_fused(g1, ap[p], base + m * 32 + b1);
-                    }
-                } else if constexpr (PPL == 1) {
-                    while (mask) {
-                        const int b1 = __ffs(mask) - 1;
-                        mask &= mask - 1;
-                        const Rec<T> g1 = s_rec[m * 32 + b1];
-                        T dx1, dy1, a1;
-                        const bool ok1 =
-                            PixelEval<T>::template alpha<GA>(g1, px[0], py[0], dx1, dy1, a1);
-                        if (mask) {
-                            const int b2 = __ffs(mask) - 1;
-                            mask &= mask - 1;
-                            const Rec<T> g2 = s_rec[m * 32 + b2];
-                            T dx2, dy2, a2;
-                            const bool ok2 =
-                                PixelEval<T>::template alpha<GA>(g2, px[0], py[0], dx2, dy2, a2);
-                            if (ok1) acc[0].add(g1, dx1, dy1, a1, base + m * 32 + b1);
-                            if (ok2) acc[0].add(g2, dx2, dy2, a2, base + m * 32 + b2);
-                        } else if (ok1) {
-                            acc[0].add(g1, dx1, dy1, a1, base + m * 32 + b1);
-                        }
-                    }
-                } else {
-                    while (mask) {
-                        const int b1 = __ffs(mask) - 1;
-                        mask &= mask - 1;
-                        const Rec<T> g1 = s_rec[m * 32 + b1];
-                        T dxp[PPL], dyp[PPL], ap[PPL];
-                        bool okp[PPL];
-#pragma unroll
-                        for (int p = 0; p < PPL; ++p)
-                            okp[p] = PixelEval<T>::template alpha<GA>(g1, px[p], py[p], dxp[p],
-                                                                      dyp[p], ap[p]);
-#pragma unroll
-                        for (int p = 0; p < PPL; ++p)
-                            if (okp[p]) acc[p].add(g1, dxp[p], dyp[p], ap[p], base + m * 32 + b1);
-                    }
+        } else {
+            const int nt = blockDim.x;
+            Rec<T> pre;
+            if (range.x + tid < range.y) pre = recs[__ldg(ids + range.x + tid)];
+            for (int base = range.x; base < range.y; base += nt) {
+                const int cnt = min(nt, range.y - base);
+                __syncthreads();
+                if (tid < cnt) {
+                    s_rec[tid] = pre;
+                    s_bits[tid] = region_bits<T, ELL, FL>(pre, R, tx0, ty0);
+                }
+                __syncthreads();
+                if (base + nt + tid < range.y) pre = recs[__ldg(ids + base + nt + tid)];
+                for (int m = 0; m * 32 < cnt; ++m) {
+                    const int t = m * 32 + lane;
+                    walk(__ballot_sync(FULL, t < cnt && ((s_bits[t] >> w) & 1u)), s_rec + m * 32,
+                         base + m * 32);
                 }
             }
         }
@@ -794,6 +834,9 @@ struct alignas(16) PixRec {
     T vd[GA ? 9 : 1];  // vdx.rgb, vdy.rgb, vdxy.rgb
 };
 
+#ifndef LIG_RASTER_BWD_STREAM
+#define LIG_RASTER_BWD_STREAM 0  // lean backward: warps stream the tile list independently
+#endif
 #ifndef LIG_RASTER_BWD_COLS
 #define LIG_RASTER_BWD_COLS 1  // lean backward: column-major region walk
 #endif
@@ -1169,7 +1212,146 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
     }
 }
 
-template <typename T, bool GA, bool LEAN, int MAXT, int MINB>
+// Lean backward, streamed per warp (no block barriers within a tile): warp w
+// stages its region's 32 pixels, then walks the tile's list in chunks of 32
+// on its own — each lane loads one record and tests it against the region
+// (cull box, then the exact ellipse) — queueing the hits in a 64-entry ring
+// in shared memory; every full group of 32 queued hits is processed one
+// Gaussian per lane (lean_region), the last partial group with lanes split
+// as in bwd_tile.  The list is cut at the region's largest final index.
+constexpr int kBwdRing = 64;
+
+template <typename T>
+__host__ __device__ constexpr size_t bwd_stream_smem(int nt) {
+    return (size_t)nt * sizeof(PixRec<T, false>) +
+           (size_t)(nt / 32) * kBwdRing * (sizeof(Rec<T>) + sizeof(int32_t));
+}
+
+template <typename T>
+__device__ __forceinline__ void bwd_tile_stream(const TileCtx &tc, int tile,
+                                                const int32_t *__restrict__ ids,
+                                                const int2 *__restrict__ tile_bins,
+                                                const Rec<T> *__restrict__ recs,
+                                                const int32_t *__restrict__ final_idx,
+                                                CotSrc<T> cot, T clamp, T *__restrict__ packed) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int nt = blockDim.x;
+    const unsigned FULL = 0xffffffffu;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    PixRec<T, false> *my_pix = reinterpret_cast<PixRec<T, false> *>(smem_raw) + w * 32;
+    Rec<T> *ring = reinterpret_cast<Rec<T> *>(reinterpret_cast<PixRec<T, false> *>(smem_raw) +
+                                              nt) + w * kBwdRing;
+    int32_t *ring_id = reinterpret_cast<int32_t *>(
+                           reinterpret_cast<Rec<T> *>(reinterpret_cast<PixRec<T, false> *>(
+                                                          smem_raw) + nt) + (nt / 32) * kBwdRing) +
+                       w * kBwdRing;
+    if (tc.empty) return;  // gradients stay zero (rasterize.py:156-161)
+    const int B = tc.B, H = tc.H, W = tc.W, tx0 = tc.tx0, ty0 = tc.ty0;
+    cot.scale = (T)(2.0 / (3.0 * (double)H * (double)W));
+    const Regions R = Regions::make(0, B);
+
+    int w_end;
+    {  // stage this lane's pixel (region w, slot lane)
+        int lx, ly;
+        R.pixel(w, lane, 0, lx, ly);
+        const int gx = tx0 + lx, gy = ty0 + ly;
+        const bool inside = lx < B && ly < B && gx < W && gy < H;
+        const int p = inside ? tc.poff + gy * W + gx : 0;
+        PixRec<T, false> c;
+        c.px = (T)gx + (T)0.5;
+        c.py = (T)gy + (T)0.5;
+        c.vo0 = c.vo1 = c.vo2 = c.vw = (T)0;
+        if (inside) cot.get(p, c.vo0, c.vo1, c.vo2, c.vw);
+        c.fin = inside ? final_idx[p] : -1;
+        c.vd[0] = (T)0;
+        __syncwarp();  // the previous tile's readers of my_pix are done
+        my_pix[lane] = c;
+        w_end = c.fin;
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) w_end = max(w_end, __shfl_xor_sync(FULL, w_end, o));
+        __syncwarp();
+    }
+    const int2 range = tile_bins[tile];
+    const int end = min(range.y, w_end + 1);
+    const T px_base = (T)(tx0 + (w % R.nbx) * 8) + (T)0.5;
+    const T py0 = (T)(ty0 + (w / R.nbx) * 4) + (T)0.5;
+
+    // one group of `left` (<= 32) queued Gaussians from ring[head ...]
+    auto group = [&](int head, int left) {
+        const int lsplit = !LIG_RASTER_BWD_SPLIT ? 0 : left <= 4 ? 3 : left <= 8 ? 2
+                                                     : left <= 16 ? 1 : 0;
+        const int gi = lane >> lsplit, part = lane & ((1 << lsplit) - 1);
+        const bool act = gi < left;
+        const int slot = (head + (act ? gi : 0)) & (kBwdRing - 1);
+        const Rec<T> g = ring[slot];
+        T acc[11];
+#pragma unroll
+        for (int q = 0; q < 11; ++q) acc[q] = 0;
+        const T px0 = px_base + (T)part;
+        if (act) {
+            switch (lsplit) {
+            case 0: lean_region<T, 0>(g, clamp, my_pix, part, px0, py0, acc); break;
+            case 1: lean_region<T, 1>(g, clamp, my_pix, part, px0, py0, acc); break;
+            case 2: lean_region<T, 2>(g, clamp, my_pix, part, px0, py0, acc); break;
+            default: lean_region<T, 3>(g, clamp, my_pix, part, px0, py0, acc); break;
+            }
+        }
+        for (int o = 1; o < (1 << lsplit); o <<= 1) {  // combine the lane group
+#pragma unroll
+            for (int q = 0; q < 11; ++q) {
+                if (q == 2 || q == 3 || q == 10) continue;
+                acc[q] += __shfl_xor_sync(FULL, acc[q], o);
+            }
+        }
+        if (act && part == 0) {
+            // v_xy = (a Sx + b Sy, b Sx + c Sy); v_conic = (Sxx/2, Sxy, Syy/2)
+            const T sx = acc[0], sy = acc[1];
+            T *dst = packed + (size_t)ring_id[slot] * 8;
+            const T v[8] = {g.a * sx + g.b * sy, g.b * sx + g.c * sy, (T)0.5 * acc[4], acc[5],
+                            (T)0.5 * acc[6], acc[7], acc[8], acc[9]};
+            if constexpr (sizeof(T) == 4) {
+                float4 *d4 = reinterpret_cast<float4 *>(dst);
+                atomicAdd(d4, make_float4(v[0], v[1], v[2], v[3]));
+                atomicAdd(d4 + 1, make_float4(v[4], v[5], v[6], v[7]));
+            } else {
+#pragma unroll
+                for (int q = 0; q < 8; ++q) atomicAdd(dst + q, v[q]);
+            }
+        }
+    };
+
+    int head = 0, qn = 0;  // ring state (warp-uniform)
+    Rec<T> pre;
+    int pre_id = -1;
+    if (range.x + lane < end) {
+        pre_id = __ldg(ids + range.x + lane);
+        pre = recs[pre_id];
+    }
+    for (int base = range.x; base < end; base += 32) {
+        const bool hit = base + lane < end && region_hit<T, true, false>(pre, R, w, tx0, ty0);
+        const uint32_t mask = __ballot_sync(FULL, hit);
+        if (hit) {
+            const int pos = (head + qn + __popc(mask & ((1u << lane) - 1u))) & (kBwdRing - 1);
+            ring[pos] = pre;
+            ring_id[pos] = pre_id;
+        }
+        qn += __popc(mask);
+        if (base + 32 + lane < end) {
+            pre_id = __ldg(ids + base + 32 + lane);
+            pre = recs[pre_id];
+        }
+        __syncwarp();
+        if (qn >= 32) {
+            group(head, 32);
+            __syncwarp();  // the group's ring slots are read before they are refilled
+            head = (head + 32) & (kBwdRing - 1);
+            qn -= 32;
+        }
+    }
+    if (qn > 0) group(head, qn);
+}
+
+template <typename T, bool GA, bool LEAN, int MAXT, int MINB, bool STREAM = false>
 __global__ void __launch_bounds__(MAXT, MINB)
 raster_bwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work,
                   const int32_t *__restrict__ ids, const int2 *__restrict__ tile_bins,
@@ -1182,8 +1364,11 @@ raster_bwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work
     for (int tile = next_tile(work, s_slot, true); tile < n_tiles;
          tile = next_tile(work, s_slot, false)) {
         const TileCtx tc = tile_ctx(geo, cum, d_total, tile);
-        bwd_tile<T, GA, LEAN>(tc, tile, ids, tile_bins, recs, final_idx, cot, v_dx, v_dy, v_dxy,
-                              clamp, packed, s_end);
+        if constexpr (STREAM)
+            bwd_tile_stream<T>(tc, tile, ids, tile_bins, recs, final_idx, cot, clamp, packed);
+        else
+            bwd_tile<T, GA, LEAN>(tc, tile, ids, tile_bins, recs, final_idx, cot, v_dx, v_dy,
+                                  v_dxy, clamp, packed, s_end);
     }
 }
 
@@ -1386,14 +1571,19 @@ int raster_bwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
     const int nt = 32 * Regions::make(ga ? 2 : 0, geo.B).count;
     const int nw = nt / 32;
     const size_t pix = ga ? sizeof(PixRec<T, true>) : sizeof(PixRec<T, false>);
-    const size_t sm = (size_t)nt * pix + (size_t)nt * (sizeof(Rec<T>) + 2 * sizeof(uint32_t)) +
-                      (size_t)nw * nt * sizeof(uint16_t);
+    // (the per-warp rings of 32-wide fp64 tiles would not fit in shared memory)
+    const bool stream = lean && LIG_RASTER_BWD_STREAM && bwd_stream_smem<T>(nt) <= 160 * 1024;
+    const size_t sm = stream ? bwd_stream_smem<T>(nt)
+                             : (size_t)nt * pix + (size_t)nt * (sizeof(Rec<T>) + 2 * sizeof(uint32_t)) +
+                                   (size_t)nw * nt * sizeof(uint16_t);
     using K = void (*)(const BatchGeo, const int32_t *, int *, const int32_t *, const int2 *,
                        const int32_t *, const Rec<T> *, const int32_t *, CotSrc<T>, const T *,
                        const T *, const T *, T, T *);
     const bool small = nt <= 256;
     K fn = ga ? (small ? raster_bwd_kernel<T, true, false, 256, LIG_RASTER_BWD_MINB>
                        : raster_bwd_kernel<T, true, false, 1024, 1>)
+              : stream ? (small ? raster_bwd_kernel<T, false, true, 256, LIG_RASTER_BWD_LEAN_MINB, true>
+                                : raster_bwd_kernel<T, false, true, 1024, 1, true>)
               : lean ? (small ? raster_bwd_kernel<T, false, true, 256, LIG_RASTER_BWD_LEAN_MINB>
                               : raster_bwd_kernel<T, false, true, 1024, 1>)
                      : (small ? raster_bwd_kernel<T, false, false, 256, LIG_RASTER_BWD_MINB>
