@@ -834,9 +834,6 @@ struct alignas(16) PixRec {
     T vd[GA ? 9 : 1];  // vdx.rgb, vdy.rgb, vdxy.rgb
 };
 
-#ifndef LIG_RASTER_BWD_STREAM
-#define LIG_RASTER_BWD_STREAM 0  // lean backward: warps stream the tile list independently
-#endif
 #ifndef LIG_RASTER_BWD_COLS
 #define LIG_RASTER_BWD_COLS 1  // lean backward: column-major region walk
 #endif
@@ -1212,146 +1209,7 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
     }
 }
 
-// Lean backward, streamed per warp (no block barriers within a tile): warp w
-// stages its region's 32 pixels, then walks the tile's list in chunks of 32
-// on its own — each lane loads one record and tests it against the region
-// (cull box, then the exact ellipse) — queueing the hits in a 64-entry ring
-// in shared memory; every full group of 32 queued hits is processed one
-// Gaussian per lane (lean_region), the last partial group with lanes split
-// as in bwd_tile.  The list is cut at the region's largest final index.
-constexpr int kBwdRing = 64;
-
-template <typename T>
-__host__ __device__ constexpr size_t bwd_stream_smem(int nt) {
-    return (size_t)nt * sizeof(PixRec<T, false>) +
-           (size_t)(nt / 32) * kBwdRing * (sizeof(Rec<T>) + sizeof(int32_t));
-}
-
-template <typename T>
-__device__ __forceinline__ void bwd_tile_stream(const TileCtx &tc, int tile,
-                                                const int32_t *__restrict__ ids,
-                                                const int2 *__restrict__ tile_bins,
-                                                const Rec<T> *__restrict__ recs,
-                                                const int32_t *__restrict__ final_idx,
-                                                CotSrc<T> cot, T clamp, T *__restrict__ packed) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int nt = blockDim.x;
-    const unsigned FULL = 0xffffffffu;
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    PixRec<T, false> *my_pix = reinterpret_cast<PixRec<T, false> *>(smem_raw) + w * 32;
-    Rec<T> *ring = reinterpret_cast<Rec<T> *>(reinterpret_cast<PixRec<T, false> *>(smem_raw) +
-                                              nt) + w * kBwdRing;
-    int32_t *ring_id = reinterpret_cast<int32_t *>(
-                           reinterpret_cast<Rec<T> *>(reinterpret_cast<PixRec<T, false> *>(
-                                                          smem_raw) + nt) + (nt / 32) * kBwdRing) +
-                       w * kBwdRing;
-    if (tc.empty) return;  // gradients stay zero (rasterize.py:156-161)
-    const int B = tc.B, H = tc.H, W = tc.W, tx0 = tc.tx0, ty0 = tc.ty0;
-    cot.scale = (T)(2.0 / (3.0 * (double)H * (double)W));
-    const Regions R = Regions::make(0, B);
-
-    int w_end;
-    {  // stage this lane's pixel (region w, slot lane)
-        int lx, ly;
-        R.pixel(w, lane, 0, lx, ly);
-        const int gx = tx0 + lx, gy = ty0 + ly;
-        const bool inside = lx < B && ly < B && gx < W && gy < H;
-        const int p = inside ? tc.poff + gy * W + gx : 0;
-        PixRec<T, false> c;
-        c.px = (T)gx + (T)0.5;
-        c.py = (T)gy + (T)0.5;
-        c.vo0 = c.vo1 = c.vo2 = c.vw = (T)0;
-        if (inside) cot.get(p, c.vo0, c.vo1, c.vo2, c.vw);
-        c.fin = inside ? final_idx[p] : -1;
-        c.vd[0] = (T)0;
-        __syncwarp();  // the previous tile's readers of my_pix are done
-        my_pix[lane] = c;
-        w_end = c.fin;
-#pragma unroll
-        for (int o = 16; o >= 1; o >>= 1) w_end = max(w_end, __shfl_xor_sync(FULL, w_end, o));
-        __syncwarp();
-    }
-    const int2 range = tile_bins[tile];
-    const int end = min(range.y, w_end + 1);
-    const T px_base = (T)(tx0 + (w % R.nbx) * 8) + (T)0.5;
-    const T py0 = (T)(ty0 + (w / R.nbx) * 4) + (T)0.5;
-
-    // one group of `left` (<= 32) queued Gaussians from ring[head ...]
-    auto group = [&](int head, int left) {
-        const int lsplit = !LIG_RASTER_BWD_SPLIT ? 0 : left <= 4 ? 3 : left <= 8 ? 2
-                                                     : left <= 16 ? 1 : 0;
-        const int gi = lane >> lsplit, part = lane & ((1 << lsplit) - 1);
-        const bool act = gi < left;
-        const int slot = (head + (act ? gi : 0)) & (kBwdRing - 1);
-        const Rec<T> g = ring[slot];
-        T acc[11];
-#pragma unroll
-        for (int q = 0; q < 11; ++q) acc[q] = 0;
-        const T px0 = px_base + (T)part;
-        if (act) {
-            switch (lsplit) {
-            case 0: lean_region<T, 0>(g, clamp, my_pix, part, px0, py0, acc); break;
-            case 1: lean_region<T, 1>(g, clamp, my_pix, part, px0, py0, acc); break;
-            case 2: lean_region<T, 2>(g, clamp, my_pix, part, px0, py0, acc); break;
-            default: lean_region<T, 3>(g, clamp, my_pix, part, px0, py0, acc); break;
-            }
-        }
-        for (int o = 1; o < (1 << lsplit); o <<= 1) {  // combine the lane group
-#pragma unroll
-            for (int q = 0; q < 11; ++q) {
-                if (q == 2 || q == 3 || q == 10) continue;
-                acc[q] += __shfl_xor_sync(FULL, acc[q], o);
-            }
-        }
-        if (act && part == 0) {
-            // v_xy = (a Sx + b Sy, b Sx + c Sy); v_conic = (Sxx/2, Sxy, Syy/2)
-            const T sx = acc[0], sy = acc[1];
-            T *dst = packed + (size_t)ring_id[slot] * 8;
-            const T v[8] = {g.a * sx + g.b * sy, g.b * sx + g.c * sy, (T)0.5 * acc[4], acc[5],
-                            (T)0.5 * acc[6], acc[7], acc[8], acc[9]};
-            if constexpr (sizeof(T) == 4) {
-                float4 *d4 = reinterpret_cast<float4 *>(dst);
-                atomicAdd(d4, make_float4(v[0], v[1], v[2], v[3]));
-                atomicAdd(d4 + 1, make_float4(v[4], v[5], v[6], v[7]));
-            } else {
-#pragma unroll
-                for (int q = 0; q < 8; ++q) atomicAdd(dst + q, v[q]);
-            }
-        }
-    };
-
-    int head = 0, qn = 0;  // ring state (warp-uniform)
-    Rec<T> pre;
-    int pre_id = -1;
-    if (range.x + lane < end) {
-        pre_id = __ldg(ids + range.x + lane);
-        pre = recs[pre_id];
-    }
-    for (int base = range.x; base < end; base += 32) {
-        const bool hit = base + lane < end && region_hit<T, true, false>(pre, R, w, tx0, ty0);
-        const uint32_t mask = __ballot_sync(FULL, hit);
-        if (hit) {
-            const int pos = (head + qn + __popc(mask & ((1u << lane) - 1u))) & (kBwdRing - 1);
-            ring[pos] = pre;
-            ring_id[pos] = pre_id;
-        }
-        qn += __popc(mask);
-        if (base + 32 + lane < end) {
-            pre_id = __ldg(ids + base + 32 + lane);
-            pre = recs[pre_id];
-        }
-        __syncwarp();
-        if (qn >= 32) {
-            group(head, 32);
-            __syncwarp();  // the group's ring slots are read before they are refilled
-            head = (head + 32) & (kBwdRing - 1);
-            qn -= 32;
-        }
-    }
-    if (qn > 0) group(head, qn);
-}
-
-template <typename T, bool GA, bool LEAN, int MAXT, int MINB, bool STREAM = false>
+template <typename T, bool GA, bool LEAN, int MAXT, int MINB>
 __global__ void __launch_bounds__(MAXT, MINB)
 raster_bwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work,
                   const int32_t *__restrict__ ids, const int2 *__restrict__ tile_bins,
@@ -1364,11 +1222,8 @@ raster_bwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work
     for (int tile = next_tile(work, s_slot, true); tile < n_tiles;
          tile = next_tile(work, s_slot, false)) {
         const TileCtx tc = tile_ctx(geo, cum, d_total, tile);
-        if constexpr (STREAM)
-            bwd_tile_stream<T>(tc, tile, ids, tile_bins, recs, final_idx, cot, clamp, packed);
-        else
-            bwd_tile<T, GA, LEAN>(tc, tile, ids, tile_bins, recs, final_idx, cot, v_dx, v_dy,
-                                  v_dxy, clamp, packed, s_end);
+        bwd_tile<T, GA, LEAN>(tc, tile, ids, tile_bins, recs, final_idx, cot, v_dx, v_dy, v_dxy,
+                              clamp, packed, s_end);
     }
 }
 
@@ -1571,19 +1426,14 @@ int raster_bwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
     const int nt = 32 * Regions::make(ga ? 2 : 0, geo.B).count;
     const int nw = nt / 32;
     const size_t pix = ga ? sizeof(PixRec<T, true>) : sizeof(PixRec<T, false>);
-    // (the per-warp rings of 32-wide fp64 tiles would not fit in shared memory)
-    const bool stream = lean && LIG_RASTER_BWD_STREAM && bwd_stream_smem<T>(nt) <= 160 * 1024;
-    const size_t sm = stream ? bwd_stream_smem<T>(nt)
-                             : (size_t)nt * pix + (size_t)nt * (sizeof(Rec<T>) + 2 * sizeof(uint32_t)) +
-                                   (size_t)nw * nt * sizeof(uint16_t);
+    const size_t sm = (size_t)nt * pix + (size_t)nt * (sizeof(Rec<T>) + 2 * sizeof(uint32_t)) +
+                      (size_t)nw * nt * sizeof(uint16_t);
     using K = void (*)(const BatchGeo, const int32_t *, int *, const int32_t *, const int2 *,
                        const int32_t *, const Rec<T> *, const int32_t *, CotSrc<T>, const T *,
                        const T *, const T *, T, T *);
     const bool small = nt <= 256;
     K fn = ga ? (small ? raster_bwd_kernel<T, true, false, 256, LIG_RASTER_BWD_MINB>
                        : raster_bwd_kernel<T, true, false, 1024, 1>)
-              : stream ? (small ? raster_bwd_kernel<T, false, true, 256, LIG_RASTER_BWD_LEAN_MINB, true>
-                                : raster_bwd_kernel<T, false, true, 1024, 1, true>)
               : lean ? (small ? raster_bwd_kernel<T, false, true, 256, LIG_RASTER_BWD_LEAN_MINB>
                               : raster_bwd_kernel<T, false, true, 1024, 1>)
                      : (small ? raster_bwd_kernel<T, false, false, 256, LIG_RASTER_BWD_MINB>
