@@ -37,10 +37,12 @@
 
 namespace lig {
 
+// The fields every evaluation reads come first (two 16-byte loads); opacity
+// and the cull data, read at staging or only with opacities, last.
 template <typename T> struct alignas(16) Rec {
-    T x, y, a, b;     // mean, conic (a, b)
-    T c, o, wx, wy;   // conic c, opacity, cull half-widths (negative: never cull)
-    T r, g, bl, thr;  // colour, cull threshold on sigma
+    T x, y, a, b;      // mean, conic (a, b)
+    T c, r, g, bl;     // conic c, colour
+    T o, wx, wy, thr;  // opacity, cull half-widths (negative: never cull), sigma threshold
 };
 
 // ------------------------------------------------------------------ pack
