@@ -33,6 +33,7 @@ from __future__ import annotations
 
 import ctypes
 import json
+import collections
 import math
 import os
 from dataclasses import dataclass
@@ -388,14 +389,24 @@ class BatchedFit:
             for _ in range(self._recover()):
                 self.step(target)
 
-    def fit(self, iters: int) -> BatchStats:
+    def fit(self, iters: int, max_ahead: Optional[int] = None) -> BatchStats:
         """Run until `iters` Adam steps have been applied (skipped steps are
-        redone after the capacity grows)."""
+        redone after the capacity grows).  max_ahead: enqueue at most this
+        many iterations ahead of the device (the host waits on an event,
+        without the GIL), so that other threads' launches on the device —
+        a server's renders — never queue behind a long chunk of fit work."""
         applied = 0
+        pending = collections.deque()
         while True:
             while applied < iters:
                 self.step()
                 applied += 1
+                if max_ahead:
+                    ev = torch.cuda.Event()
+                    ev.record(torch.cuda.current_stream(self.dev))
+                    pending.append(ev)
+                    if len(pending) > max_ahead:
+                        pending.popleft().synchronize()
                 if int(self.host_skipped[0]) > 0:  # pinned copy, no sync
                     applied -= self._recover()
             torch.cuda.current_stream(self.dev).synchronize()

@@ -273,7 +273,10 @@ __global__ void radix_upsweep_kernel(const uint32_t *__restrict__ keys, const in
 // (consecutive threads -> consecutive output positions of one digit).
 // Shared layout: wcnt[kSortWarps][bins] | bofs[bins] | gbase[bins] |
 //                skeys[4096] | svals[4096].
-__global__ void __launch_bounds__(kSortThreads)
+#ifndef LIG_SORT_MINB
+#define LIG_SORT_MINB 4  // resident downsweep blocks per SM asked of the register allocator
+#endif
+__global__ void __launch_bounds__(kSortThreads, LIG_SORT_MINB)
 radix_downsweep_kernel(const uint32_t *__restrict__ keys_in, const int32_t *__restrict__ vals_in,
                        uint32_t *__restrict__ keys_out, int32_t *__restrict__ vals_out,
                        const int32_t *d_total, int capacity, int shift, int bins,
@@ -295,16 +298,16 @@ radix_downsweep_kernel(const uint32_t *__restrict__ keys_in, const int32_t *__re
         gbase[i] = hist_scan[(int64_t)i * nblk + blockIdx.x];
     __syncthreads();
 
+    // keys in registers; ranks (< 4096) two per register; the values are
+    // read again at the scatter (a small register footprint keeps more
+    // blocks resident)
     uint32_t k[kSortRounds];
-    int32_t v[kSortRounds];
-    uint32_t rk[kSortRounds];
+    uint32_t rk2[kSortRounds / 2];
     int64_t wbase = base + warp * kWarpSeg;
 #pragma unroll
     for (int r = 0; r < kSortRounds; ++r) {
         int64_t i = wbase + r * 32 + lane;
-        bool ok = i < m;
-        k[r] = ok ? keys_in[i] : 0u;
-        v[r] = ok ? vals_in[i] : 0;
+        k[r] = i < m ? keys_in[i] : 0u;
     }
     uint32_t lt_mask = (1u << lane) - 1u;
     uint32_t *my = wcnt + warp * bins;
@@ -319,7 +322,9 @@ radix_downsweep_kernel(const uint32_t *__restrict__ keys_in, const int32_t *__re
         __syncwarp();
         if (ok && before == 0) my[d] = old + __popc(peers);
         __syncwarp();
-        rk[r] = old + before;
+        const uint32_t rank = old + before;
+        if (r & 1) rk2[r >> 1] |= rank << 16;
+        else rk2[r >> 1] = rank;
     }
     __syncthreads();
     // exclusive prefix over warps per digit; block digit totals into bofs
@@ -361,9 +366,9 @@ radix_downsweep_kernel(const uint32_t *__restrict__ keys_in, const int32_t *__re
         int64_t i = wbase + r * 32 + lane;
         if (i < m) {
             uint32_t d = (k[r] >> shift) & (uint32_t)(bins - 1);
-            uint32_t pos = bofs[d] + wcnt[warp * bins + d] + rk[r];
+            uint32_t pos = bofs[d] + wcnt[warp * bins + d] + ((rk2[r >> 1] >> (16 * (r & 1))) & 0xffffu);
             skeys[pos] = k[r];
-            svals[pos] = v[r];
+            svals[pos] = vals_in[i];
         }
     }
     __syncthreads();

@@ -178,11 +178,14 @@ class Server:
     """Render + fit server on one GPU (see module docstring).
 
     budget_bytes: HBM budget for admission; max_fit_batch: images per batched
-    fit (<= 64); fit_chunk: iterations between batch changes."""
+    fit (<= 64); fit_chunk: iterations between batch changes; fit_ahead: fit
+    iterations the fit worker may have queued on the device at once (a
+    deeper queue makes a render's launches wait behind it)."""
 
     def __init__(self, budget_bytes: int = 150 * 10**9, device="cuda", block: int = 16,
                  max_fit_batch: int = 64, fit_chunk: int = 20, fit_graph: bool = True,
-                 reserve_fit_bytes: int = 0, reserve_render_bytes: int = 0):
+                 reserve_fit_bytes: int = 0, reserve_render_bytes: int = 0,
+                 fit_ahead: int = 2):
         dev = torch.device(device)
         if dev.type == "cuda" and dev.index is None:
             dev = torch.device("cuda", torch.cuda.current_device())
@@ -191,6 +194,7 @@ class Server:
         self.max_fit_batch = max_fit_batch
         self.fit_chunk = fit_chunk
         self.fit_graph = fit_graph
+        self.fit_ahead = fit_ahead
         self.budget = MemoryBudget(budget_bytes)
         # lower is higher priority; out-of-range values map to the extremes
         self.render_stream = torch.cuda.Stream(self.dev, priority=-16)
@@ -390,7 +394,7 @@ class Server:
                         self.fit_phases.append((t0, time.perf_counter(), "build"))
                     k = min(self.fit_chunk, min(j.req.iters - j.done for j in batch_jobs))
                     t0 = time.perf_counter()
-                    batch.fit(k)
+                    batch.fit(k, max_ahead=self.fit_ahead)
                     self.fit_phases.append((t0, time.perf_counter(), "iterate"))
                 except Exception as e:  # fail this batch's jobs, keep serving
                     for j in active:
@@ -486,18 +490,30 @@ def poisson_requests(duration_s: float, rate: float, fit_frac: float, sets: Dict
                                       "origin": (ox, oy)}))
 
 
-def warm_up(server: Server, sides=(256, 1024, 2048, 4096), scales=(0.25, 1.0, 2.0)):
+def warm_up(server: Server, sides=(256, 1024, 2048, 4096), scales=(0.25, 1.0, 2.0),
+            fit_side: int = 1024, fit_points: int = 50_000):
     """Render a few views of each resident set's kind at several output sizes
-    and scales on the render stream, so the first requests do not pay for
-    first-use costs (kernel loading, tile-count-dependent sort set-up,
-    allocator growth)."""
+    and scales on the render stream, and run a small batched fit (through its
+    CUDA-graph capture) on the fit stream, so the first requests do not pay
+    for first-use costs (kernel loading, tile-count-dependent sort set-up,
+    the first graph capture, pinned staging words, allocator growth) while
+    other requests are in flight."""
     gs = next(iter(server.sets.values()), None)
-    if gs is None:
-        return
-    with torch.cuda.stream(server.render_stream):
-        for side in sides:
-            for s in scales:
-                render_view(gs, side, side, (0.0, 0.0), (s, s), server.block)
+    if gs is not None:
+        with torch.cuda.stream(server.render_stream):
+            for side in sides:
+                for s in scales:
+                    render_view(gs, side, side, (0.0, 0.0), (s, s), server.block)
+    if fit_side > 0:
+        with torch.cuda.stream(server.fit_stream):
+            g = torch.Generator(device=server.dev).manual_seed(1)
+            target = torch.rand(fit_side, fit_side, 3, generator=g, device=server.dev)
+            init = FitState(synthetic.gaussians_on_device(fit_points, fit_side, fit_side,
+                                                          server.dev, seed=2))
+            fit = BatchedFit([target], [fit_points], block=server.block, lr=1e-3, init=[init],
+                             graph=server.fit_graph)
+            fit.fit(4, max_ahead=server.fit_ahead)
+            del fit, target, init
     torch.cuda.synchronize(server.dev)
 
 

@@ -45,6 +45,8 @@ def main():
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--sets", type=int, default=64)
     ap.add_argument("--fit-chunk", type=int, default=20)
+    ap.add_argument("--fit-ahead", type=int, default=2,
+                    help="fit iterations queued on the device at most (0: a whole chunk)")
     ap.add_argument("--no-fit-graph", action="store_true")
     ap.add_argument("--reserve-fit-gb", type=float, default=60.0)
     ap.add_argument("--reserve-render-gb", type=float, default=8.0)
@@ -58,7 +60,7 @@ def main():
                                 seed=5000)
     srv = Server(budget_bytes=int(a.budget_gb * 1e9), fit_chunk=a.fit_chunk,
                  fit_graph=not a.no_fit_graph, reserve_fit_bytes=int(a.reserve_fit_gb * 1e9),
-                 reserve_render_bytes=int(a.reserve_render_gb * 1e9))
+                 reserve_render_bytes=int(a.reserve_render_gb * 1e9), fit_ahead=a.fit_ahead)
     for k, gs in sets.items():
         srv.add_set(k, gs)
     # start the workers and warm the render path before the clock starts
@@ -82,7 +84,7 @@ def main():
                                          ("device", st.render_device_ms))},
         "fit_s": {"p50": percentile(f, 50), "p99": percentile(f, 99), "n": len(f)},
         "throughput_per_s": {"render": len(r) / st.wall_s, "fit": len(f) / st.wall_s},
-        "slow_render_fit_phases": st.slow_render_phases,
+        "slow_render_fit_phases": st.slow_render_phases, "fit_ahead": a.fit_ahead,
         "fit_phase_s": {ph: round(sum(b - a for a, b, p in srv.fit_phases if p == ph), 2)
                         for ph in ("build", "iterate", "finish")},
         "fit_batches": srv.fit_batches, "budget_peak_gb": srv.budget.peak / 1e9,

@@ -101,3 +101,22 @@ def test_unknown_set_is_an_error_result():
     assert srv.drain(timeout=60)
     srv.stop()
     assert srv.results[rid].error and "nope" in srv.results[rid].error
+
+
+def test_warm_up_then_serve():
+    """warm_up (renders and a small fit through its graph capture, before
+    the clock) leaves the server serving normally."""
+    from lig_b200.serve import warm_up
+    sets = {"a": _set(1500, 128, 54)}
+    srv = Server()
+    for k, gs in sets.items():
+        srv.add_set(k, gs)
+    srv.start()
+    warm_up(srv, sides=(64, 96), scales=(1.0,), fit_side=96, fit_points=600)
+    req = RenderRequest("a", 80, 72, (5.0, 9.0), 1.25)
+    rid = srv.submit(req)
+    assert srv.drain(timeout=120)
+    srv.stop()
+    assert not srv.errors, srv.errors
+    alone, _ = _serve([req], sets)
+    assert torch.equal(srv.results[rid].output, alone[0].output)
