@@ -303,6 +303,9 @@ __device__ __forceinline__ int next_tile(int *work, int &s_slot, bool first) {
 #ifndef LIG_RASTER_FWD_ELLIPSE
 #define LIG_RASTER_FWD_ELLIPSE 1  // sum forward: exact ellipse test per region
 #endif
+#ifndef LIG_RASTER_FWD_ELLIPSE_GA
+#define LIG_RASTER_FWD_ELLIPSE_GA 1  // the same in the gradient-aware forward
+#endif
 #ifndef LIG_RASTER_FWD_FUSED
 #define LIG_RASTER_FWD_FUSED 1  // specialised fused-loss forward (no opacities)
 #endif
@@ -495,9 +498,9 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
     const int B = tc.B, tx0 = tc.tx0, ty0 = tc.ty0;
     static_assert(PPL == 1 || PPL == 2 || PPL == 4, "one, two or four pixels per lane");
     const Regions R = Regions::make(PPL == 1 ? 0 : (PPL == 2 ? 1 : 3), B);
-    // sum forward: a warp lists only the Gaussians whose alpha >= 1/255
-    // ellipse meets its region (one test per Gaussian and region, staged)
-    constexpr bool ELL = !GA && LIG_RASTER_FWD_ELLIPSE;
+    // a warp lists only the Gaussians whose alpha >= 1/255 ellipse meets
+    // its region (one test per Gaussian and region)
+    constexpr bool ELL = LIG_RASTER_FWD_ELLIPSE && (!GA || LIG_RASTER_FWD_ELLIPSE_GA);
     bool inside[PPL];
     int pix[PPL];
     T px[PPL], py[PPL];
