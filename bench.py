@@ -181,11 +181,39 @@ def evaluations(fit) -> tuple[int, int]:
 
 
 # -------------------------------------------------------------- CPU side
+def _synthetic_module():
+    """lig_b200/synthetic.py (the seeded draws; torch only) loaded by path:
+    importing it through the package would load the CUDA library, which the
+    CPU reference arm must not touch."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "lig_synthetic_draws", os.path.join(ROOT, "lig_b200", "synthetic.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _adam_np(params, grads, state, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8):
+    """torch.optim.Adam's update (the GPU step's optimiser) on float32 arrays."""
+    state["t"] = state.get("t", 0) + 1
+    t = state["t"]
+    for i, (p, g) in enumerate(zip(params, grads)):
+        m = state.setdefault(("m", i), np.zeros_like(p))
+        v = state.setdefault(("v", i), np.zeros_like(p))
+        m *= b1
+        m += (1 - b1) * g
+        v *= b2
+        v += (1 - b2) * g * g
+        mhat = m / (1 - b1 ** t)
+        vhat = v / (1 - b2 ** t)
+        p -= (lr * mhat / (np.sqrt(vhat) + eps)).astype(np.float32)
+
+
 def cpu_band_sample(size, n, target_secs, steps, diag=DIAG):
     """Time the oracle (C restatement, OpenMP) on horizontal bands of the
     workload; returns (iters/s for the full image, cores, description)."""
-    from lig_b200 import synthetic
     from oracle import oracle as O
+    synthetic = _synthetic_module()
     cores = os.cpu_count() or 1
     means, chol, colors = synthetic.gaussians(n, size, size, diag=diag, seed=synthetic.SEED_INIT)
     means, chol, colors = means.numpy(), chol.numpy(), colors.numpy()
@@ -195,6 +223,7 @@ def cpu_band_sample(size, n, target_secs, steps, diag=DIAG):
         sel = (means[:, 1] >= -32) & (means[:, 1] < rows + 32)
         m, L, c = means[sel], chol[sel], colors[sel]
         tgt = rng.uniform(0, 1, (rows, size, 3)).astype(np.float32)
+        state = {}
         t0 = time.perf_counter()
         xys, ext, con, cnt = O.project_fwd(L, m, None, rows, size, BLOCK, chol=True)
         bn = O.bin_and_sort(xys, ext, cnt, rows, size, BLOCK)
@@ -203,7 +232,8 @@ def cpu_band_sample(size, n, target_secs, steps, diag=DIAG):
         v_img = (2.0 / img.size) * (np.clip(img, 0, 1) - tgt) * ((img >= 0) & (img <= 1))
         g = O.raster_bwd(rows, size, BLOCK, bn, xys, con, c, None, out["final_idx"],
                          v_img.astype(np.float32), np.zeros((rows, size), np.float32))
-        O.project_bwd(ext, L, con, g["v_xy"], g["v_conic"], chol=True)
+        v_L, v_m = O.project_bwd(ext, L, con, g["v_xy"], g["v_conic"], chol=True)
+        _adam_np([c, m, L], [g["v_rgb"], v_m, v_L], state)
         return time.perf_counter() - t0
 
     probe_rows = max(BLOCK, (size // 64) // BLOCK * BLOCK)
@@ -214,7 +244,7 @@ def cpu_band_sample(size, n, target_secs, steps, diag=DIAG):
     t = statistics.median(times)
     full_secs = t * size / rows
     desc = (f"{rows}x{size} band of the {size}^2 level-2 fit step (Gaussians with centres in "
-            f"the band +-32 px), project+bin+raster fwd+L2 grad+raster bwd+proj bwd, "
+            f"the band +-32 px), project+bin+raster fwd+L2 grad+raster bwd+proj bwd+Adam, "
             f"fp32, scaled by {size / rows:.2f} to the full image; median of {steps}")
     return 1.0 / full_secs, cores, desc, times, rows
 

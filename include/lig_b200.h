@@ -224,9 +224,9 @@ int lig_l2_clamped_loss(int dtype, int64_t n, const void *img, const void *targe
  * lig_raster_fwd with out_dx/out_dy/out_dxy = NULL.  Returns
  * LIG_ERR_TOO_LARGE when num_points > LIG_STATIC_MAX_POINTS.  The first call
  * on a device looks up the array's device address, so make it before any
- * stream capture.  All calls on a device share the array (each call rewrites
- * the records it uses): calls that overlap on that GPU, e.g. on two streams,
- * race. */
+ * stream capture (after a device reset the next call looks it up again).
+ * All calls on a device share the array (each call rewrites the records it
+ * uses): calls that overlap on that GPU, e.g. on two streams, race. */
 #define LIG_STATIC_MAX_POINTS 131072
 int lig_raster_fwd_noalloc(int img_h, int img_w, int block_width, int num_points,
                            const int32_t *gaussian_ids_sorted, const int32_t *tile_bins,

@@ -34,6 +34,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "pair.cuh"
 
 namespace lig {
 
@@ -912,6 +913,82 @@ __device__ __forceinline__ void lean_region(const Rec<T> &g, T clamp,
     acc[7] = c0; acc[8] = c1; acc[9] = c2;
 }
 
+#ifndef LIG_RASTER_BWD_F2
+#define LIG_RASTER_BWD_F2 1  // lean backward (float): pixel pairs in f32x2 arithmetic
+#endif
+
+// The lean backward's pixel cotangents in pair layout: region entry
+// row * 4 + cp holds columns cp and cp + 4 of that row, channel by channel,
+// so one 16-byte and one 8-byte load give three ready (column cp, cp + 4)
+// pairs.
+struct alignas(16) PixPair {
+    float v[8];  // v0 (cp, cp+4), v1 (cp, cp+4), v2 (cp, cp+4), unused
+};
+
+// lean_region in f32x2 form (float): the lane takes NCP column pairs
+// c0, c0 + CSTEP, ... (columns cp and cp + 4 of each) in NR rows r0.. of the
+// 8x4 region, and evaluates the two pixels of a pair with one packed
+// operation where lean_region uses two.  Per pixel the operations and their
+// roundings are lean_region's — sigma = fma(b dx, dy, fma((a/2) dx, dx,
+// ((c/2) dy) dy)), alpha = min(clamp, exp(-sigma)) and the same alpha test —
+// so the alpha decisions are bit-identical; only the order in which the
+// moment and colour sums are added differs.  Same outputs in acc[].
+template <int NCP, int CSTEP, int NR>
+__device__ __forceinline__ void lean_region_f2(const Rec<float> &g, float clamp,
+                                               const PixPair *__restrict__ pp, int c0, int r0,
+                                               float px0, float py0, float (&acc)[11]) {
+    const float ha = 0.5f * g.a, hc = 0.5f * g.c;
+    const f2 HA = f2_dup(ha), BB = f2_dup(g.b);
+    const f2 CR = f2_dup(g.r), CG = f2_dup(g.g), CB = f2_dup(g.bl);
+    f2 DY[NR], CDD[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        const float dy = g.y - (py0 + (float)(r0 + r));
+        DY[r] = f2_dup(dy);
+        CDD[r] = f2_dup(__fmul_rn(__fmul_rn(hc, dy), dy));
+    }
+    f2 sx = f2_zero(), sy = f2_zero(), sxx = f2_zero(), sxy = f2_zero(), syy = f2_zero();
+    f2 sr = f2_zero(), sg = f2_zero(), sb = f2_zero();
+#pragma unroll
+    for (int k = 0; k < NCP; ++k) {
+        const int cp = c0 + k * CSTEP;
+        const f2 DX = f2_pack(g.x - (px0 + (float)cp), g.x - (px0 + (float)(cp + 4)));
+        const f2 HADX = f2_mul(HA, DX), BDX = f2_mul(BB, DX);
+        f2 wc = f2_zero(), yc = f2_zero();
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            const PixPair *e = pp + (r0 + r) * 4 + cp;
+            const ulonglong2 v01 = *reinterpret_cast<const ulonglong2 *>(e->v);
+            const f2 V0{v01.x}, V1{v01.y};
+            const f2 V2{*reinterpret_cast<const unsigned long long *>(e->v + 4)};
+            const f2 S = f2_fma(BDX, DY[r], f2_fma(HADX, DX, CDD[r]));
+            float s0, s1;
+            f2_unpack(S, s0, s1);
+            const float al0 = fminf(clamp, __expf(-s0)), al1 = fminf(clamp, __expf(-s1));
+            const float a0 = (s0 < 0.f || al0 < 1.f / 255.f) ? 0.f : al0;
+            const float a1 = (s1 < 0.f || al1 < 1.f / 255.f) ? 0.f : al1;
+            const f2 A = f2_pack(a0, a1);
+            sr = f2_fma(A, V0, sr);
+            sg = f2_fma(A, V1, sg);
+            sb = f2_fma(A, V2, sb);
+            // -v_sigma per pixel
+            const f2 WV = f2_mul(A, f2_fma(CB, V2, f2_fma(CG, V1, f2_mul(CR, V0))));
+            wc = f2_add(wc, WV);
+            const f2 TY = f2_mul(WV, DY[r]);
+            yc = f2_add(yc, TY);
+            syy = f2_fma(TY, DY[r], syy);
+        }
+        const f2 TX = f2_mul(wc, DX);
+        sx = f2_add(sx, TX);
+        sxx = f2_fma(TX, DX, sxx);
+        sy = f2_add(sy, yc);
+        sxy = f2_fma(yc, DX, sxy);
+    }
+    acc[0] = -f2_sum(sx); acc[1] = -f2_sum(sy);
+    acc[4] = -f2_sum(sxx); acc[5] = -f2_sum(sxy); acc[6] = -f2_sum(syy);
+    acc[7] = f2_sum(sr); acc[8] = f2_sum(sg); acc[9] = f2_sum(sb);
+}
+
 // LEAN (sum backward of the fused fit loss, no opacities, no wsum
 // cotangent): only the gradients the fit needs — v_xy, v_conic, v_rgb — are
 // accumulated (no |v_xy| sums, no opacity gradient) and each (Gaussian,
@@ -926,6 +1003,8 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
                                          const T *__restrict__ v_dxy, T clamp,
                                          T *__restrict__ packed, int &s_end) {
     using M = Math<T>;
+    // float lean backward: pixel pairs in f32x2 arithmetic (lean_region_f2)
+    constexpr bool kPairs = LEAN && !GA && LIG_RASTER_BWD_F2 && sizeof(T) == 4;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nt = blockDim.x;  // = 32 * regions: region-major pixel slots
     PixRec<T, GA> *s_pix = reinterpret_cast<PixRec<T, GA> *>(smem_raw);
@@ -967,7 +1046,18 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
                 c.vd[6 + ch] = inside ? v_dxy[3 * p + ch] : (T)0;
             }
         }
-        s_pix[tid] = c;
+        if constexpr (kPairs) {
+            // region w's pair entries: (row, column) -> entry row * 4 + col % 4,
+            // half col / 4 (the pixel slots are row-major 8x4, kind 0)
+            PixPair *e = reinterpret_cast<PixPair *>(smem_raw) + w * 16 + (lane >> 3) * 4 +
+                         (lane & 3);
+            const int h = (lane >> 2) & 1;
+            e->v[h] = c.vo0;
+            e->v[2 + h] = c.vo1;
+            e->v[4 + h] = c.vo2;
+        } else {
+            s_pix[tid] = c;
+        }
         int my_max = c.fin;
 #pragma unroll
         for (int o = 16; o >= 1; o >>= 1) my_max = max(my_max, __shfl_xor_sync(FULL, my_max, o));
@@ -1036,7 +1126,26 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
 #pragma unroll
             for (int q = 0; q < 11; ++q) acc[q] = 0;
             bool touched = false;
-            if constexpr (LEAN && !GA && LIG_RASTER_BWD_COLS) {
+            if constexpr (kPairs) {
+                // as below, two pixels per packed operation: lanes of a group
+                // take column pairs (1 / 2 / 4 lanes) or column pairs and row
+                // halves (8 lanes)
+                touched = act;
+                const float px0 = (float)(tx0 + (w % R.nbx) * 8) + 0.5f;
+                const float py0 = (float)(ty0 + (w / R.nbx) * 4) + 0.5f;
+                const PixPair *pp = reinterpret_cast<const PixPair *>(smem_raw) + w * 16;
+                if (act) {
+                    switch (lsplit) {
+                    case 0: lean_region_f2<4, 1, 4>(g, clamp, pp, 0, 0, px0, py0, acc); break;
+                    case 1: lean_region_f2<2, 2, 4>(g, clamp, pp, part, 0, px0, py0, acc); break;
+                    case 2: lean_region_f2<1, 1, 4>(g, clamp, pp, part, 0, px0, py0, acc); break;
+                    default:
+                        lean_region_f2<1, 1, 2>(g, clamp, pp, part & 3, 2 * (part >> 2), px0,
+                                                py0, acc);
+                        break;
+                    }
+                }
+            } else if constexpr (LEAN && !GA && LIG_RASTER_BWD_COLS) {
                 // every listed (Gaussian, region) pair met the region's
                 // ellipse test; an untouched one adds zeros
                 touched = act;
@@ -1588,7 +1697,11 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[(size_t)LIG_STATIC_MAX
 
 // Device address of the scratch array, looked up once per device (host code
 // cannot use the symbol itself: on the host it names a stand-in, not device
-// memory).  The first call on a device does the lookup.
+// memory).  The first call on a device does the lookup.  A device reset by
+// the host application (cudaDeviceReset) ends the context the address
+// belongs to: each call first checks, with a host-side pointer query, that
+// the cached address is still this device's memory, and looks it up again
+// when it is not.
 static void *noalloc_scratch_ptr(int &rc) {
     static std::mutex mu;
     static void *ptrs[128] = {};
@@ -1598,6 +1711,14 @@ static void *noalloc_scratch_ptr(int &rc) {
         return nullptr;
     }
     std::lock_guard<std::mutex> lock(mu);
+    if (ptrs[dev]) {
+        cudaPointerAttributes a{};
+        if (cudaPointerGetAttributes(&a, ptrs[dev]) != cudaSuccess ||
+            a.type != cudaMemoryTypeDevice || a.device != dev) {
+            (void)cudaGetLastError();  // the failed query must not reach the launch check
+            ptrs[dev] = nullptr;
+        }
+    }
     if (!ptrs[dev]) {
         void *p = nullptr;
         if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {

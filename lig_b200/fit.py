@@ -27,6 +27,9 @@ from .gsplat2d import gradient_aware_upscale, project_gaussians_cholesky, raster
 class LevelFit:
     """One LIG level: N Gaussians fitted to an [H, W, 3] target.
 
+    rgb_init "uniform" draws colours U(0,1) (the fit configurations);
+    "zeros" starts them at zero as gaussianlig.py:57 does.
+
     engine "graph" (default): the iteration runs as a one-image BatchedFit —
     fused-loss forward, backward from the masked difference, projection
     backward and the flat guarded Adam, captured as a CUDA graph (one per
@@ -37,13 +40,17 @@ class LevelFit:
 
     def __init__(self, n: int, H: int, W: int, device="cuda", lr: float = 1e-3, block: int = 16,
                  diag=(0.5, 6.0), seed: int = synthetic.SEED_INIT, fused_adam: bool = True,
-                 fused_loss: bool = True, engine: str = "graph"):
+                 fused_loss: bool = True, engine: str = "graph", rgb_init: str = "uniform"):
         if engine not in ("graph", "autograd"):
             raise ValueError("engine must be 'graph' or 'autograd'")
+        if rgb_init not in ("uniform", "zeros"):
+            raise ValueError("rgb_init must be 'uniform' or 'zeros'")
         self.H, self.W, self.block, self.lr = H, W, block, lr
         self.fused_loss = fused_loss
         self.engine = engine if fused_loss else "autograd"
         means, chol, colors = synthetic.gaussians(n, H, W, diag=diag, seed=seed)
+        if rgb_init == "zeros":  # gaussianlig.py:57 initialises colours to zero
+            colors = torch.zeros_like(colors)
         self.means = torch.nn.Parameter(means.to(device))
         self.chol = torch.nn.Parameter(chol.to(device))
         self.rgbs = torch.nn.Parameter(colors.to(device))
@@ -127,6 +134,7 @@ def downsample(gt_hwc: torch.Tensor, factor: int) -> torch.Tensor:
 class TwoLevelResult:
     psnr: float
     level_psnr: list = field(default_factory=list)
+    up_psnr: float = 0.0        # upscaled level-1 render alone vs the full-resolution target
     iters_per_s: list = field(default_factory=list)
     store_min: float = 0.0
     store_max: float = 0.0
@@ -134,7 +142,7 @@ class TwoLevelResult:
 
 def fit_two_level(gt_hwc: torch.Tensor, n1: int, n2: int, iters: int, lr: float = 1e-3,
                   factor: int = 4, diag=(0.5, 6.0), block: int = 16,
-                  log_every: Optional[int] = None) -> TwoLevelResult:
+                  log_every: Optional[int] = None, rgb_init: str = "uniform") -> TwoLevelResult:
     """The LIG level pipeline (train.py:93-158) with the gradient-aware upscale
     between levels: level 1 fits the factor-x downsampled image, its render is
     upscaled with gradient_aware_upscale, level 2 fits the min-max normalised
@@ -145,18 +153,19 @@ def fit_two_level(gt_hwc: torch.Tensor, n1: int, n2: int, iters: int, lr: float 
     res = TwoLevelResult(psnr=0.0)
     t1 = downsample(gt_hwc, factor)
     h1, w1 = t1.shape[:2]
-    lvl1 = LevelFit(n1, h1, w1, dev, lr=lr, block=block, diag=diag)
+    lvl1 = LevelFit(n1, h1, w1, dev, lr=lr, block=block, diag=diag, rgb_init=rgb_init)
     res.iters_per_s.append(_run(lvl1, t1, iters, log_every))
     with torch.no_grad():
         img, _, dx, dy, dxy = lvl1.render(grad_aware=True)
         res.level_psnr.append(psnr(torch.clamp(img, 0, 1), t1))
         up = gradient_aware_upscale(img, dx, dy, dxy, H, W)
+        res.up_psnr = psnr(torch.clamp(up, 0, 1), gt_hwc)
         resid = gt_hwc - up + 0.5
         lo, hi = resid.min(), resid.max()
         t2 = ((resid - lo) / (hi - lo)).contiguous()
     del lvl1
     lvl2 = LevelFit(n2, H, W, dev, lr=lr, block=block, diag=diag,
-                    seed=synthetic.SEED_INIT + 1)
+                    seed=synthetic.SEED_INIT + 1, rgb_init=rgb_init)
     res.iters_per_s.append(_run(lvl2, t2, iters, log_every))
     with torch.no_grad():
         r2 = torch.clamp(lvl2.render()[0], 0, 1)

@@ -8,8 +8,12 @@ This module serves both kinds of work at once:
 * **Render requests** decode a crop of a resident set at a scale: the view
   transform means' = (means - origin) * s, L' = s L is folded into the
   projection (lig_project_fwd_view), then binning and the forward rasterizer
-  produce the [h, w, 3] image in HBM.  They run on a high-priority CUDA
-  stream, so their thread blocks are scheduled ahead of queued fit blocks.
+  produce the [h, w, 3] image in HBM.  The renders queued when the render
+  worker is free are decoded together (continuous batching): one batched
+  binning and one batched forward launch for all of them (render_views),
+  each image identical to its own single render.  They run on a
+  high-priority CUDA stream, so their thread blocks are scheduled ahead of
+  queued fit blocks.
 * **Fit requests** (target image, Gaussian count, iterations) run on a
   low-priority stream as one BatchedFit over every admitted fit: jobs join
   and leave the batch between chunks of iterations (continuous batching);
@@ -34,8 +38,8 @@ from typing import Dict, List, Optional
 
 import torch
 
-from . import ops, synthetic
-from .batch import BatchedFit, FitState
+from . import _lib, ops, synthetic
+from .batch import BatchedFit, BatchLayout, FitState
 
 
 @dataclass
@@ -77,6 +81,70 @@ def render_view(gs: GaussianSet, out_h: int, out_w: int, origin=(0.0, 0.0), scal
         _, outs = ops.bin_gaussians(xys, ext, cnt, out_h, out_w, block, after_enqueue=enqueue)
     img, wsum, dx, dy, dxy, _ = outs
     return (img, wsum, dx, dy, dxy) if grad_aware else (img, wsum)
+
+
+def render_views(views, block: int = 16) -> List[torch.Tensor]:
+    """Decode several views in one launch chain per stage.
+
+    views: [(GaussianSet, out_h, out_w, origin, scale), ...] (at most
+    LIG_MAX_BATCH).  Each view is projected (lig_project_fwd_view) into its
+    slice of concatenated per-Gaussian arrays; one batched prefix sum,
+    binning (lig_bin_batch: a single stable sort, tile keys offset per view)
+    and forward (lig_raster_fwd_batch) then render every view.  A view's tile
+    lists are exactly its single-view lists, so each [out_h, out_w, 3] image
+    equals render_view's bit for bit.  Runs on the current stream; one host
+    synchronisation (the intersection count sizes the sort)."""
+    if not views:
+        return []
+    L = BatchLayout([v[1] for v in views], [v[2] for v in views], [v[0].n for v in views],
+                    block)
+    dev = views[0][0].means.device
+    N = L.points
+    f32 = dict(dtype=torch.float32, device=dev)
+    xys, ext = torch.empty(max(N, 1), 2, **f32), torch.empty(max(N, 1), 2, **f32)
+    con, rgbs = torch.empty(max(N, 1), 3, **f32), torch.empty(max(N, 1), 3, **f32)
+    cnt = torch.empty(max(N, 1), dtype=torch.int32, device=dev)
+    any_op = any(v[0].opacities is not None for v in views)
+    opac = torch.ones(max(N, 1), **f32) if any_op else None
+    st = ops._stream(dev)
+    p = ops._p
+    for k, (gs, h, w, origin, scale) in enumerate(views):
+        a, b = L.g_off[k], L.g_off[k + 1]
+        if b == a:
+            continue
+        # inputs held in locals: a converted copy must outlive the launch
+        o = None if gs.opacities is None else ops._c(gs.opacities, torch.float32)
+        in3, mu = ops._c(gs.chol, torch.float32), ops._c(gs.means, torch.float32)
+        ops.call("lig_project_fwd_view", _lib.LIG_F32, b - a, int(gs.cholesky), p(in3), p(mu),
+                 p(o), int(h), int(w), int(block), float(origin[0]), float(origin[1]),
+                 float(scale[0]), float(scale[1]), p(xys[a:b]), p(ext[a:b]), p(con[a:b]),
+                 p(cnt[a:b]), st)
+        rgbs[a:b].copy_(gs.rgbs)
+        if o is not None:
+            opac[a:b].copy_(o)
+    cum = torch.empty(max(N, 1), dtype=torch.int32, device=dev)
+    total = torch.zeros(1, dtype=torch.int32, device=dev)
+    if N > 0:
+        cws = torch.empty(_lib.lib.lig_cumsum_workspace_bytes(N), dtype=torch.uint8, device=dev)
+        ops.call("lig_cumsum_tiles", N, p(cnt), p(cum), p(total), p(cws), cws.numel(), st)
+    m = int(total.item())
+    cap = max(m, 1)
+    bws = torch.empty(max(_lib.lib.lig_bin_workspace_bytes(N, cap, L.tiles), 1),
+                      dtype=torch.uint8, device=dev)
+    gids = torch.empty(cap, dtype=torch.int32, device=dev)
+    bins = torch.empty(L.tiles, 2, dtype=torch.int32, device=dev)
+    status = torch.empty(1, dtype=torch.int32, device=dev)
+    ops.call("lig_bin_batch", _lib.LIG_F32, *L.args(), L.block, p(xys), p(ext), p(cum),
+             p(total), cap, p(bws), bws.numel(), p(gids), p(bins), p(status), st)
+    rws = torch.empty(_lib.lib.lig_raster_workspace_bytes(_lib.LIG_F32, N), dtype=torch.uint8,
+                      device=dev)
+    img = torch.empty(max(L.pixels, 1), 3, **f32)
+    wsum = torch.empty(max(L.pixels, 1), **f32)
+    fin = torch.empty(max(L.pixels, 1), dtype=torch.int32, device=dev)
+    ops.call("lig_raster_fwd_batch", _lib.LIG_F32, *L.args(), L.block, p(gids), p(bins),
+             p(total), p(cum), p(xys), p(con), p(rgbs), p(opac), 0, None, p(rws), rws.numel(),
+             p(img), p(wsum), None, None, None, p(fin), st)
+    return [L.image(img, k).clone() for k in range(L.n)]
 
 
 # ---------------------------------------------------------------- requests
@@ -146,13 +214,15 @@ class MemoryBudget:
 
 
 def render_bytes(gs: GaussianSet, out_h: int, out_w: int, block: int = 16) -> int:
-    """Upper estimate of a decode's device bytes: per-Gaussian projection and
-    record buffers, intersections (keys, ids, sort buffers) from the worst
-    tile coverage of a Gaussian of this set at this output size, outputs."""
+    """Upper estimate of a decode's device bytes: per-Gaussian projection,
+    colour / opacity copies of a batched decode and record buffers,
+    intersections (keys, ids, sort buffers) from the worst tile coverage of a
+    Gaussian of this set at this output size, outputs (and the batch
+    buffer's copy of them)."""
     n, p = gs.n, out_h * out_w
     tiles = ((out_w + block - 1) // block) * ((out_h + block - 1) // block)
     m = min(n * 16, n + 4 * tiles * 64)
-    return n * (36 + 48 + 8) + m * 20 + p * 20 + tiles * 8 + (1 << 20)
+    return n * (36 + 16 + 48 + 8) + m * 20 + p * 32 + tiles * 8 + (1 << 20)
 
 
 def fit_bytes(h: int, w: int, n: int, block: int = 16) -> int:
@@ -180,12 +250,15 @@ class Server:
     budget_bytes: HBM budget for admission; max_fit_batch: images per batched
     fit (<= 64); fit_chunk: iterations between batch changes; fit_ahead: fit
     iterations the fit worker may have queued on the device at once (a
-    deeper queue makes a render's launches wait behind it)."""
+    deeper queue makes a render's launches wait behind it);
+    max_render_batch / render_batch_pixels: most renders, and most output
+    pixels, decoded together in one batch."""
 
     def __init__(self, budget_bytes: int = 150 * 10**9, device="cuda", block: int = 16,
                  max_fit_batch: int = 64, fit_chunk: int = 20, fit_graph: bool = True,
                  reserve_fit_bytes: int = 0, reserve_render_bytes: int = 0,
-                 fit_ahead: int = 2):
+                 fit_ahead: int = 2, max_render_batch: int = 16,
+                 render_batch_pixels: int = 64 << 20):
         dev = torch.device(device)
         if dev.type == "cuda" and dev.index is None:
             dev = torch.device("cuda", torch.cuda.current_device())
@@ -209,6 +282,9 @@ class Server:
         self._abort = False
         self._threads: List[threading.Thread] = []
         self.fit_batches = 0
+        self.max_render_batch = max(1, min(int(max_render_batch), _lib.LIG_MAX_BATCH))
+        self.render_batch_pixels = int(render_batch_pixels)
+        self.render_batches: List[int] = []  # renders per decoded batch
         self.errors: List[str] = []
         # device memory taken into the allocator's cache per stream at start,
         # so the workers' allocations come from the cache: a large cudaMalloc
@@ -290,6 +366,29 @@ class Server:
             self._cv.notify_all()
 
     # -------------------------------------------------------------- renders
+    def _take_renders(self):
+        """Under the lock: the queued renders to decode next, FIFO, as many as
+        memory, max_render_batch and render_batch_pixels allow (the head of
+        the queue waits for memory); unknown sets are returned as errors."""
+        batch, errors, pixels = [], [], 0
+        while self._render_q and len(batch) < self.max_render_batch:
+            rid, req = self._render_q[0]
+            gs = self.sets.get(req.set_id)
+            if gs is None:
+                self._render_q.popleft()
+                errors.append((rid, req))
+                continue
+            px = req.out_h * req.out_w
+            if batch and pixels + px > self.render_batch_pixels:
+                break
+            need = render_bytes(gs, req.out_h, req.out_w, self.block)
+            if not self.budget.try_reserve(need):
+                break
+            self._render_q.popleft()
+            batch.append((rid, req, gs, need))
+            pixels += px
+        return batch, errors
+
     def _render_loop(self):
         torch.cuda.set_device(self.dev)
         while True:
@@ -302,30 +401,37 @@ class Server:
                     if not self._running:
                         return
                     continue
-                rid, req = self._render_q[0]
-                gs = self.sets.get(req.set_id)
-                need = render_bytes(gs, req.out_h, req.out_w, self.block) if gs else 0
-                if gs is not None and not self.budget.try_reserve(need):
+                batch, errors = self._take_renders()
+                if not batch and not errors:
                     self._cv.wait(0.01)  # head of line waits for memory
                     continue
-                self._render_q.popleft()
-            if gs is None:
+            for rid, req in errors:
                 self._finish(rid, error=f"unknown set {req.set_id}")
+            if not batch:
                 continue
-            self.results[rid].t_start = time.perf_counter()
+            t0 = time.perf_counter()
+            for rid, *_ in batch:
+                self.results[rid].t_start = t0
             try:
                 with torch.cuda.stream(self.render_stream):
-                    img, _ = render_view(gs, req.out_h, req.out_w, req.origin,
-                                         (req.scale, req.scale), self.block)
+                    imgs = render_views([(gs, req.out_h, req.out_w, req.origin,
+                                          (req.scale, req.scale)) for _, req, gs, _ in batch],
+                                        self.block)
                     ev = torch.cuda.Event()
                     ev.record(self.render_stream)
-                self.results[rid].t_enqueued = time.perf_counter()
+                t1 = time.perf_counter()
+                for rid, *_ in batch:
+                    self.results[rid].t_enqueued = t1
+                self.render_batches.append(len(batch))
                 ev.synchronize()
-                self._finish(rid, img if req.keep else None)
+                for (rid, req, _, _), img in zip(batch, imgs):
+                    self._finish(rid, img if req.keep else None)
             except Exception as e:  # reported per request; the loop keeps serving
-                self._finish(rid, error=repr(e))
+                for rid, *_ in batch:
+                    self._finish(rid, error=repr(e))
             finally:
-                self.budget.release(need)
+                for *_, need in batch:
+                    self.budget.release(need)
 
     # ----------------------------------------------------------------- fits
     def _admit_fits(self, active: List[_FitJob]) -> bool:

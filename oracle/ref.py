@@ -54,13 +54,24 @@ def _p(t: Optional[torch.Tensor]):
     return None if t is None else ctypes.c_void_p(t.data_ptr())
 
 
+# Converted input copies made by _f stay referenced until the launch that
+# reads them has been enqueued (_chk runs after it): freed earlier, the
+# caching allocator could hand the block to a later copy in the same call.
+_keep = []
+
+
 def _chk(rc, name):
+    _keep.clear()
     if rc != 0:
         raise RuntimeError(f"{name}: CUDA error {rc}")
 
 
 def _f(t):
-    return None if t is None else t.detach().to(torch.float32).contiguous()
+    if t is None:
+        return None
+    t = t.detach().to(torch.float32).contiguous()
+    _keep.append(t)
+    return t
 
 
 def project_fwd(in3, means, opac, H, W, B, chol=True):

@@ -34,7 +34,7 @@ def load_reference(root):
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("LIG_REFERENCE", "/root/reference")
     mod = load_reference(root)
     g = torch.Generator().manual_seed(21)
     out = {}

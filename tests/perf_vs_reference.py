@@ -18,10 +18,12 @@ import torch
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 from lig_b200 import synthetic  # noqa: E402
 from lig_b200.fit import LevelFit, downsample, fit_two_level, make_target, psnr  # noqa: E402
 from oracle import ref  # noqa: E402
+from _reffit import RefFit, ref_two_level  # noqa: E402
 
 CONFIGS = {
     # name: (H=W, fit N, teacher N, diag, noise, noise std, timed iters, psnr iters)
@@ -29,41 +31,6 @@ CONFIGS = {
     "c1l2": (8192, 2_000_000, 2_000_000, (0.5, 6.0), "spectral", 0.03, 20, 100),
     "c3": (4096, 1_000_000, 1_000_000, (0.5, 8.0), "white", 0.02, 20, 0),
 }
-
-
-class RefFit:
-    """The same fit driven by the reference kernels."""
-
-    def __init__(self, n, H, W, diag, lr=1e-3, B=16, seed=synthetic.SEED_INIT):
-        means, chol, colors = synthetic.gaussians(n, H, W, diag=diag, seed=seed)
-        self.means = means.cuda().requires_grad_()
-        self.chol = chol.cuda().requires_grad_()
-        self.rgbs = colors.cuda().requires_grad_()
-        self.H, self.W, self.B = H, W, B
-        self.opt = torch.optim.Adam([self.rgbs, self.means, self.chol], lr=lr, fused=True)
-
-    def render(self):
-        with torch.no_grad():
-            return ref.render(self.chol, self.means, self.rgbs, None, self.H, self.W, self.B)
-
-    def step(self, target):
-        H, W, B = self.H, self.W, self.B
-        with torch.no_grad():
-            r = ref.render(self.chol, self.means, self.rgbs, None, H, W, B)
-            img = r["img"]
-            c = torch.clamp(img, 0, 1)
-            diff = c - target
-            loss = (diff * diff).mean()
-            v_img = (2.0 / img.numel()) * diff * ((img >= 0) & (img <= 1))
-            v_w = torch.zeros(H, W, device=img.device)
-            g = ref.raster_bwd(H, W, B, r["binning"], r["xys"], r["conics"], self.rgbs, None,
-                               r["final_idx"], v_img, v_w)
-            v_chol, v_mean = ref.project_bwd(r["extents"], self.chol, r["conics"], g["v_xy"],
-                                             g["v_conic"], chol=True)
-        self.means.grad, self.chol.grad, self.rgbs.grad = v_mean, v_chol, g["v_rgb"]
-        self.opt.step()
-        self.opt.zero_grad(set_to_none=True)
-        return loss
 
 
 def timed(fit, target, iters):
@@ -79,54 +46,19 @@ def timed(fit, target, iters):
     return iters / (s.elapsed_time(e) / 1e3)
 
 
-def _iters_per_s(fit, target, iters):
-    torch.cuda.synchronize()
-    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s.record()
-    for _ in range(iters):
-        fit.step(target)
-    e.record()
-    torch.cuda.synchronize()
-    return iters / (s.elapsed_time(e) / 1e3)
-
-
-def ref_two_level(gt, n1, n2, iters, factor=4, diag=(0.5, 6.0)):
-    """fit_two_level (lig_b200/fit.py) with every kernel replaced by the
-    reference's: level fits, the gradient-aware render and upscale."""
-    H, W, _ = gt.shape
-    t1 = downsample(gt, factor)
-    h1, w1 = t1.shape[:2]
-    lvl1 = RefFit(n1, h1, w1, diag)
-    ips1 = _iters_per_s(lvl1, t1, iters)
-    with torch.no_grad():
-        r = ref.render(lvl1.chol, lvl1.means, lvl1.rgbs, None, h1, w1, 16, True, True)
-        p1 = psnr(torch.clamp(r["img"], 0, 1), t1)
-        up = ref.upscale_fwd(r["img"], r["dx"], r["dy"], r["dxy"], H, W)
-        resid = gt - up + 0.5
-        lo, hi = resid.min(), resid.max()
-        t2 = ((resid - lo) / (hi - lo)).contiguous()
-    del lvl1
-    lvl2 = RefFit(n2, H, W, diag, seed=synthetic.SEED_INIT + 1)
-    ips2 = _iters_per_s(lvl2, t2, iters)
-    with torch.no_grad():
-        r2 = torch.clamp(lvl2.render()["img"], 0, 1)
-        p2 = psnr(r2, t2)
-        out = torch.clamp(r2 * (hi - lo) + up - 0.5 + lo, 0, 1)
-        pf = psnr(out, gt)
-    return {"psnr": pf, "level_psnr": [p1, p2], "iters_per_s": [ips1, ips2]}
-
-
-def run_two_level(iters):
+def run_two_level(iters, rgb_init="uniform", lr=1e-3):
     """Config 1 end to end: 8192^2 target (2M teacher, diag U[0.5,6], 1/f^2
     noise std 0.03), level 1 = 1M Gaussians on the 4x bicubic-downsampled
-    image, gradient-aware upscale, level 2 = 2M Gaussians on the residual."""
+    image, gradient-aware upscale, level 2 = 2M Gaussians on the residual.
+    rgb_init "uniform" is the configuration's colour draw, "zeros" the
+    reference's own initialisation (gaussianlig.py:57)."""
     gt = make_target(8192, 8192, 2_000_000, (0.5, 6.0), noise="spectral", noise_std=0.03)
     ref.STRICT_SYNC = False
-    mine = fit_two_level(gt, 1_000_000, 2_000_000, iters)
+    mine = fit_two_level(gt, 1_000_000, 2_000_000, iters, lr=lr, rgb_init=rgb_init)
     torch.cuda.empty_cache()
-    theirs = ref_two_level(gt, 1_000_000, 2_000_000, iters)
-    out = {"config": "c1_two_level", "iters_per_level": iters,
-           "lig": {"psnr": mine.psnr, "level_psnr": mine.level_psnr,
+    theirs = ref_two_level(gt, 1_000_000, 2_000_000, iters, lr=lr, rgb_init=rgb_init)
+    out = {"config": "c1_two_level", "iters_per_level": iters, "rgb_init": rgb_init, "lr": lr,
+           "lig": {"psnr": mine.psnr, "level_psnr": mine.level_psnr, "up_psnr": mine.up_psnr,
                    "iters_per_s": mine.iters_per_s},
            "ref": theirs, "psnr_delta_db": mine.psnr - theirs["psnr"],
            "speedup_per_level": [a / b for a, b in zip(mine.iters_per_s,
@@ -168,11 +100,17 @@ def main():
     ap.add_argument("--configs", default="c0,c1l2")
     ap.add_argument("--two-level-iters", type=int, default=0,
                     help="also run config 1 end to end with this many iterations per level")
+    ap.add_argument("--rgb-init", default="uniform,zeros",
+                    help="colour initialisations of the two-level runs")
+    ap.add_argument("--two-level-lr", default="0.001,0.01",
+                    help="Adam learning rate per colour initialisation")
     a = ap.parse_args()
     for c in [c for c in a.configs.split(",") if c]:
         run(c)
     if a.two_level_iters:
-        run_two_level(a.two_level_iters)
+        lrs = [float(x) for x in a.two_level_lr.split(",")]
+        for init, lr in zip(a.rgb_init.split(","), lrs):
+            run_two_level(a.two_level_iters, init, lr)
 
 
 if __name__ == "__main__":

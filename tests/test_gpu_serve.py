@@ -6,7 +6,8 @@ import pytest
 import torch
 
 from lig_b200 import gsplat2d, synthetic
-from lig_b200.serve import (FitRequest, GaussianSet, RenderRequest, Server, render_view)
+from lig_b200.serve import (FitRequest, GaussianSet, RenderRequest, Server, render_view,
+                            render_views)
 
 pytestmark = pytest.mark.gpu
 
@@ -33,6 +34,44 @@ def test_render_view_equals_transformed_render(origin, scale, out):
     xys, ext, con, cnt = gsplat2d.project_gaussians_cholesky(ch, mu, h, w, 16)
     ref = gsplat2d.rasterize_gaussians(xys, ext, con, cnt, gs.rgbs, None, h, w, 16)[0]
     assert torch.equal(img, ref)
+
+
+def test_render_views_equal_single_renders():
+    """A batch of decodes (different sets, sizes, crops and scales; one set
+    with opacities, one parameterised by cov2d) gives each view's own render
+    bit for bit."""
+    a = _set(3000, 256, 55)
+    g = torch.Generator().manual_seed(56)
+    b = _set(2000, 160, 57)
+    b.opacities = (0.05 + 0.95 * torch.rand(b.n, generator=g)).cuda()
+    c = _set(1200, 128, 58)
+    l11, l21, l22 = c.chol[:, 0], c.chol[:, 1], c.chol[:, 2]
+    c = GaussianSet(c.means, torch.stack([l11 * l11, l11 * l21, l21 * l21 + l22 * l22], 1),
+                    c.rgbs, c.H, c.W, cholesky=False)
+    views = [(a, 96, 128, (0.0, 0.0), (1.0, 1.0)), (b, 200, 150, (12.5, 30.0), (1.5, 1.5)),
+             (a, 64, 64, (100.0, 40.0), (0.5, 0.5)), (c, 120, 100, (3.0, 4.0), (1.25, 1.25)),
+             (b, 33, 47, (0.0, 0.0), (0.25, 0.25))]
+    imgs = render_views(views)
+    for (gs, h, w, o, sc), img in zip(views, imgs):
+        assert torch.equal(img, render_view(gs, h, w, o, sc)[0])
+
+
+def test_queued_renders_are_decoded_together():
+    sets = {"a": _set(4000, 256, 52), "b": _set(2500, 192, 53)}
+    reqs = [RenderRequest("a" if k % 2 else "b", 64 + 16 * k, 96 + 8 * k,
+                          (float(3 * k), float(5 * k)), 0.5 + 0.25 * k) for k in range(8)]
+    srv = Server()
+    for k, gs in sets.items():
+        srv.add_set(k, gs)
+    ids = [srv.submit(r) for r in reqs]   # queued before the workers start
+    srv.start()
+    assert srv.drain(timeout=120)
+    srv.stop()
+    assert not srv.errors, srv.errors
+    assert max(srv.render_batches) == len(reqs)
+    for rid, r in zip(ids, reqs):
+        ref = render_view(sets[r.set_id], r.out_h, r.out_w, r.origin, (r.scale, r.scale))[0]
+        assert torch.equal(srv.results[rid].output, ref)
 
 
 def _serve(reqs, sets, **kw):
