@@ -255,6 +255,20 @@ int lig_upscale_bwd(int dtype, int mode, int src_h, int src_w, int dst_h, int ds
                     const void *grad_out, void *grad_render, void *grad_dx, void *grad_dy,
                     void *grad_dxy, void *stream);
 
+/* lig_upscale_fwd / lig_upscale_bwd for HWC planes of `channels` (1 or 3)
+ * channels: channels == 1 is the single-channel form,
+ * torch_gradient_aware_upscale_single_channel (upscaler_torch.py:91-165),
+ * which the reference applies per channel; the 3-channel entries above are
+ * these with channels == 3. */
+int lig_upscale_fwd_nc(int dtype, int mode, int channels, int src_h, int src_w, int dst_h,
+                       int dst_w, double roi_x1, double roi_y1, double roi_x2, double roi_y2,
+                       const void *render, const void *dx, const void *dy, const void *dxy,
+                       void *out, void *stream);
+int lig_upscale_bwd_nc(int dtype, int mode, int channels, int src_h, int src_w, int dst_h,
+                       int dst_w, double roi_x1, double roi_y1, double roi_x2, double roi_y2,
+                       const void *grad_out, void *grad_render, void *grad_dx, void *grad_dy,
+                       void *grad_dxy, void *stream);
+
 /* Forward projection of a view of the Gaussians (region decode at a scale):
  * every Gaussian is first mapped to means' = (means - origin) * (sx, sy) and
  * L' = diag(sx, sy) L (cholesky != 0; the scale_to rule of

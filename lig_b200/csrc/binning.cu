@@ -13,6 +13,7 @@
 // stable LSD radix sort over exactly those bits with <= 10-bit digits, so the
 // order inside a tile is emission order (ascending Gaussian id), which is the
 // order of the reference's stable torch.sort.
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 
@@ -423,6 +424,314 @@ __global__ void flag_overflow_kernel(const int32_t *d_total, int capacity, int32
     if (*d_total > capacity) atomicOr(status, LIG_STATUS_OVERFLOW);
 }
 
+// ---------------------------------------------------- scatter binning
+// Alternative to emission + radix sort + boundary pass (LIG_BIN_SCATTER):
+//   1. count: every tile slot of every Gaussian (the emission enumeration
+//      above) adds 1 to its tile's counter;
+//   2. an exclusive scan of the counters gives each tile's first position;
+//   3. scatter: every slot takes the next free position of its tile (an
+//      atomic cursor), so a tile's entries are contiguous but in arbitrary
+//      order;
+//   4. each tile's entries are sorted by Gaussian index, which restores the
+//      stable sort's order (ascending Gaussian id within a tile, as the
+//      reference's stable torch.sort of (tile << 32) keys in emission
+//      order gives), and tile_bins is written from the counts.
+// The sort key is the Gaussian index; a slot of a Gaussian with extent <= 0
+// (the reference's zero "phantom" slots in the image's first tile) carries
+// bit 31 and is written as the image's first Gaussian id after sorting.
+#ifndef LIG_BIN_SCATTER
+#define LIG_BIN_SCATTER 0
+#endif
+constexpr uint32_t kPhantom = 0x80000000u;
+constexpr int kSegSmem = 2048;     // warp-sorted in shared memory up to this length
+constexpr int kSegWarps = 4;       // warps per CTA of the per-tile sort
+
+// The emission enumeration of emit_kernel, calling f(slot, key, sort_value)
+// for every slot below `capacity` (slots past it set overflow).
+template <typename T, typename F>
+__device__ __forceinline__ void for_each_slot(int n, const T *__restrict__ xys,
+                                              const T *__restrict__ extents,
+                                              const int32_t *__restrict__ cum,
+                                              const BatchGeo &geo, int capacity,
+                                              int32_t *__restrict__ status, F f) {
+    const unsigned FULL = 0xffffffffu;
+    int lane = threadIdx.x & 31;
+    int64_t warp_id = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int64_t g0 = warp_id * 32;
+    if (g0 >= n) return;
+    int g = (int)(g0 + lane);
+    int cnt = 0, start = 0, x0 = 0, y0 = 0, bw = 1, bh = 0;
+    unsigned tbx = 1, toff = 0;
+    bool valid = false;
+    if (g < n) {
+        const int im = geo.image_of_gauss(g);
+        tbx = geo.tbx[im];
+        toff = (unsigned)geo.tile_off[im];
+        int prev = g > 0 ? cum[g - 1] : 0;
+        start = prev;
+        cnt = cum[g] - prev;
+        T ex = extents[2 * g], ey = extents[2 * g + 1];
+        valid = !(ex <= (T)0 || ey <= (T)0);
+        if (valid && cnt > 0) {
+            int x1, y1;
+            tile_bbox(xys[2 * g], xys[2 * g + 1], ex, ey, tbx, geo.tby(im), geo.B, x0, y0, x1, y1);
+            bw = x1 - x0;
+            bh = y1 - y0;
+            if (bw <= 0 || bw * bh != cnt) {
+                if (status) atomicOr(status, LIG_STATUS_BADBOX);
+                valid = false;
+                bw = 1;
+            }
+        }
+    }
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += t;
+    }
+    int total = __shfl_sync(FULL, incl, 31);
+    bool overflow = false;
+    for (int s0 = 0; s0 < total; s0 += 32) {
+        int sl = s0 + lane;
+        int lo = 0;
+#pragma unroll
+        for (int step = 16; step >= 1; step >>= 1) {
+            int probe = lo + step - 1;
+            int v = __shfl_sync(FULL, incl, probe);
+            if (v <= sl) lo += step;
+        }
+        int owner = lo;
+        int o_incl = __shfl_sync(FULL, incl, owner);
+        int o_cnt = __shfl_sync(FULL, cnt, owner);
+        int o_start = __shfl_sync(FULL, start, owner);
+        int o_x0 = __shfl_sync(FULL, x0, owner);
+        int o_y0 = __shfl_sync(FULL, y0, owner);
+        int o_bw = __shfl_sync(FULL, bw, owner);
+        int o_valid = __shfl_sync(FULL, (int)valid, owner);
+        unsigned o_tbx = __shfl_sync(FULL, tbx, owner);
+        unsigned o_toff = __shfl_sync(FULL, toff, owner);
+        if (sl >= total) continue;
+        int j = sl - (o_incl - o_cnt);
+        int slot = o_start + j;
+        if (slot >= capacity) {
+            overflow = true;
+            continue;
+        }
+        uint32_t key = o_toff;
+        uint32_t val = (uint32_t)(g0 + owner) | kPhantom;
+        if (o_valid) {
+            int q = j / o_bw;
+            int r = j - q * o_bw;
+            key = o_toff + (uint32_t)(o_y0 + q) * o_tbx + (uint32_t)(o_x0 + r);
+            val = (uint32_t)(g0 + owner);
+        }
+        f(slot, key, val);
+    }
+    if (overflow && status) atomicOr(status, LIG_STATUS_OVERFLOW);
+}
+
+// 1. per-tile counts (slots below capacity; the rest is flagged as overflow)
+template <typename T>
+__global__ void tile_count_kernel(int n, const T *__restrict__ xys, const T *__restrict__ ext,
+                                  const int32_t *__restrict__ cum, BatchGeo geo, int capacity,
+                                  uint32_t *__restrict__ tcount, int32_t *__restrict__ status) {
+    for_each_slot<T>(n, xys, ext, cum, geo, capacity, status,
+                     [&](int, uint32_t key, uint32_t) { atomicAdd(&tcount[key], 1u); });
+}
+
+// 3. scatter into the tile's range (tstart: exclusive scan of the counts)
+template <typename T>
+__global__ void tile_scatter_kernel(int n, const T *__restrict__ xys, const T *__restrict__ ext,
+                                    const int32_t *__restrict__ cum, BatchGeo geo, int capacity,
+                                    const uint32_t *__restrict__ tstart,
+                                    uint32_t *__restrict__ tfill, uint32_t *__restrict__ out,
+                                    int64_t *__restrict__ keys64, int32_t *__restrict__ gids) {
+    for_each_slot<T>(n, xys, ext, cum, geo, capacity, nullptr,
+                     [&](int slot, uint32_t key, uint32_t val) {
+                         out[tstart[key] + atomicAdd(&tfill[key], 1u)] = val;
+                         if (keys64) {  // the reference's emission-order outputs
+                             const bool ph = (val & kPhantom) != 0;
+                             const int g = (int)(val & ~kPhantom);
+                             const int im = geo.image_of_gauss(g);
+                             keys64[slot] = ph ? (int64_t)geo.tile_off[im] << 32
+                                               : (int64_t)key << 32;
+                             gids[slot] = ph ? geo.g_off[im] : g;
+                         }
+                     });
+}
+
+// sort value -> Gaussian id (phantom slots: the image's first Gaussian)
+__device__ __forceinline__ int32_t slot_id(uint32_t v, const BatchGeo &geo) {
+    if (!(v & kPhantom)) return (int32_t)v;
+    return geo.g_off[geo.image_of_gauss((int)(v & ~kPhantom))];
+}
+
+// Bitonic sort of E * 32 values held E per lane (value k of lane l is
+// element k * 32 + l): pairs within a lane are exchanged in registers,
+// pairs across lanes with shuffles.
+template <int E>
+__device__ __forceinline__ void warp_bitonic(uint32_t (&v)[E]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int size = 2; size <= 32 * E; size <<= 1) {
+#pragma unroll
+        for (int j = size >> 1; j > 0; j >>= 1) {
+            if (j >= 32) {
+                const int kk = j >> 5;
+#pragma unroll
+                for (int k = 0; k < E; ++k) {
+                    const int k2 = k ^ kk;
+                    if (k2 > k) {
+                        const bool asc = (((k * 32 + lane) & size) == 0);
+                        const uint32_t a = v[k], b = v[k2];
+                        const bool sw = asc ? (a > b) : (a < b);
+                        v[k] = sw ? b : a;
+                        v[k2] = sw ? a : b;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < E; ++k) {
+                    const uint32_t o = __shfl_xor_sync(0xffffffffu, v[k], j);
+                    const bool asc = (((k * 32 + lane) & size) == 0);
+                    const bool lower = (lane & j) == 0;
+                    v[k] = (lower == asc) ? min(v[k], o) : max(v[k], o);
+                }
+            }
+        }
+    }
+}
+
+template <int E>
+__device__ __forceinline__ void sort_segment_regs(uint32_t *seg, int L, int32_t *dst,
+                                                  const BatchGeo &geo) {
+    const int lane = threadIdx.x & 31;
+    uint32_t v[E];
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+        const int i = k * 32 + lane;
+        v[k] = i < L ? seg[i] : 0xffffffffu;
+    }
+    warp_bitonic<E>(v);
+    // element k*32+lane of the sorted order
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+        const int i = k * 32 + lane;
+        if (i < L) dst[i] = slot_id(v[k], geo);
+    }
+}
+
+// Bitonic sort of a segment of length L <= kSegSmem by one warp in shared
+// memory (padded to a power of two with the largest value).
+__device__ void sort_segment_smem(const uint32_t *seg, int L, int32_t *dst, uint32_t *buf,
+                                  const BatchGeo &geo) {
+    const int lane = threadIdx.x & 31;
+    int P = 1;
+    while (P < L) P <<= 1;
+    for (int i = lane; i < P; i += 32) buf[i] = i < L ? seg[i] : 0xffffffffu;
+    __syncwarp();
+    for (int size = 2; size <= P; size <<= 1) {
+        for (int j = size >> 1; j > 0; j >>= 1) {
+            for (int t = lane; t < P / 2; t += 32) {
+                const int i = 2 * t - (t & (j - 1));   // lower index of pair t
+                const int k = i + j;
+                const bool asc = (i & size) == 0;
+                const uint32_t a = buf[i], b = buf[k];
+                if (asc ? (a > b) : (a < b)) {
+                    buf[i] = b;
+                    buf[k] = a;
+                }
+            }
+            __syncwarp();
+        }
+    }
+    for (int i = lane; i < L; i += 32) dst[i] = slot_id(buf[i], geo);
+    __syncwarp();
+}
+
+// 4. one warp per tile: sort its entries (from `vals`, written to `ids` as
+// Gaussian ids), write tile_bins ((0, 0) for an empty tile, as the
+// reference's zero-initialised edges) and, when asked, the sorted 64-bit
+// keys.  Tiles longer than kSegSmem are queued for sort_long_kernel.
+__global__ void __launch_bounds__(32 * kSegWarps)
+tile_sort_kernel(BatchGeo geo, const uint32_t *__restrict__ tcount,
+                 const uint32_t *__restrict__ tstart, int capacity, uint32_t *__restrict__ vals,
+                 int32_t *__restrict__ ids, int2 *__restrict__ tile_bins,
+                 int64_t *__restrict__ isect_sorted, int32_t *__restrict__ long_list) {
+    __shared__ uint32_t s_buf[kSegWarps][kSegSmem];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int T = geo.total_tiles();
+    const int nwarps = gridDim.x * kSegWarps;
+    for (int t = blockIdx.x * kSegWarps + w; t < T; t += nwarps) {
+        const uint32_t c = tcount[t];
+        const int a = (int)min((uint32_t)capacity, tstart[t]);
+        const int b = (int)min((uint32_t)capacity, tstart[t] + c);
+        if (lane == 0) tile_bins[t] = c ? make_int2(a, b) : make_int2(0, 0);
+        const int L = b - a;
+        if (L <= 0) continue;
+        if (isect_sorted)
+            for (int i = lane; i < L; i += 32) isect_sorted[a + i] = (int64_t)t << 32;
+        uint32_t *seg = vals + a;
+        int32_t *dst = ids + a;
+        if (L <= 32) sort_segment_regs<1>(seg, L, dst, geo);
+        else if (L <= 64) sort_segment_regs<2>(seg, L, dst, geo);
+        else if (L <= 128) sort_segment_regs<4>(seg, L, dst, geo);
+        else if (L <= 256) sort_segment_regs<8>(seg, L, dst, geo);
+        else if (L <= kSegSmem) sort_segment_smem(seg, L, dst, s_buf[w], geo);
+        else if (lane == 0) long_list[1 + atomicAdd(long_list, 1)] = t;
+    }
+}
+
+// Tiles with more than kSegSmem entries: one CTA per tile sorts the segment
+// in place in global memory, then converts it to ids.  The network is the
+// bitonic sort written with ascending comparators only (each merge starts by
+// comparing mirrored positions of its block, then half-cleaners), so the
+// padding up to a power of two (conceptually the largest value, always at
+// the higher index of a comparator) never moves and is not stored: every
+// comparator that reaches past the segment is skipped.  Rare (thousands of
+// Gaussians over one tile).
+__global__ void __launch_bounds__(1024)
+tile_sort_long_kernel(BatchGeo geo, const uint32_t *__restrict__ tcount,
+                      const uint32_t *__restrict__ tstart, int capacity,
+                      uint32_t *__restrict__ vals, int32_t *__restrict__ ids,
+                      const int32_t *__restrict__ long_list) {
+    const int nlong = long_list[0];
+    for (int q = blockIdx.x; q < nlong; q += gridDim.x) {
+        const int t = long_list[1 + q];
+        const int a = (int)min((uint32_t)capacity, tstart[t]);
+        const int b = (int)min((uint32_t)capacity, tstart[t] + tcount[t]);
+        const int L = b - a;
+        uint32_t *seg = vals + a;
+        int P = 1;
+        while (P < L) P <<= 1;
+        for (int size = 2; size <= P; size <<= 1) {
+            for (int j = size >> 1; j > 0; j >>= 1) {
+                for (int p = threadIdx.x; p < P / 2; p += blockDim.x) {
+                    int i, k;
+                    if (j == size >> 1) {  // mirrored pair of the block
+                        const int blk = p / j, o = p - blk * j;
+                        i = blk * size + o;
+                        k = blk * size + size - 1 - o;
+                    } else {  // half-cleaner at distance j
+                        i = 2 * p - (p & (j - 1));
+                        k = i + j;
+                    }
+                    if (k >= L) continue;
+                    const uint32_t x = seg[i], y = seg[k];
+                    if (x > y) {
+                        seg[i] = y;
+                        seg[k] = x;
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        for (int i = threadIdx.x; i < L; i += blockDim.x) ids[a + i] = slot_id(seg[i], geo);
+        __syncthreads();
+    }
+}
+
 // ------------------------------------------------------- workspace plan
 struct BinPlan {
     int bits, passes, dbits, bins, nblk;
@@ -454,11 +763,84 @@ inline BinPlan make_plan(int capacity, int num_tiles) {
     return p;
 }
 
+// Workspace of the scatter path: per-tile counts, first positions and
+// cursors, scan partials, the long-tile list.  The sort keys are scattered
+// into gid_sorted itself and sorted in place there.
+struct ScatterPlan {
+    size_t off_count, off_start, off_fill, off_part, off_long, total;
+};
+
+inline ScatterPlan make_scatter_plan(int num_tiles) {
+    ScatterPlan p{};
+    size_t t = (size_t)(num_tiles > 0 ? num_tiles : 1);
+    size_t off = 0;
+    p.off_count = off; off = align_up(off + 4 * t);
+    p.off_start = off; off = align_up(off + 4 * t);
+    p.off_fill = off; off = align_up(off + 4 * t);
+    p.off_part = off; off = align_up(off + 4 * ((t + kScanTile - 1) / kScanTile + 1));
+    p.off_long = off; off = align_up(off + 4 * (t + 1));
+    p.total = off;
+    return p;
+}
+
+template <typename T>
+int run_bin_scatter(const BatchGeo &geo, const void *xys, const void *ext, const int32_t *cum,
+                    const int32_t *d_total, int capacity, void *ws, size_t ws_bytes,
+                    int32_t *gid_sorted, int32_t *tile_bins, int64_t *isect, int32_t *gids,
+                    int64_t *isect_sorted, int32_t *status, cudaStream_t s) {
+    const int n = geo.total_points();
+    const int T_ = geo.total_tiles();
+    ScatterPlan p = make_scatter_plan(T_);
+    if (ws_bytes < p.total) return LIG_ERR_WORKSPACE;
+    char *base = (char *)ws;
+    uint32_t *tcount = (uint32_t *)(base + p.off_count);
+    uint32_t *tstart = (uint32_t *)(base + p.off_start);
+    uint32_t *tfill = (uint32_t *)(base + p.off_fill);
+    uint32_t *part = (uint32_t *)(base + p.off_part);
+    int32_t *long_list = (int32_t *)(base + p.off_long);
+    cudaMemsetAsync(status, 0, sizeof(int32_t), s);
+    if (n == 0 || capacity == 0) {
+        cudaMemsetAsync(tile_bins, 0, sizeof(int32_t) * 2 * (size_t)T_, s);
+        flag_overflow_kernel<<<1, 1, 0, s>>>(d_total, capacity, status);
+        note_launches(1);
+        LIG_LAUNCH_CHECK();
+        return LIG_OK;
+    }
+    cudaMemsetAsync(tcount, 0, sizeof(uint32_t) * (size_t)T_, s);
+    cudaMemsetAsync(tfill, 0, sizeof(uint32_t) * (size_t)T_, s);
+    cudaMemsetAsync(long_list, 0, sizeof(int32_t), s);
+    const int warps = (n + 31) / 32;
+    const int eblocks = (warps * 32 + 255) / 256;
+    tile_count_kernel<T><<<eblocks, 256, 0, s>>>(n, (const T *)xys, (const T *)ext, cum, geo,
+                                                 capacity, tcount, status);
+    flag_overflow_kernel<<<1, 1, 0, s>>>(d_total, capacity, status);
+    note_launches(2);
+    LIG_LAUNCH_CHECK();
+    int rc = device_scan(tcount, tstart, T_, false, part, nullptr, s);
+    if (rc) return rc;
+    uint32_t *vals = (uint32_t *)gid_sorted;
+    tile_scatter_kernel<T><<<eblocks, 256, 0, s>>>(n, (const T *)xys, (const T *)ext, cum, geo,
+                                                   capacity, tstart, tfill, vals, isect, gids);
+    const int sort_blocks = (int)std::min<int64_t>(((int64_t)T_ + kSegWarps - 1) / kSegWarps,
+                                                   148 * 32);
+    tile_sort_kernel<<<sort_blocks, 32 * kSegWarps, 0, s>>>(geo, tcount, tstart, capacity, vals,
+                                                          gid_sorted, (int2 *)tile_bins,
+                                                          isect_sorted, long_list);
+    tile_sort_long_kernel<<<148, 1024, 0, s>>>(geo, tcount, tstart, capacity, vals, gid_sorted,
+                                               long_list);
+    note_launches(3);
+    LIG_LAUNCH_CHECK();
+    return LIG_OK;
+}
+
 template <typename T>
 int run_bin(const BatchGeo &geo, const void *xys, const void *ext, const int32_t *cum,
             const int32_t *d_total, int capacity, void *ws, size_t ws_bytes, int32_t *gid_sorted,
             int32_t *tile_bins, int64_t *isect, int32_t *gids, int64_t *isect_sorted,
             int32_t *status, cudaStream_t s) {
+    if (LIG_BIN_SCATTER)
+        return run_bin_scatter<T>(geo, xys, ext, cum, d_total, capacity, ws, ws_bytes,
+                                  gid_sorted, tile_bins, isect, gids, isect_sorted, status, s);
     const int n = geo.total_points();
     const int T_ = geo.total_tiles();
     BinPlan p = make_plan(capacity, T_);
@@ -561,6 +943,7 @@ extern "C" int lig_cumsum_tiles(int n, const int32_t *counts, int32_t *cum, int3
 
 extern "C" size_t lig_bin_workspace_bytes(int n, int capacity, int num_tiles) {
     (void)n;
+    if (LIG_BIN_SCATTER) return make_scatter_plan(num_tiles).total;
     return make_plan(capacity, num_tiles).total;
 }
 

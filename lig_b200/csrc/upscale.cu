@@ -1,5 +1,6 @@
 // Gradient-aware Hermite-bicubic upscale (value, d/dx, d/dy, d2/dxdy planes,
-// HWC with 3 channels), forward and backward.
+// HWC with 3 channels, or 1 for the single-channel form of
+// upscaler_torch.py:91-165), forward and backward.
 //
 // Coordinate maps:
 //   mode 0  half-pixel over a ROI with the ROI extent truncated to int,
@@ -90,24 +91,24 @@ constexpr int kFwdRows = 8, kFwdCols = 64, kFwdThreads = 256;
 constexpr int kFwdMaxSW = kFwdCols + 4;   // staged source columns (scale <= 1 fits)
 constexpr int kFwdMaxSH = kFwdRows + 4;   // staged source rows
 
-template <typename T>
+template <typename T, int C>
 struct FwdSmem {
     int x0[kFwdCols], x1[kFwdCols];
     T cx[kFwdCols][4];
     int y0[kFwdRows], y1[kFwdRows];
     T cy[kFwdRows][4];
-    T src[4][kFwdMaxSH][kFwdMaxSW * 3];   // f, fx, fy, fxy
-    T vf[kFwdRows][kFwdMaxSW * 3];        // F*cy columns 0/1 (value)
-    T vd[kFwdRows][kFwdMaxSW * 3];        // F*cy columns 2/3 (x-derivative)
+    T src[4][kFwdMaxSH][kFwdMaxSW * C];   // f, fx, fy, fxy
+    T vf[kFwdRows][kFwdMaxSW * C];        // F*cy columns 0/1 (value)
+    T vd[kFwdRows][kFwdMaxSW * C];        // F*cy columns 2/3 (x-derivative)
 };
 
-template <typename T>
+template <typename T, int C>
 __global__ void __launch_bounds__(kFwdThreads)
 upscale_fwd_kernel(UpMap mx, UpMap my, int src_w, const T *__restrict__ f,
                    const T *__restrict__ fx, const T *__restrict__ fy,
                    const T *__restrict__ fxy, T *__restrict__ out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    FwdSmem<T> &S = *reinterpret_cast<FwdSmem<T> *>(smem_raw);
+    FwdSmem<T, C> &S = *reinterpret_cast<FwdSmem<T, C> *>(smem_raw);
     const int dst_w = mx.dst_n, dst_h = my.dst_n;
     const int c0 = blockIdx.x * kFwdCols, r0 = blockIdx.y * kFwdRows;
     const int ncol = min(kFwdCols, dst_w - c0), nrow = min(kFwdRows, dst_h - r0);
@@ -124,11 +125,11 @@ upscale_fwd_kernel(UpMap mx, UpMap my, int src_w, const T *__restrict__ f,
     const T *planes[4] = {f, fx, fy, fxy};
     if (SW >= 1 && SH >= 1 && SW <= kFwdMaxSW && SH <= kFwdMaxSH) {
         // stage source window (coalesced: one contiguous 3*SW segment per row)
-        const int seg = 3 * SW;
+        const int seg = C * SW;
         for (int idx = tid; idx < 4 * SH * seg; idx += kFwdThreads) {
             int p = idx / (SH * seg), rem = idx % (SH * seg);
             int r = rem / seg, q = rem % seg;
-            S.src[p][r][q] = planes[p][((int64_t)(ys_lo + r) * src_w + xs_lo) * 3 + q];
+            S.src[p][r][q] = planes[p][((int64_t)(ys_lo + r) * src_w + xs_lo) * C + q];
         }
         __syncthreads();
         // column products per (output row, source column): the reference's
@@ -139,8 +140,8 @@ upscale_fwd_kernel(UpMap mx, UpMap my, int src_w, const T *__restrict__ f,
             int yb = min(max(S.y1[r] - ys_lo, 0), SH - 1);
             const T *cy = S.cy[r];
 #pragma unroll
-            for (int ch = 0; ch < 3; ++ch) {
-                int q = 3 * x + ch;
+            for (int ch = 0; ch < C; ++ch) {
+                int q = C * x + ch;
                 S.vf[r][q] = S.src[0][ya][q] * cy[0] + S.src[0][yb][q] * cy[1] +
                              S.src[2][ya][q] * cy[2] + S.src[2][yb][q] * cy[3];
                 S.vd[r][q] = S.src[1][ya][q] * cy[0] + S.src[1][yb][q] * cy[1] +
@@ -154,11 +155,11 @@ upscale_fwd_kernel(UpMap mx, UpMap my, int src_w, const T *__restrict__ f,
             int xa = min(max(S.x0[c] - xs_lo, 0), SW - 1);
             int xb = min(max(S.x1[c] - xs_lo, 0), SW - 1);
             const T *cx = S.cx[c];
-            T *o = out + ((int64_t)(r0 + r) * dst_w + c0 + c) * 3;
+            T *o = out + ((int64_t)(r0 + r) * dst_w + c0 + c) * C;
 #pragma unroll
-            for (int ch = 0; ch < 3; ++ch)
-                o[ch] = cx[0] * S.vf[r][3 * xa + ch] + cx[1] * S.vf[r][3 * xb + ch] +
-                        cx[2] * S.vd[r][3 * xa + ch] + cx[3] * S.vd[r][3 * xb + ch];
+            for (int ch = 0; ch < C; ++ch)
+                o[ch] = cx[0] * S.vf[r][C * xa + ch] + cx[1] * S.vf[r][C * xb + ch] +
+                        cx[2] * S.vd[r][C * xa + ch] + cx[3] * S.vd[r][C * xb + ch];
         }
         return;
     }
@@ -169,13 +170,13 @@ upscale_fwd_kernel(UpMap mx, UpMap my, int src_w, const T *__restrict__ f,
         const T *cx = S.cx[c], *cy = S.cy[r];
         int64_t i00 = (int64_t)S.y0[r] * src_w + S.x0[c], i01 = (int64_t)S.y0[r] * src_w + S.x1[c];
         int64_t i10 = (int64_t)S.y1[r] * src_w + S.x0[c], i11 = (int64_t)S.y1[r] * src_w + S.x1[c];
-        T *o = out + ((int64_t)(r0 + r) * dst_w + c0 + c) * 3;
+        T *o = out + ((int64_t)(r0 + r) * dst_w + c0 + c) * C;
 #pragma unroll
-        for (int ch = 0; ch < 3; ++ch) {
-            T F0 = f[3 * i00 + ch] * cy[0] + f[3 * i10 + ch] * cy[1] + fy[3 * i00 + ch] * cy[2] + fy[3 * i10 + ch] * cy[3];
-            T F1 = f[3 * i01 + ch] * cy[0] + f[3 * i11 + ch] * cy[1] + fy[3 * i01 + ch] * cy[2] + fy[3 * i11 + ch] * cy[3];
-            T F2 = fx[3 * i00 + ch] * cy[0] + fx[3 * i10 + ch] * cy[1] + fxy[3 * i00 + ch] * cy[2] + fxy[3 * i10 + ch] * cy[3];
-            T F3 = fx[3 * i01 + ch] * cy[0] + fx[3 * i11 + ch] * cy[1] + fxy[3 * i01 + ch] * cy[2] + fxy[3 * i11 + ch] * cy[3];
+        for (int ch = 0; ch < C; ++ch) {
+            T F0 = f[C * i00 + ch] * cy[0] + f[C * i10 + ch] * cy[1] + fy[C * i00 + ch] * cy[2] + fy[C * i10 + ch] * cy[3];
+            T F1 = f[C * i01 + ch] * cy[0] + f[C * i11 + ch] * cy[1] + fy[C * i01 + ch] * cy[2] + fy[C * i11 + ch] * cy[3];
+            T F2 = fx[C * i00 + ch] * cy[0] + fx[C * i10 + ch] * cy[1] + fxy[C * i00 + ch] * cy[2] + fxy[C * i10 + ch] * cy[3];
+            T F3 = fx[C * i01 + ch] * cy[0] + fx[C * i11 + ch] * cy[1] + fxy[C * i01 + ch] * cy[2] + fxy[C * i11 + ch] * cy[3];
             o[ch] = cx[0] * F0 + cx[1] * F1 + cx[2] * F2 + cx[3] * F3;
         }
     }
@@ -185,7 +186,7 @@ upscale_fwd_kernel(UpMap mx, UpMap my, int src_w, const T *__restrict__ f,
 constexpr int kBwdTexH = 8, kBwdTexW = 16, kBwdThreads = 256;
 constexpr int kBwdMaxDW = 72, kBwdMaxDH = 40;   // staged output patch (scale <= 4 fits)
 
-template <typename T>
+template <typename T, int C>
 struct BwdSmem {
     int i_lo, i_hi, j_lo, j_hi;
     int x0[kBwdMaxDW], x1[kBwdMaxDW];
@@ -193,9 +194,9 @@ struct BwdSmem {
     int y0[kBwdMaxDH], y1[kBwdMaxDH];
     T cy[kBwdMaxDH][4];
     int ia[kBwdTexW], ib[kBwdTexW], ja[kBwdTexH], jb[kBwdTexH];
-    T g[kBwdMaxDH][kBwdMaxDW * 3];
-    T uv[kBwdMaxDH][kBwdTexW * 3];   // x-reduced with value weights
-    T ud[kBwdMaxDH][kBwdTexW * 3];   // x-reduced with derivative weights
+    T g[kBwdMaxDH][kBwdMaxDW * C];
+    T uv[kBwdMaxDH][kBwdTexW * C];   // x-reduced with value weights
+    T ud[kBwdMaxDH][kBwdTexW * C];   // x-reduced with derivative weights
 };
 
 // first index in [0, n) whose map (i0 or i1) satisfies pred, binary search
@@ -226,13 +227,13 @@ __device__ __forceinline__ void wx_of(int s, int a, int b, const T *w, T &wv, T 
     wd = (a == s ? w[2] : (T)0) + (b == s ? w[3] : (T)0);
 }
 
-template <typename T>
+template <typename T, int C>
 __global__ void __launch_bounds__(kBwdThreads)
 upscale_bwd_kernel(UpMap mx, UpMap my, int src_w, int src_h, const T *__restrict__ g,
                    T *__restrict__ gf, T *__restrict__ gfx, T *__restrict__ gfy,
                    T *__restrict__ gfxy) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    BwdSmem<T> &S = *reinterpret_cast<BwdSmem<T> *>(smem_raw);
+    BwdSmem<T, C> &S = *reinterpret_cast<BwdSmem<T, C> *>(smem_raw);
     const int dst_w = mx.dst_n;
     const int sx0 = blockIdx.x * kBwdTexW, sy0 = blockIdx.y * kBwdTexH;
     const int nsx = min(kBwdTexW, src_w - sx0), nsy = min(kBwdTexH, src_h - sy0);
@@ -249,9 +250,9 @@ upscale_bwd_kernel(UpMap mx, UpMap my, int src_w, int src_h, const T *__restrict
     const int DW = i_hi - i_lo + 1, DH = j_hi - j_lo + 1;
     const bool staged = DW <= kBwdMaxDW && DH <= kBwdMaxDH;
     if (DW <= 0 || DH <= 0) {
-        for (int idx = tid; idx < nsy * nsx * 3; idx += kBwdThreads) {
-            int r = idx / (nsx * 3), q = idx % (nsx * 3);
-            int64_t o = ((int64_t)(sy0 + r) * src_w + sx0) * 3 + q;
+        for (int idx = tid; idx < nsy * nsx * C; idx += kBwdThreads) {
+            int r = idx / (nsx * C), q = idx % (nsx * C);
+            int64_t o = ((int64_t)(sy0 + r) * src_w + sx0) * C + q;
             gf[o] = 0; gfx[o] = 0; gfy[o] = 0; gfxy[o] = 0;
         }
         return;
@@ -259,10 +260,10 @@ upscale_bwd_kernel(UpMap mx, UpMap my, int src_w, int src_h, const T *__restrict
     if (staged) {
         for (int i = tid; i < DW; i += kBwdThreads) coord<T>(mx, i_lo + i, S.x0[i], S.x1[i], S.cx[i]);
         for (int j = tid; j < DH; j += kBwdThreads) coord<T>(my, j_lo + j, S.y0[j], S.y1[j], S.cy[j]);
-        const int seg = 3 * DW;
+        const int seg = C * DW;
         for (int idx = tid; idx < DH * seg; idx += kBwdThreads) {
             int r = idx / seg, q = idx % seg;
-            S.g[r][q] = g[((int64_t)(j_lo + r) * dst_w + i_lo) * 3 + q];
+            S.g[r][q] = g[((int64_t)(j_lo + r) * dst_w + i_lo) * C + q];
         }
         __syncthreads();
         // candidate output ranges per source column / row (monotone maps)
@@ -281,43 +282,43 @@ upscale_bwd_kernel(UpMap mx, UpMap my, int src_w, int src_h, const T *__restrict
         // x-reduction: for each staged output row and source column
         for (int idx = tid; idx < DH * nsx; idx += kBwdThreads) {
             int r = idx / nsx, sc = idx % nsx, s = sx0 + sc;
-            T av[3] = {0, 0, 0}, ad[3] = {0, 0, 0};
+            T av[C] = {}, ad[C] = {};
             for (int i = S.ia[sc]; i <= S.ib[sc]; ++i) {
                 T wv, wd;
                 wx_of<T>(s, S.x0[i], S.x1[i], S.cx[i], wv, wd);
 #pragma unroll
-                for (int ch = 0; ch < 3; ++ch) {
-                    T gv = S.g[r][3 * i + ch];
+                for (int ch = 0; ch < C; ++ch) {
+                    T gv = S.g[r][C * i + ch];
                     av[ch] += gv * wv;
                     ad[ch] += gv * wd;
                 }
             }
 #pragma unroll
-            for (int ch = 0; ch < 3; ++ch) {
-                S.uv[r][3 * sc + ch] = av[ch];
-                S.ud[r][3 * sc + ch] = ad[ch];
+            for (int ch = 0; ch < C; ++ch) {
+                S.uv[r][C * sc + ch] = av[ch];
+                S.ud[r][C * sc + ch] = ad[ch];
             }
         }
         __syncthreads();
         // y-reduction and write-out
         for (int idx = tid; idx < nsy * nsx; idx += kBwdThreads) {
             int rr = idx / nsx, sc = idx % nsx, s = sy0 + rr;
-            T a0[3] = {0, 0, 0}, a1[3] = {0, 0, 0}, a2[3] = {0, 0, 0}, a3[3] = {0, 0, 0};
+            T a0[C] = {}, a1[C] = {}, a2[C] = {}, a3[C] = {};
             for (int j = S.ja[rr]; j <= S.jb[rr]; ++j) {
                 T wv, wd;
                 wx_of<T>(s, S.y0[j], S.y1[j], S.cy[j], wv, wd);
 #pragma unroll
-                for (int ch = 0; ch < 3; ++ch) {
-                    T uv = S.uv[j][3 * sc + ch], ud = S.ud[j][3 * sc + ch];
+                for (int ch = 0; ch < C; ++ch) {
+                    T uv = S.uv[j][C * sc + ch], ud = S.ud[j][C * sc + ch];
                     a0[ch] += uv * wv;   // value plane
                     a1[ch] += ud * wv;   // x-derivative plane
                     a2[ch] += uv * wd;   // y-derivative plane
                     a3[ch] += ud * wd;   // mixed plane
                 }
             }
-            int64_t o = ((int64_t)s * src_w + sx0 + sc) * 3;
+            int64_t o = ((int64_t)s * src_w + sx0 + sc) * C;
 #pragma unroll
-            for (int ch = 0; ch < 3; ++ch) {
+            for (int ch = 0; ch < C; ++ch) {
                 gf[o + ch] = a0[ch]; gfx[o + ch] = a1[ch]; gfy[o + ch] = a2[ch]; gfxy[o + ch] = a3[ch];
             }
         }
@@ -326,7 +327,7 @@ upscale_bwd_kernel(UpMap mx, UpMap my, int src_w, int src_h, const T *__restrict
     // large patches (strong down-scaling): per texel, straight from global memory
     for (int idx = tid; idx < nsy * nsx; idx += kBwdThreads) {
         int rr = idx / nsx, sc = idx % nsx, sy = sy0 + rr, sx = sx0 + sc;
-        T a0[3] = {0, 0, 0}, a1[3] = {0, 0, 0}, a2[3] = {0, 0, 0}, a3[3] = {0, 0, 0};
+        T a0[C] = {}, a1[C] = {}, a2[C] = {}, a3[C] = {};
         int jl = first_x1_ge<T>(my, sy), jh = last_x0_le<T>(my, sy);
         int il = first_x1_ge<T>(mx, sx), ih = last_x0_le<T>(mx, sx);
         for (int j = jl; j <= jh; ++j) {
@@ -342,9 +343,9 @@ upscale_bwd_kernel(UpMap mx, UpMap my, int src_w, int src_h, const T *__restrict
                 coord<T>(mx, i, xa, xb, cx);
                 T xv, xd;
                 wx_of<T>(sx, xa, xb, cx, xv, xd);
-                const T *gp = g + ((int64_t)j * dst_w + i) * 3;
+                const T *gp = g + ((int64_t)j * dst_w + i) * C;
 #pragma unroll
-                for (int ch = 0; ch < 3; ++ch) {
+                for (int ch = 0; ch < C; ++ch) {
                     T gv = gp[ch];
                     a0[ch] += gv * xv * yv;
                     a1[ch] += gv * xd * yv;
@@ -353,9 +354,9 @@ upscale_bwd_kernel(UpMap mx, UpMap my, int src_w, int src_h, const T *__restrict
                 }
             }
         }
-        int64_t o = ((int64_t)sy * src_w + sx) * 3;
+        int64_t o = ((int64_t)sy * src_w + sx) * C;
 #pragma unroll
-        for (int ch = 0; ch < 3; ++ch) {
+        for (int ch = 0; ch < C; ++ch) {
             gf[o + ch] = a0[ch]; gfx[o + ch] = a1[ch]; gfy[o + ch] = a2[ch]; gfxy[o + ch] = a3[ch];
         }
     }
@@ -367,33 +368,33 @@ inline bool set_smem(const void *fn, size_t bytes) {
            cudaSuccess;
 }
 
-template <typename T>
+template <typename T, int C>
 int upscale_fwd(int mode, int src_h, int src_w, int dst_h, int dst_w, double x1, double y1,
                 double x2, double y2, const void *f, const void *fx, const void *fy,
                 const void *fxy, void *out, cudaStream_t s) {
     // the reference truncates the ROI extent to int (csrc/gradient_aware_upscaler.cu:201-202)
     UpMap mx{mode, dst_w, src_w, (int)((T)x2 - (T)x1), (double)(T)x1};
     UpMap my{mode, dst_h, src_h, (int)((T)y2 - (T)y1), (double)(T)y1};
-    size_t sm = sizeof(FwdSmem<T>);
-    if (!set_smem((const void *)upscale_fwd_kernel<T>, sm)) return LIG_ERR_LAUNCH;
+    size_t sm = sizeof(FwdSmem<T, C>);
+    if (!set_smem((const void *)upscale_fwd_kernel<T, C>, sm)) return LIG_ERR_LAUNCH;
     dim3 grid((dst_w + kFwdCols - 1) / kFwdCols, (dst_h + kFwdRows - 1) / kFwdRows);
-    upscale_fwd_kernel<T><<<grid, kFwdThreads, sm, s>>>(mx, my, src_w, (const T *)f, (const T *)fx,
+    upscale_fwd_kernel<T, C><<<grid, kFwdThreads, sm, s>>>(mx, my, src_w, (const T *)f, (const T *)fx,
                                                        (const T *)fy, (const T *)fxy, (T *)out);
     note_launches(1);
     LIG_LAUNCH_CHECK();
     return LIG_OK;
 }
 
-template <typename T>
+template <typename T, int C>
 int upscale_bwd(int mode, int src_h, int src_w, int dst_h, int dst_w, double x1, double y1,
                 double x2, double y2, const void *g, void *gf, void *gfx, void *gfy, void *gfxy,
                 cudaStream_t s) {
     UpMap mx{mode, dst_w, src_w, (int)((T)x2 - (T)x1), (double)(T)x1};
     UpMap my{mode, dst_h, src_h, (int)((T)y2 - (T)y1), (double)(T)y1};
-    size_t sm = sizeof(BwdSmem<T>);
-    if (!set_smem((const void *)upscale_bwd_kernel<T>, sm)) return LIG_ERR_LAUNCH;
+    size_t sm = sizeof(BwdSmem<T, C>);
+    if (!set_smem((const void *)upscale_bwd_kernel<T, C>, sm)) return LIG_ERR_LAUNCH;
     dim3 grid((src_w + kBwdTexW - 1) / kBwdTexW, (src_h + kBwdTexH - 1) / kBwdTexH);
-    upscale_bwd_kernel<T><<<grid, kBwdThreads, sm, s>>>(mx, my, src_w, src_h, (const T *)g,
+    upscale_bwd_kernel<T, C><<<grid, kBwdThreads, sm, s>>>(mx, my, src_w, src_h, (const T *)g,
                                                        (T *)gf, (T *)gfx, (T *)gfy, (T *)gfxy);
     note_launches(1);
     LIG_LAUNCH_CHECK();
@@ -408,22 +409,66 @@ inline bool up_args_ok(int mode, int sh, int sw, int dh, int dw) {
 
 using namespace lig;
 
+namespace lig {
+template <int C>
+int upscale_fwd_dt(int dtype, int mode, int sh, int sw, int dh, int dw, double x1, double y1,
+                   double x2, double y2, const void *f, const void *fx, const void *fy,
+                   const void *fxy, void *out, cudaStream_t s) {
+    if (dtype == LIG_F32)
+        return upscale_fwd<float, C>(mode, sh, sw, dh, dw, x1, y1, x2, y2, f, fx, fy, fxy, out, s);
+    if (dtype == LIG_F64)
+        return upscale_fwd<double, C>(mode, sh, sw, dh, dw, x1, y1, x2, y2, f, fx, fy, fxy, out, s);
+    return LIG_ERR_INVALID;
+}
+template <int C>
+int upscale_bwd_dt(int dtype, int mode, int sh, int sw, int dh, int dw, double x1, double y1,
+                   double x2, double y2, const void *g, void *gf, void *gfx, void *gfy,
+                   void *gfxy, cudaStream_t s) {
+    if (dtype == LIG_F32)
+        return upscale_bwd<float, C>(mode, sh, sw, dh, dw, x1, y1, x2, y2, g, gf, gfx, gfy, gfxy, s);
+    if (dtype == LIG_F64)
+        return upscale_bwd<double, C>(mode, sh, sw, dh, dw, x1, y1, x2, y2, g, gf, gfx, gfy, gfxy,
+                                      s);
+    return LIG_ERR_INVALID;
+}
+}  // namespace lig
+
+extern "C" int lig_upscale_fwd_nc(int dtype, int mode, int channels, int sh, int sw, int dh,
+                                  int dw, double x1, double y1, double x2, double y2,
+                                  const void *f, const void *fx, const void *fy, const void *fxy,
+                                  void *out, void *stream) {
+    if (!up_args_ok(mode, sh, sw, dh, dw) || !f || !fx || !fy || !fxy || !out) return LIG_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (channels == 3)
+        return upscale_fwd_dt<3>(dtype, mode, sh, sw, dh, dw, x1, y1, x2, y2, f, fx, fy, fxy, out, s);
+    if (channels == 1)
+        return upscale_fwd_dt<1>(dtype, mode, sh, sw, dh, dw, x1, y1, x2, y2, f, fx, fy, fxy, out, s);
+    return LIG_ERR_INVALID;
+}
+
+extern "C" int lig_upscale_bwd_nc(int dtype, int mode, int channels, int sh, int sw, int dh,
+                                  int dw, double x1, double y1, double x2, double y2,
+                                  const void *g, void *gf, void *gfx, void *gfy, void *gfxy,
+                                  void *stream) {
+    if (!up_args_ok(mode, sh, sw, dh, dw) || !g || !gf || !gfx || !gfy || !gfxy) return LIG_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (channels == 3)
+        return upscale_bwd_dt<3>(dtype, mode, sh, sw, dh, dw, x1, y1, x2, y2, g, gf, gfx, gfy, gfxy, s);
+    if (channels == 1)
+        return upscale_bwd_dt<1>(dtype, mode, sh, sw, dh, dw, x1, y1, x2, y2, g, gf, gfx, gfy, gfxy, s);
+    return LIG_ERR_INVALID;
+}
+
 extern "C" int lig_upscale_fwd(int dtype, int mode, int sh, int sw, int dh, int dw, double x1,
                                double y1, double x2, double y2, const void *f, const void *fx,
                                const void *fy, const void *fxy, void *out, void *stream) {
-    if (!up_args_ok(mode, sh, sw, dh, dw) || !f || !fx || !fy || !fxy || !out) return LIG_ERR_INVALID;
-    cudaStream_t s = (cudaStream_t)stream;
-    if (dtype == LIG_F32) return upscale_fwd<float>(mode, sh, sw, dh, dw, x1, y1, x2, y2, f, fx, fy, fxy, out, s);
-    if (dtype == LIG_F64) return upscale_fwd<double>(mode, sh, sw, dh, dw, x1, y1, x2, y2, f, fx, fy, fxy, out, s);
-    return LIG_ERR_INVALID;
+    return lig_upscale_fwd_nc(dtype, mode, 3, sh, sw, dh, dw, x1, y1, x2, y2, f, fx, fy, fxy, out,
+                              stream);
 }
 
 extern "C" int lig_upscale_bwd(int dtype, int mode, int sh, int sw, int dh, int dw, double x1,
                                double y1, double x2, double y2, const void *g, void *gf,
                                void *gfx, void *gfy, void *gfxy, void *stream) {
-    if (!up_args_ok(mode, sh, sw, dh, dw) || !g || !gf || !gfx || !gfy || !gfxy) return LIG_ERR_INVALID;
-    cudaStream_t s = (cudaStream_t)stream;
-    if (dtype == LIG_F32) return upscale_bwd<float>(mode, sh, sw, dh, dw, x1, y1, x2, y2, g, gf, gfx, gfy, gfxy, s);
-    if (dtype == LIG_F64) return upscale_bwd<double>(mode, sh, sw, dh, dw, x1, y1, x2, y2, g, gf, gfx, gfy, gfxy, s);
-    return LIG_ERR_INVALID;
+    return lig_upscale_bwd_nc(dtype, mode, 3, sh, sw, dh, dw, x1, y1, x2, y2, g, gf, gfx, gfy,
+                              gfxy, stream);
 }

@@ -490,17 +490,19 @@ def l2_clamped_loss(img, target):
 
 # ------------------------------------------------------------------ upscale
 def upscale_fwd(render, dx, dy, dxy, dst_h, dst_w, roi=None, mode: int = 0):
+    """[H, W, C] value / dx / dy / dxy planes (C = 3, or 1 for the
+    single-channel form) -> [dst_h, dst_w, C]."""
     _check_cuda(render, dx, dy, dxy)
     render = _c(render)
     dt = render.dtype
     dx, dy, dxy = _c(dx, dt), _c(dy, dt), _c(dxy, dt)
     h, w, c = render.shape
-    if c != 3:
-        raise ValueError("gradient-aware upscale expects [H, W, 3] planes")
+    if c not in (1, 3):
+        raise ValueError("gradient-aware upscale expects [H, W, 3] (or [H, W, 1]) planes")
     if roi is None:
         roi = (0.0, 0.0, float(w), float(h))
-    out = torch.empty((int(dst_h), int(dst_w), 3), dtype=dt, device=render.device)
-    call("lig_upscale_fwd", _dt(render), int(mode), h, w, int(dst_h), int(dst_w),
+    out = torch.empty((int(dst_h), int(dst_w), c), dtype=dt, device=render.device)
+    call("lig_upscale_fwd_nc", _dt(render), int(mode), c, h, w, int(dst_h), int(dst_w),
          float(roi[0]), float(roi[1]), float(roi[2]), float(roi[3]), _p(render), _p(dx), _p(dy),
          _p(dxy), _p(out), _stream(render.device))
     return out
@@ -510,12 +512,14 @@ def upscale_bwd(grad_out, src_h, src_w, roi=None, mode: int = 0):
     _check_cuda(grad_out)
     grad_out = _c(grad_out)
     dt = grad_out.dtype
-    dh, dw, _ = grad_out.shape
+    dh, dw, c = grad_out.shape
+    if c not in (1, 3):
+        raise ValueError("gradient-aware upscale expects [H, W, 3] (or [H, W, 1]) planes")
     if roi is None:
         roi = (0.0, 0.0, float(src_w), float(src_h))
-    outs = [torch.empty((int(src_h), int(src_w), 3), dtype=dt, device=grad_out.device)
+    outs = [torch.empty((int(src_h), int(src_w), c), dtype=dt, device=grad_out.device)
             for _ in range(4)]
-    call("lig_upscale_bwd", _dt(grad_out), int(mode), int(src_h), int(src_w), dh, dw,
+    call("lig_upscale_bwd_nc", _dt(grad_out), int(mode), c, int(src_h), int(src_w), dh, dw,
          float(roi[0]), float(roi[1]), float(roi[2]), float(roi[3]), _p(grad_out),
          *[_p(o) for o in outs], _stream(grad_out.device))
     return tuple(outs)

@@ -25,12 +25,13 @@ class _AlignCornersUpscale(Function):
 
 def torch_gradient_aware_upscale(render_hwc: torch.Tensor, dx: torch.Tensor, dy: torch.Tensor,
                                  dxy: torch.Tensor, new_h: int, new_w: int) -> torch.Tensor:
-    """[H, W, C] value/dx/dy/dxy planes -> [new_h, new_w, C] (C == 3)."""
+    """[H, W, 3] value/dx/dy/dxy planes -> [new_h, new_w, 3]."""
     return _AlignCornersUpscale.apply(render_hwc.contiguous(), dx.contiguous(), dy.contiguous(),
                                       dxy.contiguous(), int(new_h), int(new_w))
 
 
 def torch_gradient_aware_upscale_single_channel(render, dx, dy, dxy, new_h: int, new_w: int):
-    """Single-channel form [H, W] -> [new_h, new_w] (upscaler_torch.py:91-165)."""
-    planes = [t.unsqueeze(-1).expand(*t.shape, 3) for t in (render, dx, dy, dxy)]
-    return torch_gradient_aware_upscale(*planes, new_h, new_w)[..., 0]
+    """Single-channel form [H, W] -> [new_h, new_w] (upscaler_torch.py:91-165),
+    on the kernel's one-channel instantiation."""
+    planes = [t.unsqueeze(-1).contiguous() for t in (render, dx, dy, dxy)]
+    return _AlignCornersUpscale.apply(*planes, int(new_h), int(new_w))[..., 0]

@@ -141,6 +141,32 @@ def test_align_corners_upscaler_matches_oracle():
         assert rel_err(np_(a.grad), b) <= 1e-12
 
 
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_single_channel_upscaler_is_one_channel_of_the_rgb_form(dtype):
+    """torch_gradient_aware_upscale_single_channel runs the one-channel
+    kernel: value and gradients equal channel k of the 3-channel upscale of
+    planes whose channel k holds the single-channel input (half-pixel ROI
+    path through ops too)."""
+    h, w, nh, nw = 37, 45, 90, 131
+    g = torch.Generator().manual_seed(18)
+    planes = [torch.randn(h, w, generator=g, dtype=dtype).cuda() for _ in range(4)]
+    gout = torch.randn(nh, nw, generator=g, dtype=dtype).cuda()
+    x1 = [p.clone().requires_grad_() for p in planes]
+    y1 = upscaler_torch.torch_gradient_aware_upscale_single_channel(*x1, nh, nw)
+    y1.backward(gout)
+    rgb = [torch.stack([torch.zeros_like(p), p, torch.zeros_like(p)], -1) for p in planes]
+    x3 = [p.clone().requires_grad_() for p in rgb]
+    y3 = upscaler_torch.torch_gradient_aware_upscale(*x3, nh, nw)
+    y3.backward(torch.stack([torch.zeros_like(gout), gout, torch.zeros_like(gout)], -1))
+    assert y1.shape == (nh, nw) and torch.equal(y1, y3[..., 1])
+    for a, b in zip(x1, x3):
+        assert torch.equal(a.grad, b.grad[..., 1])
+    roi = (3.0, 2.5, 40.0, 30.0)
+    o1 = ops.upscale_fwd(*[p.unsqueeze(-1) for p in planes], nh, nw, roi=roi, mode=0)
+    o3 = ops.upscale_fwd(*rgb, nh, nw, roi=roi, mode=0)
+    assert torch.equal(o1[..., 0], o3[..., 1])
+
+
 def test_lig_training_step_decreases_loss():
     H, W, B, n = 96, 96, 16, 2000
     means, L, colors, _ = scene(n, H, W, diag=(0.5, 3.0), seed=2)
@@ -186,6 +212,30 @@ def test_fused_render_l2_matches_unfused_chain():
     assert abs(l1.item() - l2.item()) <= 1e-6 * abs(l1.item())
     for a, b in zip(p2, p1):
         assert rel_err(np_(a.grad), np_(b.grad)) <= 1e-5
+
+
+def test_fused_l2_forward_nonfinite_colours():
+    """Gaussians with infinite or NaN colours: the fused forward's masked
+    difference and final indices equal the plain forward's exactly (the
+    packed four-pixel loop hands such Gaussians to its scalar path)."""
+    H, W, B, n = 1040, 1100, 16, 20000
+    means, L, colors, _ = scene(n, H, W, diag=(0.5, 5.0), seed=16)
+    bad = torch.arange(0, n, n // 24, device="cuda")[:24]
+    vals = torch.tensor([float("inf"), -float("inf"), float("nan")], device="cuda")
+    colors = colors.clone()
+    colors[bad, torch.arange(24, device="cuda") % 3] = vals[torch.arange(24, device="cuda") % 3]
+    g = torch.Generator().manual_seed(17)
+    target = torch.rand(H, W, 3, generator=g).cuda()
+    xys, ext, con, cnt = ops.project_fwd(L, means, None, H, W, B, True)
+    b = ops.bin_gaussians(xys, ext, cnt, H, W, B)
+    img, _, _, _, _, fin = ops.raster_fwd(H, W, B, b.gaussian_ids_sorted, b.tile_bins, b.total,
+                                          xys, con, colors, None, False)
+    diff, fin2, _ = ops.raster_fwd_l2(H, W, B, b.gaussian_ids_sorted, b.tile_bins, b.total,
+                                      xys, con, colors, None, target)
+    assert not torch.isfinite(img).all()
+    exp = torch.where((img >= 0) & (img <= 1), torch.clamp(img, 0, 1) - target,
+                      torch.zeros_like(img))
+    assert torch.equal(diff, exp) and torch.equal(fin2, fin)
 
 
 @pytest.mark.parametrize("H,W,B,n", [(150, 170, 16, 3000),
