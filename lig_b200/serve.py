@@ -564,6 +564,76 @@ def resident_sets(n_sets: int = 64, n_min: int = 100_000, n_max: int = 3_000_000
     return out
 
 
+def fitted_sets(n_sets: int = 64, n_min: int = 100_000, n_max: int = 3_000_000,
+                seed: int = 5000, iters: int = 100, lr: float = 1e-2, directory=None,
+                device="cuda", block: int = 16,
+                max_batch_pixels: int = 120_000_000) -> Dict[str, GaussianSet]:
+    """Resident sets that are fits, stored and loaded as LIG stores them.
+
+    Set k has the Gaussian count and image side of resident_sets (N_k ~
+    U[n_min, n_max], side sqrt(N_k / 0.2)).  Its target is a seeded
+    synthetic image of that side (teacher render at the fit configurations'
+    density plus N(0, 0.02) noise); N_k Gaussians (means / Cholesky factors
+    drawn as resident_sets draws them, colours starting at zero as
+    gaussianlig.py:57) are fitted for `iters` Adam iterations, in
+    BatchedFits of at most max_batch_pixels target pixels.  Each fitted set
+    is written with save_lig (the reference's checkpoint layout,
+    train.py:172-176) into `directory` (a temporary directory by default)
+    and read back with load_lig (train.py:49-67); the loaded sets are
+    returned."""
+    import os
+    import tempfile
+
+    from .fit import make_target
+    from .levels import load_lig, save_lig
+
+    g = torch.Generator().manual_seed(seed)
+    counts, sides = [], []
+    for k in range(n_sets):
+        n = int(n_min + (n_max - n_min) * torch.rand(1, generator=g).item())
+        counts.append(n)
+        sides.append(int(round(math.sqrt(n / 0.2))))
+    # batches of sets under a pixel budget (32-bit pixel-channel indexing and
+    # memory), fitted one after another
+    groups, cur, px = [], [], 0
+    for k, side in enumerate(sides):
+        if cur and px + side * side > max_batch_pixels:
+            groups.append(cur)
+            cur, px = [], 0
+        cur.append(k)
+        px += side * side
+    groups.append(cur)
+    own = directory is None
+    d = tempfile.mkdtemp(prefix="lig_sets_") if own else directory
+    out = {}
+    try:
+        for grp in groups:
+            targets, init = [], []
+            for k in grp:
+                n, side = counts[k], sides[k]
+                n_teacher = int(round(20000 / 512**2 * side * side))
+                targets.append(make_target(side, side, n_teacher, (0.5, 4.0), noise="white",
+                                           noise_std=0.02, device=device, block=block))
+                mu, ch, _ = synthetic.gaussians(n, side, side, diag=(0.5, 4.0),
+                                                seed=seed + 1 + k)
+                init.append((mu.to(device), ch.to(device), torch.zeros(n, 3, device=device)))
+            fit = BatchedFit(targets, [counts[k] for k in grp], block=block, lr=lr, init=init)
+            fit.fit(iters)
+            for i, k in enumerate(grp):
+                mu, ch, co = (t.detach() for t in fit.params_of(i))
+                path = os.path.join(d, f"set{k}.pth")
+                save_lig(path, [GaussianSet(mu, ch, co, sides[k], sides[k])], [], [])
+                out[f"set{k}"] = load_lig(path, device=device).levels[0]
+                if own:
+                    os.remove(path)
+            del fit, targets, init
+            torch.cuda.empty_cache()
+    finally:
+        if own:
+            os.rmdir(d)
+    return out
+
+
 def poisson_requests(duration_s: float, rate: float, fit_frac: float, sets: Dict[str, GaussianSet],
                      fit_iters: int = 300, fit_side=(512, 4096), render_side=(256, 4096),
                      render_scale=(0.25, 2.0), seed: int = 5000):

@@ -1,7 +1,9 @@
 """Serving loop under a Poisson mix of renders and fits (one GPU).
 
-Workload (seeded, synthetic): 64 resident sets of 100k-3M Gaussians
-(lig_b200.serve.resident_sets, 0.2 Gaussians per pixel of the set's image);
+Workload (seeded, synthetic): 64 resident sets of 100k-3M Gaussians, 0.2
+Gaussians per pixel of the set's image, fitted to synthetic images and
+stored / loaded in LIG's checkpoint format (lig_b200.serve.fitted_sets;
+--random-sets uses unfitted seeded draws instead);
 Poisson arrivals at --rate per second for --duration seconds, a --fit-frac
 share of fits (square target side U[512, 4096], min(0.2 side^2, 1M)
 Gaussians, --fit-iters iterations, targets cropped from one 4096^2 teacher
@@ -31,8 +33,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
 
 from lig_b200.fit import make_target  # noqa: E402
-from lig_b200.serve import (Server, percentile, poisson_requests, resident_sets,  # noqa: E402
-                            run_workload)
+from lig_b200.serve import (Server, fitted_sets, percentile, poisson_requests,  # noqa: E402
+                            resident_sets, run_workload)
 
 
 def main():
@@ -44,6 +46,10 @@ def main():
     ap.add_argument("--drain", type=float, default=30.0)
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--sets", type=int, default=64)
+    ap.add_argument("--set-fit-iters", type=int, default=100,
+                    help="iterations of the resident sets' fits")
+    ap.add_argument("--random-sets", action="store_true",
+                    help="unfitted seeded draws as resident sets")
     ap.add_argument("--fit-chunk", type=int, default=20)
     ap.add_argument("--fit-ahead", type=int, default=2,
                     help="fit iterations queued on the device at most (0: a whole chunk)")
@@ -53,7 +59,9 @@ def main():
     ap.add_argument("--dump", default="", help="write per-request timings (CSV) here")
     a = ap.parse_args()
     t0 = time.time()
-    sets = resident_sets(a.sets)
+    sets = (resident_sets(a.sets) if a.random_sets
+            else fitted_sets(a.sets, iters=a.set_fit_iters))
+    torch.cuda.empty_cache()
     master = make_target(4096, 4096, int(round(20000 / 512**2 * 4096**2)), (0.5, 4.0),
                          noise="white", noise_std=0.02)
     schedule = poisson_requests(a.duration, a.rate, a.fit_frac, sets, fit_iters=a.fit_iters,
@@ -88,6 +96,12 @@ def main():
         "fit_phase_s": {ph: round(sum(b - a for a, b, p in srv.fit_phases if p == ph), 2)
                         for ph in ("build", "iterate", "finish")},
         "fit_batches": srv.fit_batches, "budget_peak_gb": srv.budget.peak / 1e9,
+        "sets": "random draws" if a.random_sets else f"fitted ({a.set_fit_iters} iters), "
+                                                      "saved and loaded with save_lig/load_lig",
+        "render_batches": {"count": len(srv.render_batches),
+                           "mean_size": (sum(srv.render_batches) / len(srv.render_batches)
+                                         if srv.render_batches else 0.0),
+                           "max_size": max(srv.render_batches, default=0)},
         "errors": srv.errors[:5],
     }
     if a.dump:

@@ -74,6 +74,23 @@ def test_queued_renders_are_decoded_together():
         assert torch.equal(srv.results[rid].output, ref)
 
 
+def test_fitted_sets_round_trip_through_the_checkpoint(tmp_path):
+    """fitted_sets fits each set, writes it in LIG's checkpoint layout and
+    serves what load_lig reads back: the files hold the same parameters."""
+    from lig_b200.levels import load_lig
+    from lig_b200.serve import fitted_sets
+    sets = fitted_sets(n_sets=3, n_min=2000, n_max=6000, iters=5, directory=str(tmp_path))
+    assert sorted(sets) == ["set0", "set1", "set2"]
+    for k, gs in sets.items():
+        again = load_lig(str(tmp_path / f"{k}.pth")).levels[0]
+        assert torch.equal(again.means, gs.means) and torch.equal(again.chol, gs.chol)
+        assert torch.equal(again.rgbs, gs.rgbs) and (gs.H, gs.W) == (again.H, again.W)
+        assert 2000 <= gs.n <= 6000 and gs.cholesky
+        assert float(gs.rgbs.abs().sum()) > 0  # colours moved from their zero start
+        img = render_view(gs, gs.H, gs.W)[0]
+        assert torch.isfinite(img).all()
+
+
 def _serve(reqs, sets, **kw):
     srv = Server(**kw)
     for k, gs in sets.items():
