@@ -94,11 +94,14 @@ int lig_cumsum_tiles(int num_points, const int32_t *num_tiles_hit, int32_t *cum_
                      int32_t *num_intersects, void *workspace, size_t workspace_bytes,
                      void *stream);
 
-/* Workspace bytes needed by lig_bin for `capacity` intersections. */
+/* Workspace bytes needed by lig_bin for `capacity` intersections over
+ * num_tiles tiles (per-tile counters and scan partials). */
 size_t lig_bin_workspace_bytes(int num_points, int capacity, int num_tiles);
 
-/* Key emission + stable LSD radix sort by tile + tile ranges, in one call.
- * Reads the intersection count from the device word *num_intersects and
+/* Binning by tile in one call: per-tile counts of the emitted (Gaussian,
+ * tile) slots, their prefix sum, a scatter of every slot into its tile's
+ * range and a per-tile sort by Gaussian index, which gives the order of the
+ * reference's stable sort of the emitted keys.  Reads the intersection count from the device word *num_intersects and
  * handles at most `capacity` of them; if more exist it sets
  * LIG_STATUS_OVERFLOW in *status (device int32, zeroed by the call) and the
  * outputs are incomplete.  Outputs: gaussian_ids_sorted [capacity],
@@ -308,7 +311,7 @@ int lig_project_bwd_batch(int dtype, int n_img, const int32_t *heights, const in
                           const void *v_xy, int64_t v_xy_stride, const void *v_conic,
                           int64_t v_conic_stride, void *v_in3, void *v_mean2d, void *stream);
 
-/* Emission + stable radix sort + tile ranges over the whole batch (one sort);
+/* lig_bin over the whole batch (one count, scan, scatter and sort);
  * tile_bins has sum_i tiles_i entries.  Workspace: lig_bin_workspace_bytes
  * with the batch's total tile count.  cum / num_intersects as lig_bin (the
  * inclusive prefix sum over the concatenated counts). */

@@ -1,18 +1,21 @@
-// Tile binning: prefix sum of tile counts, key emission, stable LSD radix
-// sort by tile, tile ranges.
+// Tile binning: prefix sum of tile counts, key emission, and the ordering
+// of the emitted (Gaussian, tile) slots by tile.
 //
-// Layout in HBM (workspace of lig_bin): keys0/vals0/keys1 [capacity] u32/i32,
-// radix histogram [bins x blocks] u32, scan partials.  The intersection count
-// lives in a device word written by lig_cumsum_tiles; every kernel here reads
-// it and bounds its work by the caller's capacity, so the whole chain runs
-// without a host round trip (the reference reads it back with .item(),
-// gsplat2d/gsplat2d/utils.py:66).
+// The intersection count lives in a device word written by
+// lig_cumsum_tiles; every kernel here reads it and bounds its work by the
+// caller's capacity, so the whole chain runs without a host round trip (the
+// reference reads it back with .item(), gsplat2d/gsplat2d/utils.py:66).
 //
-// Keys are 32-bit tile ids (the reference's int64 (tile << 32) | depth keys
-// carry depth 0, so only ceil(log2 T) bits hold information).  The sort is a
-// stable LSD radix sort over exactly those bits with <= 10-bit digits, so the
-// order inside a tile is emission order (ascending Gaussian id), which is the
-// order of the reference's stable torch.sort.
+// Ordering (default, LIG_BIN_SCATTER): per-tile counters, their exclusive
+// scan, an atomic scatter of every slot into its tile's range and a per-tile
+// sort by Gaussian index (see "scatter binning" below); workspace: three
+// counters per tile.  Alternative kept for comparison: keys are 32-bit tile
+// ids (the reference's int64 (tile << 32) | depth keys carry depth 0, so only
+// ceil(log2 T) bits hold information) sorted by a stable LSD radix sort over
+// exactly those bits with <= 10-bit digits, then tile ranges from the
+// boundaries; workspace keys0/vals0/keys1 [capacity], histograms.  Both give
+// the order inside a tile of the reference's stable torch.sort: ascending
+// Gaussian id (emission order).
 #include <algorithm>
 #include <atomic>
 #include <mutex>
@@ -436,13 +439,14 @@ __global__ void flag_overflow_kernel(const int32_t *d_total, int capacity, int32
 //      stable sort's order (ascending Gaussian id within a tile, as the
 //      reference's stable torch.sort of (tile << 32) keys in emission
 //      order gives), and tile_bins is written from the counts.
-// The sort key is the Gaussian index; a slot of a Gaussian with extent <= 0
-// (the reference's zero "phantom" slots in the image's first tile) carries
-// bit 31 and is written as the image's first Gaussian id after sorting.
+// The sort key is twice the Gaussian index; a slot of a Gaussian with
+// extent <= 0 (the reference's zero "phantom" slots in the image's first
+// tile, which sort at their Gaussian's emission position) adds 1, and is
+// written as the image's first Gaussian id after sorting.
 #ifndef LIG_BIN_SCATTER
-#define LIG_BIN_SCATTER 0
+#define LIG_BIN_SCATTER 1
 #endif
-constexpr uint32_t kPhantom = 0x80000000u;
+constexpr uint32_t kPhantom = 1u;  // low bit of the sort key (key = 2 g + phantom)
 constexpr int kSegSmem = 2048;     // warp-sorted in shared memory up to this length
 constexpr int kSegWarps = 4;       // warps per CTA of the per-tile sort
 
@@ -519,12 +523,12 @@ __device__ __forceinline__ void for_each_slot(int n, const T *__restrict__ xys,
             continue;
         }
         uint32_t key = o_toff;
-        uint32_t val = (uint32_t)(g0 + owner) | kPhantom;
+        uint32_t val = ((uint32_t)(g0 + owner) << 1) | kPhantom;
         if (o_valid) {
             int q = j / o_bw;
             int r = j - q * o_bw;
             key = o_toff + (uint32_t)(o_y0 + q) * o_tbx + (uint32_t)(o_x0 + r);
-            val = (uint32_t)(g0 + owner);
+            val = (uint32_t)(g0 + owner) << 1;
         }
         f(slot, key, val);
     }
@@ -552,7 +556,7 @@ __global__ void tile_scatter_kernel(int n, const T *__restrict__ xys, const T *_
                          out[tstart[key] + atomicAdd(&tfill[key], 1u)] = val;
                          if (keys64) {  // the reference's emission-order outputs
                              const bool ph = (val & kPhantom) != 0;
-                             const int g = (int)(val & ~kPhantom);
+                             const int g = (int)(val >> 1);
                              const int im = geo.image_of_gauss(g);
                              keys64[slot] = ph ? (int64_t)geo.tile_off[im] << 32
                                                : (int64_t)key << 32;
@@ -563,8 +567,9 @@ __global__ void tile_scatter_kernel(int n, const T *__restrict__ xys, const T *_
 
 // sort value -> Gaussian id (phantom slots: the image's first Gaussian)
 __device__ __forceinline__ int32_t slot_id(uint32_t v, const BatchGeo &geo) {
-    if (!(v & kPhantom)) return (int32_t)v;
-    return geo.g_off[geo.image_of_gauss((int)(v & ~kPhantom))];
+    const int g = (int)(v >> 1);
+    if (!(v & kPhantom)) return (int32_t)g;
+    return geo.g_off[geo.image_of_gauss(g)];
 }
 
 // Bitonic sort of E * 32 values held E per lane (value k of lane l is

@@ -479,60 +479,6 @@ __device__ __forceinline__ double fwd_write(const FwdAcc<T, GA> &acc, bool insid
     return 0.0;
 }
 
-#ifndef LIG_RASTER_FWD_F2
-#define LIG_RASTER_FWD_F2 1  // fused-loss forward (float, 4 pixels per lane): f32x2 pairs
-#endif
-
-// A fused-loss record with every field duplicated into both halves of a
-// pair (mean, halved conic, colour), staged in shared memory so that the
-// lanes' packed operations read their operands with four 16-byte loads.
-struct alignas(16) RecPair {
-    f2 x, y, a, b, c, r, g, bl;
-};
-
-__device__ __forceinline__ RecPair rec_pair(const Rec<float> &q) {
-    return RecPair{f2_dup(q.x), f2_dup(q.y), f2_dup(q.a), f2_dup(q.b),
-                   f2_dup(q.c), f2_dup(q.r), f2_dup(q.g), f2_dup(q.bl)};
-}
-
-// The fused-loss forward's evaluation of one Gaussian at the lane's four
-// pixels (x, y + 4p), p < 4, as two pairs (p = 0, 1 and 2, 3): the column
-// products dx, (a/2) dx, b dx are formed once, already duplicated, and each
-// pair's dy, ((c/2) dy) dy, sigma and colour sums take one packed operation
-// per step.  Roundings are those of the scalar loop (sigma_half's order;
-// colour += colour_channel * alpha as a fused multiply-add), so alphas,
-// final indices and sums are bit-identical to it; a pixel whose alpha test
-// fails adds colour * 0, which leaves its sums unchanged because the staging
-// routes Gaussians with non-finite colours to the scalar loop.
-__device__ __forceinline__ void fused_eval_pairs(const RecPair &q, f2 npx, f2 npy01, f2 npy23,
-                                                 int idx, f2 (&col)[6], int (&cur)[4]) {
-    const f2 DX = f2_add(q.x, npx);
-    const f2 HADX = f2_mul(q.a, DX), BDX = f2_mul(q.b, DX);
-    const f2 DY0 = f2_add(q.y, npy01), DY1 = f2_add(q.y, npy23);
-    const f2 S0 = f2_fma(BDX, DY0, f2_fma(HADX, DX, f2_mul(f2_mul(q.c, DY0), DY0)));
-    const f2 S1 = f2_fma(BDX, DY1, f2_fma(HADX, DX, f2_mul(f2_mul(q.c, DY1), DY1)));
-    float s[4], a[4];
-    f2_unpack(S0, s[0], s[1]);
-    f2_unpack(S1, s[2], s[3]);
-    bool ok[4];
-#pragma unroll
-    for (int p = 0; p < 4; ++p) {
-        a[p] = fminf(0.999f, __expf(-s[p]));
-        ok[p] = !(s[p] < 0.f || a[p] < 1.f / 255.f);
-    }
-    const f2 A0 = f2_pack(ok[0] ? a[0] : 0.f, ok[1] ? a[1] : 0.f);
-    const f2 A1 = f2_pack(ok[2] ? a[2] : 0.f, ok[3] ? a[3] : 0.f);
-    col[0] = f2_fma(q.r, A0, col[0]);
-    col[1] = f2_fma(q.r, A1, col[1]);
-    col[2] = f2_fma(q.g, A0, col[2]);
-    col[3] = f2_fma(q.g, A1, col[3]);
-    col[4] = f2_fma(q.bl, A0, col[4]);
-    col[5] = f2_fma(q.bl, A1, col[5]);
-#pragma unroll
-    for (int p = 0; p < 4; ++p)
-        if (ok[p]) cur[p] = idx;
-}
-
 // PPL pixels per lane: 1 (8x4 regions, two Gaussians per iteration), 2 (8x8
 // regions, lane owns (x, y) and (x, y + 4)) or 4 (8x16, (x, y + 4p)); each
 // Gaussian's record and loop overhead are shared by the lane's evaluations,
@@ -656,78 +602,7 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
     };
     if (!tc.empty) {
         const int2 range = tile_bins[tile];
-        if constexpr (FL && PPL == 4 && LIG_RASTER_FWD_WARPS && LIG_RASTER_FWD_F2 &&
-                      sizeof(T) == 4) {
-            // as the streaming loop below, with records staged as pairs and
-            // the lane's four pixels evaluated as two pairs (fused_eval_pairs)
-            RecPair *w_rp = reinterpret_cast<RecPair *>(s_rec) + w * 32;
-            const f2 npx = f2_dup(-px[0]);
-            const f2 npy01 = f2_pack(-py[0], -py[1]), npy23 = f2_pack(-py[2], -py[3]);
-            f2 col[6];
-            int cur[4] = {0, 0, 0, 0};
-#pragma unroll
-            for (int q = 0; q < 6; ++q) col[q] = f2_zero();
-            Rec<T> pre;
-            if (range.x + lane < range.y) pre = recs[__ldg(ids + range.x + lane)];
-            for (int base = range.x; base < range.y; base += 32) {
-                const bool hit =
-                    base + lane < range.y && region_hit<T, ELL, FL>(pre, R, w, tx0, ty0);
-                const bool finite_col =
-                    isfinite((float)pre.r) && isfinite((float)pre.g) && isfinite((float)pre.bl);
-                __syncwarp();
-                w_rp[lane] = rec_pair(pre);
-                __syncwarp();
-                if (base + 32 + lane < range.y) pre = recs[__ldg(ids + base + 32 + lane)];
-                uint32_t mask = __ballot_sync(FULL, hit);
-                const uint32_t slow = __ballot_sync(FULL, hit && !finite_col);
-                while (mask) {
-                    const int b1 = __ffs(mask) - 1;
-                    mask &= mask - 1;
-                    const RecPair &q = w_rp[b1];
-                    if ((slow >> b1) & 1u) {  // non-finite colour: the scalar loop
-                        float x, y, ha, bb, hc, r, g, bl, t;
-                        f2_unpack(q.x, x, t); f2_unpack(q.y, y, t);
-                        f2_unpack(q.a, ha, t); f2_unpack(q.b, bb, t); f2_unpack(q.c, hc, t);
-                        f2_unpack(q.r, r, t); f2_unpack(q.g, g, t); f2_unpack(q.bl, bl, t);
-                        const float dx = x - px[0];
-                        const float hadx = mul_rn(ha, dx), bdx = mul_rn(bb, dx);
-#pragma unroll
-                        for (int p = 0; p < 4; ++p) {
-                            const float dy = y - py[p];
-                            const float sg =
-                                fma_rn(bdx, dy, fma_rn(hadx, dx, mul_rn(mul_rn(hc, dy), dy)));
-                            const float ap = fminf(0.999f, __expf(-sg));
-                            if (!(sg < 0.f || ap < 1.f / 255.f)) {
-                                float lo, hi;
-                                f2_unpack(col[p >> 1], lo, hi);
-                                if (p & 1) hi += r * ap; else lo += r * ap;
-                                col[p >> 1] = f2_pack(lo, hi);
-                                f2_unpack(col[2 + (p >> 1)], lo, hi);
-                                if (p & 1) hi += g * ap; else lo += g * ap;
-                                col[2 + (p >> 1)] = f2_pack(lo, hi);
-                                f2_unpack(col[4 + (p >> 1)], lo, hi);
-                                if (p & 1) hi += bl * ap; else lo += bl * ap;
-                                col[4 + (p >> 1)] = f2_pack(lo, hi);
-                                cur[p] = base + b1;
-                            }
-                        }
-                    } else {
-                        fused_eval_pairs(q, npx, npy01, npy23, base + b1, col, cur);
-                    }
-                }
-            }
-#pragma unroll
-            for (int p = 0; p < 4; ++p) {
-                float lo, hi;
-                f2_unpack(col[p >> 1], lo, hi);
-                acc[p].r = (p & 1) ? hi : lo;
-                f2_unpack(col[2 + (p >> 1)], lo, hi);
-                acc[p].g = (p & 1) ? hi : lo;
-                f2_unpack(col[4 + (p >> 1)], lo, hi);
-                acc[p].b = (p & 1) ? hi : lo;
-                acc[p].cur = cur[p];
-            }
-        } else if constexpr (LIG_RASTER_FWD_WARPS) {
+        if constexpr (LIG_RASTER_FWD_WARPS) {
             // each warp streams the tile's list in chunks of 32 on its own
             // (its region's test only, no block barriers: warps whose
             // regions have short lists do not wait for the others)
@@ -781,9 +656,6 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
 #ifndef LIG_RASTER_FWD_MINB
 #define LIG_RASTER_FWD_MINB 4
 #endif
-#ifndef LIG_RASTER_FWD_MINB64
-#define LIG_RASTER_FWD_MINB64 12  // 64-thread CTAs of the fused-loss forward (<= 85 registers)
-#endif
 #ifndef LIG_RASTER_BWD_PAIR
 #define LIG_RASTER_BWD_PAIR 1  // lean backward: two pixels per loop iteration (measured faster)
 #endif
@@ -795,7 +667,7 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
 // spilled, more warps to hide latency): measured 4% faster at 8192^2 and
 // 1% at 2048^2, but 14% slower at 512^2 (1024 tiles).
 #ifndef LIG_RASTER_BWD_LEAN_MINB_LARGE
-#define LIG_RASTER_BWD_LEAN_MINB_LARGE 6
+#define LIG_RASTER_BWD_LEAN_MINB_LARGE 5  // with the packed pixel pairs (48 registers)
 #endif
 #ifndef LIG_RASTER_BWD_LARGE_MIN_TILES
 #define LIG_RASTER_BWD_LARGE_MIN_TILES 4096
@@ -1604,24 +1476,16 @@ int raster_fwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
     const bool ppl4 = !ga && geo.total_tiles() >= LIG_RASTER_PPL4_MIN_TILES;
     const bool ppl2 = !ga && !ppl4 && geo.total_tiles() >= LIG_RASTER_PPL2_MIN_TILES;
     const int nt = 32 * Regions::make(ppl4 ? 3 : (ppl2 ? 1 : 0), geo.B).count;
-    // per thread: one record (a pair record in the float fused-loss forward
-    // with four pixels per lane) and one region mask
-    const size_t rec_b = (fl && ppl4 && sizeof(T) == 4 && LIG_RASTER_FWD_F2)
-                             ? sizeof(RecPair) : sizeof(Rec<T>);
-    const size_t sm = (size_t)nt * (rec_b + sizeof(uint32_t));
+    const size_t sm = (size_t)nt * (sizeof(Rec<T>) + sizeof(uint32_t));
     using K = void (*)(const BatchGeo, const int32_t *, int *, const int32_t *, const int2 *,
                        const int32_t *, const Rec<T> *, T *, T *, T *, T *, T *, int32_t *,
                        L2Fwd<T>);
     const bool small = nt <= 256;
     constexpr int FM = LIG_RASTER_FWD_MINB;
-    // the fused-loss forward with four pixels per lane launches 64 threads
-    // per CTA at B = 16: its own instantiation lets it keep more registers
-    constexpr int FM64 = LIG_RASTER_FWD_MINB64;
     K fn = ga ? (small ? raster_fwd_kernel<T, true, 1, 256, FM>
                        : raster_fwd_kernel<T, true, 1, 1024, 1>)
-         : fl ? (ppl4 ? (nt <= 64 ? raster_fwd_kernel<T, false, 4, 64, FM64, true>
-                         : small ? raster_fwd_kernel<T, false, 4, 256, FM, true>
-                                 : raster_fwd_kernel<T, false, 4, 1024, 1, true>)
+         : fl ? (ppl4 ? (small ? raster_fwd_kernel<T, false, 4, 256, FM, true>
+                               : raster_fwd_kernel<T, false, 4, 1024, 1, true>)
                  : ppl2 ? (small ? raster_fwd_kernel<T, false, 2, 256, FM, true>
                                  : raster_fwd_kernel<T, false, 2, 1024, 1, true>)
                         : (small ? raster_fwd_kernel<T, false, 1, 256, FM, true>

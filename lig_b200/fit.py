@@ -145,8 +145,9 @@ def fit_two_level(gt_hwc: torch.Tensor, n1: int, n2: int, iters: int, lr: float 
                   log_every: Optional[int] = None, rgb_init: str = "uniform") -> TwoLevelResult:
     """The LIG level pipeline (train.py:93-158) with the gradient-aware upscale
     between levels: level 1 fits the factor-x downsampled image, its render is
-    upscaled with gradient_aware_upscale, level 2 fits the min-max normalised
-    residual gt - up + 0.5, and the reconstruction is
+    upscaled with gradient_aware_upscale and clamped to [0, 1] (the level
+    estimate of train.py is a clamped render), level 2 fits the min-max
+    normalised residual gt - up + 0.5, and the reconstruction is
     level2 * (max - min) + up - 0.5 + min (train.py:154)."""
     H, W, _ = gt_hwc.shape
     dev = gt_hwc.device
@@ -158,8 +159,12 @@ def fit_two_level(gt_hwc: torch.Tensor, n1: int, n2: int, iters: int, lr: float 
     with torch.no_grad():
         img, _, dx, dy, dxy = lvl1.render(grad_aware=True)
         res.level_psnr.append(psnr(torch.clamp(img, 0, 1), t1))
-        up = gradient_aware_upscale(img, dx, dy, dxy, H, W)
-        res.up_psnr = psnr(torch.clamp(up, 0, 1), gt_hwc)
+        # the level-1 estimate lies in [0, 1] as train.py's im_estim does
+        # (Gaussian2D.forward clamps its render, gaussianlig.py:95); the
+        # spline of an unclamped render can overshoot far outside it and
+        # would stretch the residual's min-max range
+        up = torch.clamp(gradient_aware_upscale(img, dx, dy, dxy, H, W), 0, 1)
+        res.up_psnr = psnr(up, gt_hwc)
         resid = gt_hwc - up + 0.5
         lo, hi = resid.min(), resid.max()
         t2 = ((resid - lo) / (hi - lo)).contiguous()

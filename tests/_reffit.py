@@ -75,8 +75,8 @@ def ref_two_level(gt, n1, n2, iters, lr=1e-3, factor=4, diag=(0.5, 6.0), rgb_ini
     with torch.no_grad():
         r = lvl1.render(grad_aware=True)
         p1 = psnr(torch.clamp(r["img"], 0, 1), t1)
-        up = ref.upscale_fwd(r["img"], r["dx"], r["dy"], r["dxy"], H, W)
-        pu = psnr(torch.clamp(up, 0, 1), gt)
+        up = torch.clamp(ref.upscale_fwd(r["img"], r["dx"], r["dy"], r["dxy"], H, W), 0, 1)
+        pu = psnr(up, gt)
         resid = gt - up + 0.5
         lo, hi = resid.min(), resid.max()
         t2 = ((resid - lo) / (hi - lo)).contiguous()
