@@ -933,12 +933,21 @@ struct alignas(16) PixPair {
 // ((c/2) dy) dy)), alpha = min(clamp, exp(-sigma)) and the same alpha test —
 // so the alpha decisions are bit-identical; only the order in which the
 // moment and colour sums are added differs.  Same outputs in acc[].
-template <int NCP, int CSTEP, int NR>
+// ABS: also the per-pixel absolute values of the mean gradient summed over
+// the pixels (the reference's v_xy_abs, csrc/backward.cu:146-150), in acc[2],
+// acc[3]: per pixel v_sigma (a dx + b dy) and v_sigma (b dx + c dy).
+template <int NCP, int CSTEP, int NR, bool ABS = false>
 __device__ __forceinline__ void lean_region_f2(const Rec<float> &g, float clamp,
                                                const PixPair *__restrict__ pp, int c0, int r0,
                                                float px0, float py0, float (&acc)[11]) {
     const float ha = 0.5f * g.a, hc = 0.5f * g.c;
     const f2 HA = f2_dup(ha), BB = f2_dup(g.b);
+    f2 AA, CC;
+    float ax = 0.f, ay = 0.f;
+    if constexpr (ABS) {
+        AA = f2_dup(g.a);
+        CC = f2_dup(g.c);
+    }
     const f2 CR = f2_dup(g.r), CG = f2_dup(g.g), CB = f2_dup(g.bl);
     f2 DY[NR], CDD[NR];
 #pragma unroll
@@ -954,6 +963,8 @@ __device__ __forceinline__ void lean_region_f2(const Rec<float> &g, float clamp,
         const int cp = c0 + k * CSTEP;
         const f2 DX = f2_pack(g.x - (px0 + (float)cp), g.x - (px0 + (float)(cp + 4)));
         const f2 HADX = f2_mul(HA, DX), BDX = f2_mul(BB, DX);
+        f2 AX;
+        if constexpr (ABS) AX = f2_mul(AA, DX);
         f2 wc = f2_zero(), yc = f2_zero();
 #pragma unroll
         for (int r = 0; r < NR; ++r) {
@@ -977,6 +988,13 @@ __device__ __forceinline__ void lean_region_f2(const Rec<float> &g, float clamp,
             const f2 TY = f2_mul(WV, DY[r]);
             yc = f2_add(yc, TY);
             syy = f2_fma(TY, DY[r], syy);
+            if constexpr (ABS) {
+                float gx0, gx1, gy0, gy1;
+                f2_unpack(f2_mul(WV, f2_fma(BB, DY[r], AX)), gx0, gx1);
+                f2_unpack(f2_mul(WV, f2_fma(CC, DY[r], BDX)), gy0, gy1);
+                ax += fabsf(gx0) + fabsf(gx1);
+                ay += fabsf(gy0) + fabsf(gy1);
+            }
         }
         const f2 TX = f2_mul(wc, DX);
         sx = f2_add(sx, TX);
@@ -987,13 +1005,17 @@ __device__ __forceinline__ void lean_region_f2(const Rec<float> &g, float clamp,
     acc[0] = -f2_sum(sx); acc[1] = -f2_sum(sy);
     acc[4] = -f2_sum(sxx); acc[5] = -f2_sum(sxy); acc[6] = -f2_sum(syy);
     acc[7] = f2_sum(sr); acc[8] = f2_sum(sg); acc[9] = f2_sum(sb);
+    if constexpr (ABS) {
+        acc[2] = ax;
+        acc[3] = ay;
+    }
 }
 
 // LEAN (sum backward of the fused fit loss, no opacities, no wsum
 // cotangent): only the gradients the fit needs — v_xy, v_conic, v_rgb — are
 // accumulated (no |v_xy| sums, no opacity gradient) and each (Gaussian,
 // region) pair adds them with two 16-byte atomics into an [N][8] buffer.
-template <typename T, bool GA, bool LEAN>
+template <typename T, bool GA, bool LEAN, bool ABS = false>
 __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
                                          const int32_t *__restrict__ ids,
                                          const int2 *__restrict__ tile_bins,
@@ -1005,6 +1027,7 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
     using M = Math<T>;
     // float lean backward: pixel pairs in f32x2 arithmetic (lean_region_f2)
     constexpr bool kPairs = LEAN && !GA && LIG_RASTER_BWD_F2 && sizeof(T) == 4;
+    static_assert(!ABS || kPairs, "the |v_xy| sums of the lean walk need its pair form");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nt = blockDim.x;  // = 32 * regions: region-major pixel slots
     PixRec<T, GA> *s_pix = reinterpret_cast<PixRec<T, GA> *>(smem_raw);
@@ -1136,12 +1159,18 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
                 const PixPair *pp = reinterpret_cast<const PixPair *>(smem_raw) + w * 16;
                 if (act) {
                     switch (lsplit) {
-                    case 0: lean_region_f2<4, 1, 4>(g, clamp, pp, 0, 0, px0, py0, acc); break;
-                    case 1: lean_region_f2<2, 2, 4>(g, clamp, pp, part, 0, px0, py0, acc); break;
-                    case 2: lean_region_f2<1, 1, 4>(g, clamp, pp, part, 0, px0, py0, acc); break;
+                    case 0:
+                        lean_region_f2<4, 1, 4, ABS>(g, clamp, pp, 0, 0, px0, py0, acc);
+                        break;
+                    case 1:
+                        lean_region_f2<2, 2, 4, ABS>(g, clamp, pp, part, 0, px0, py0, acc);
+                        break;
+                    case 2:
+                        lean_region_f2<1, 1, 4, ABS>(g, clamp, pp, part, 0, px0, py0, acc);
+                        break;
                     default:
-                        lean_region_f2<1, 1, 2>(g, clamp, pp, part & 3, 2 * (part >> 2), px0,
-                                                py0, acc);
+                        lean_region_f2<1, 1, 2, ABS>(g, clamp, pp, part & 3, 2 * (part >> 2),
+                                                     px0, py0, acc);
                         break;
                     }
                 }
@@ -1285,7 +1314,7 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
             for (int o = 1; o < (1 << lsplit); o <<= 1) {  // combine the lane group
 #pragma unroll
                 for (int q = 0; q < 11; ++q) {
-                    if (LEAN && (q == 2 || q == 3 || q == 10)) continue;
+                    if (LEAN && (q == 10 || (!ABS && (q == 2 || q == 3)))) continue;
                     acc[q] += __shfl_xor_sync(FULL, acc[q], o);
                 }
                 touched = __shfl_xor_sync(FULL, (int)touched, o) || touched;
@@ -1303,7 +1332,13 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
                     acc[2] = M::abs_(acc[0]);
                     acc[3] = M::abs_(acc[1]);
                 }
-                if constexpr (LEAN) {
+                if constexpr (LEAN && ABS) {
+                    // the general [N][12] layout, no opacity gradient
+                    float4 *d4 = reinterpret_cast<float4 *>(packed + (size_t)s_ids[slot] * 12);
+                    atomicAdd(d4, make_float4(acc[0], acc[1], acc[2], acc[3]));
+                    atomicAdd(d4 + 1, make_float4(acc[4], acc[5], acc[6], acc[7]));
+                    atomicAdd(d4 + 2, make_float4(acc[8], acc[9], 0.f, 0.f));
+                } else if constexpr (LEAN) {
                     // [xy, conic, rgb]
                     T *dst = packed + (size_t)s_ids[slot] * 8;
                     if constexpr (sizeof(T) == 4) {
@@ -1333,7 +1368,7 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
     }
 }
 
-template <typename T, bool GA, bool LEAN, int MAXT, int MINB>
+template <typename T, bool GA, bool LEAN, int MAXT, int MINB, bool ABS = false>
 __global__ void __launch_bounds__(MAXT, MINB)
 raster_bwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work,
                   const int32_t *__restrict__ ids, const int2 *__restrict__ tile_bins,
@@ -1346,7 +1381,7 @@ raster_bwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work
     for (int tile = next_tile(work, s_slot, true); tile < n_tiles;
          tile = next_tile(work, s_slot, false)) {
         const TileCtx tc = tile_ctx(geo, cum, d_total, tile);
-        bwd_tile<T, GA, LEAN>(tc, tile, ids, tile_bins, recs, final_idx, cot, v_dx, v_dy, v_dxy,
+        bwd_tile<T, GA, LEAN, ABS>(tc, tile, ids, tile_bins, recs, final_idx, cot, v_dx, v_dy, v_dxy,
                               clamp, packed, s_end);
     }
 }
@@ -1541,6 +1576,11 @@ int raster_bwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
     // the fused-loss backward without opacities needs neither |v_xy| nor an
     // opacity gradient (nor a wsum cotangent)
     const bool lean = !ga && !cot.v_img && !cot.v_wsum && !op && !v_op;
+    // an explicit image cotangent without wsum cotangent or opacities (the
+    // drop-in API under autograd, LIG's own training loop): the same lean
+    // walk plus the per-pixel |v_xy| sums the reference returns (float)
+    const bool lean_abs = !ga && cot.v_img && !cot.v_wsum && !op && !v_op &&
+                          sizeof(T) == 4 && LIG_RASTER_BWD_F2;
     const int stride = lean ? 8 : 12;
     T *packed = reinterpret_cast<T *>((char *)ws + goff);
     cudaMemsetAsync(packed, 0, sizeof(T) * stride * (size_t)n, s);
@@ -1556,8 +1596,15 @@ int raster_bwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
                        const int32_t *, const Rec<T> *, const int32_t *, CotSrc<T>, const T *,
                        const T *, const T *, T, T *);
     const bool small = nt <= 256;
+    constexpr bool kAbs = sizeof(T) == 4 && LIG_RASTER_BWD_F2;
+    const bool large = geo.total_tiles() >= LIG_RASTER_BWD_LARGE_MIN_TILES;
     K fn = ga ? (small ? raster_bwd_kernel<T, true, false, 256, LIG_RASTER_BWD_MINB>
                        : raster_bwd_kernel<T, true, false, 1024, 1>)
+         : lean_abs ? (small ? (large ? raster_bwd_kernel<T, false, true, 256,
+                                                          LIG_RASTER_BWD_LEAN_MINB_LARGE, kAbs>
+                                      : raster_bwd_kernel<T, false, true, 256,
+                                                          LIG_RASTER_BWD_LEAN_MINB, kAbs>)
+                             : raster_bwd_kernel<T, false, true, 1024, 1, kAbs>)
               : lean ? (small ? (geo.total_tiles() >= LIG_RASTER_BWD_LARGE_MIN_TILES
                                      ? raster_bwd_kernel<T, false, true, 256,
                                                          LIG_RASTER_BWD_LEAN_MINB_LARGE>

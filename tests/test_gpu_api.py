@@ -167,6 +167,33 @@ def test_single_channel_upscaler_is_one_channel_of_the_rgb_form(dtype):
     assert torch.equal(o1[..., 0], o3[..., 1])
 
 
+@pytest.mark.parametrize("H,W,B,n", [(150, 170, 16, 3000),
+                                     (1040, 1100, 16, 20000),  # >= 4096 tiles
+                                     (97, 203, 12, 2500)])
+def test_dropin_backward_image_loss_matches_reference(H, W, B, n):
+    """The drop-in backward for an image-only loss without opacities (LIG's
+    own training loop, gaussianlig.py:70-111) runs the lean walk with the
+    per-pixel |v_xy| sums: v_xy, xys.absgrad, v_conic and v_rgb against the
+    reference kernel fed the same cotangent (1e-4 relative)."""
+    means, L, colors, _ = scene(n, H, W, diag=(0.5, 5.0), seed=19)
+    g = torch.Generator().manual_seed(20)
+    w = torch.randn(H, W, 3, generator=g).cuda()
+    xys, ext, con, cnt = gsplat2d.project_gaussians_cholesky(L, means, H, W, B)
+    xys = xys.detach().requires_grad_()
+    con = con.detach().requires_grad_()
+    col = colors.clone().requires_grad_()
+    img = gsplat2d.rasterize_gaussians(xys, ext, con, cnt, col, None, H, W, B)[0]
+    (img * w).sum().backward()
+    rb = ref.bin_and_sort(xys.detach(), ext, cnt, H, W, B)
+    rf = ref.raster_fwd(H, W, B, rb, xys.detach(), con.detach(), colors, None)
+    gr = ref.raster_bwd(H, W, B, rb, xys.detach(), con.detach(), colors, None,
+                        rf["final_idx"], w, torch.zeros(H, W, device="cuda"))
+    assert rel_err(np_(xys.grad), np_(gr["v_xy"])) <= 1e-4
+    assert rel_err(np_(xys.absgrad), np_(gr["v_xy_abs"])) <= 1e-4
+    assert rel_err(np_(con.grad), np_(gr["v_conic"])) <= 1e-4
+    assert rel_err(np_(col.grad), np_(gr["v_rgb"])) <= 1e-4
+
+
 def test_lig_training_step_decreases_loss():
     H, W, B, n = 96, 96, 16, 2000
     means, L, colors, _ = scene(n, H, W, diag=(0.5, 3.0), seed=2)
