@@ -447,7 +447,7 @@ __global__ void flag_overflow_kernel(const int32_t *d_total, int capacity, int32
 #define LIG_BIN_SCATTER 1
 #endif
 constexpr uint32_t kPhantom = 1u;  // low bit of the sort key (key = 2 g + phantom)
-constexpr int kSegSmem = 2048;     // warp-sorted in shared memory up to this length
+constexpr int kSegSmem = 4096;     // sorted in shared memory up to this length (long tiles)
 constexpr int kSegWarps = 4;       // warps per CTA of the per-tile sort
 
 // The emission enumeration of emit_kernel, calling f(slot, key, sort_value)
@@ -627,44 +627,17 @@ __device__ __forceinline__ void sort_segment_regs(uint32_t *seg, int L, int32_t 
     }
 }
 
-// Bitonic sort of a segment of length L <= kSegSmem by one warp in shared
-// memory (padded to a power of two with the largest value).
-__device__ void sort_segment_smem(const uint32_t *seg, int L, int32_t *dst, uint32_t *buf,
-                                  const BatchGeo &geo) {
-    const int lane = threadIdx.x & 31;
-    int P = 1;
-    while (P < L) P <<= 1;
-    for (int i = lane; i < P; i += 32) buf[i] = i < L ? seg[i] : 0xffffffffu;
-    __syncwarp();
-    for (int size = 2; size <= P; size <<= 1) {
-        for (int j = size >> 1; j > 0; j >>= 1) {
-            for (int t = lane; t < P / 2; t += 32) {
-                const int i = 2 * t - (t & (j - 1));   // lower index of pair t
-                const int k = i + j;
-                const bool asc = (i & size) == 0;
-                const uint32_t a = buf[i], b = buf[k];
-                if (asc ? (a > b) : (a < b)) {
-                    buf[i] = b;
-                    buf[k] = a;
-                }
-            }
-            __syncwarp();
-        }
-    }
-    for (int i = lane; i < L; i += 32) dst[i] = slot_id(buf[i], geo);
-    __syncwarp();
-}
-
 // 4. one warp per tile: sort its entries (from `vals`, written to `ids` as
 // Gaussian ids), write tile_bins ((0, 0) for an empty tile, as the
 // reference's zero-initialised edges) and, when asked, the sorted 64-bit
-// keys.  Tiles longer than kSegSmem are queued for sort_long_kernel.
+// keys.  Tiles of up to 256 entries are sorted in registers; longer ones are
+// queued for tile_sort_long_kernel (no shared memory here, so that the
+// common short tiles run at full occupancy).
 __global__ void __launch_bounds__(32 * kSegWarps)
 tile_sort_kernel(BatchGeo geo, const uint32_t *__restrict__ tcount,
                  const uint32_t *__restrict__ tstart, int capacity, uint32_t *__restrict__ vals,
                  int32_t *__restrict__ ids, int2 *__restrict__ tile_bins,
                  int64_t *__restrict__ isect_sorted, int32_t *__restrict__ long_list) {
-    __shared__ uint32_t s_buf[kSegWarps][kSegSmem];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int T = geo.total_tiles();
     const int nwarps = gridDim.x * kSegWarps;
@@ -683,33 +656,40 @@ tile_sort_kernel(BatchGeo geo, const uint32_t *__restrict__ tcount,
         else if (L <= 64) sort_segment_regs<2>(seg, L, dst, geo);
         else if (L <= 128) sort_segment_regs<4>(seg, L, dst, geo);
         else if (L <= 256) sort_segment_regs<8>(seg, L, dst, geo);
-        else if (L <= kSegSmem) sort_segment_smem(seg, L, dst, s_buf[w], geo);
         else if (lane == 0) long_list[1 + atomicAdd(long_list, 1)] = t;
     }
 }
 
-// Tiles with more than kSegSmem entries: one CTA per tile sorts the segment
-// in place in global memory, then converts it to ids.  The network is the
+// Tiles with more than 256 entries: one CTA per tile.  Up to kSegSmem
+// entries are sorted in shared memory (bitonic, padded to a power of two
+// with the largest key); longer segments in place in global memory with the
 // bitonic sort written with ascending comparators only (each merge starts by
 // comparing mirrored positions of its block, then half-cleaners), so the
-// padding up to a power of two (conceptually the largest value, always at
-// the higher index of a comparator) never moves and is not stored: every
-// comparator that reaches past the segment is skipped.  Rare (thousands of
-// Gaussians over one tile).
-__global__ void __launch_bounds__(1024)
+// padding up to a power of two (conceptually the largest key, always at the
+// higher index of a comparator) never moves and is not stored: every
+// comparator that reaches past the segment is skipped.
+constexpr int kLongThreads = 256;
+__global__ void __launch_bounds__(kLongThreads)
 tile_sort_long_kernel(BatchGeo geo, const uint32_t *__restrict__ tcount,
                       const uint32_t *__restrict__ tstart, int capacity,
                       uint32_t *__restrict__ vals, int32_t *__restrict__ ids,
                       const int32_t *__restrict__ long_list) {
+    __shared__ uint32_t s_buf[kSegSmem];
     const int nlong = long_list[0];
     for (int q = blockIdx.x; q < nlong; q += gridDim.x) {
         const int t = long_list[1 + q];
         const int a = (int)min((uint32_t)capacity, tstart[t]);
         const int b = (int)min((uint32_t)capacity, tstart[t] + tcount[t]);
         const int L = b - a;
-        uint32_t *seg = vals + a;
         int P = 1;
         while (P < L) P <<= 1;
+        const bool smem = P <= kSegSmem;
+        uint32_t *seg = smem ? s_buf : vals + a;
+        if (smem)
+            for (int i = threadIdx.x; i < P; i += blockDim.x)
+                s_buf[i] = i < L ? vals[a + i] : 0xffffffffu;
+        __syncthreads();
+        const int n = smem ? P : L;  // elements that exist
         for (int size = 2; size <= P; size <<= 1) {
             for (int j = size >> 1; j > 0; j >>= 1) {
                 for (int p = threadIdx.x; p < P / 2; p += blockDim.x) {
@@ -722,7 +702,7 @@ tile_sort_long_kernel(BatchGeo geo, const uint32_t *__restrict__ tcount,
                         i = 2 * p - (p & (j - 1));
                         k = i + j;
                     }
-                    if (k >= L) continue;
+                    if (k >= n) continue;
                     const uint32_t x = seg[i], y = seg[k];
                     if (x > y) {
                         seg[i] = y;
@@ -831,8 +811,8 @@ int run_bin_scatter(const BatchGeo &geo, const void *xys, const void *ext, const
     tile_sort_kernel<<<sort_blocks, 32 * kSegWarps, 0, s>>>(geo, tcount, tstart, capacity, vals,
                                                           gid_sorted, (int2 *)tile_bins,
                                                           isect_sorted, long_list);
-    tile_sort_long_kernel<<<148, 1024, 0, s>>>(geo, tcount, tstart, capacity, vals, gid_sorted,
-                                               long_list);
+    tile_sort_long_kernel<<<148 * 4, kLongThreads, 0, s>>>(geo, tcount, tstart, capacity, vals,
+                                                           gid_sorted, long_list);
     note_launches(3);
     LIG_LAUNCH_CHECK();
     return LIG_OK;

@@ -1047,8 +1047,21 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
     uint16_t *my_list = s_list + w * nt;
     const PixRec<T, GA> *my_pix = s_pix + w * 32;
 
+    const int2 range = tile_bins[tile];
+    int end = range.y;
+    Rec<T> pre;
+    int pre_id = -1;
+    if constexpr (LEAN) {
+        // the lean walk has no final-index test (see lean_region), so the list
+        // is not cut at the tile's last final index: the first batch's gather
+        // is issued before the pixels are staged and no barrier precedes it
+        if (range.x + tid < end) {
+            pre_id = __ldg(ids + range.x + tid);
+            pre = recs[pre_id];
+        }
+    }
     // stage this thread's pixel (region w, slot lane)
-    if (tid == 0) s_end = -1;
+    if (!LEAN && tid == 0) s_end = -1;
     {
         int lx, ly;
         R.pixel(w, lane, 0, lx, ly);
@@ -1060,7 +1073,7 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
         c.py = (T)gy + (T)0.5;
         c.vo0 = c.vo1 = c.vo2 = c.vw = (T)0;
         if (inside) cot.get(p, c.vo0, c.vo1, c.vo2, c.vw);
-        c.fin = inside ? final_idx[p] : -1;  // -1: never valid
+        c.fin = (!LEAN && inside) ? final_idx[p] : -1;  // -1: never valid (unread when lean)
         if constexpr (GA) {
 #pragma unroll
             for (int ch = 0; ch < 3; ++ch) {
@@ -1081,21 +1094,22 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
         } else {
             s_pix[tid] = c;
         }
-        int my_max = c.fin;
+        if constexpr (!LEAN) {
+            int my_max = c.fin;
 #pragma unroll
-        for (int o = 16; o >= 1; o >>= 1) my_max = max(my_max, __shfl_xor_sync(FULL, my_max, o));
-        __syncthreads();
-        if (lane == 0) atomicMax(&s_end, my_max);
+            for (int o = 16; o >= 1; o >>= 1)
+                my_max = max(my_max, __shfl_xor_sync(FULL, my_max, o));
+            __syncthreads();
+            if (lane == 0) atomicMax(&s_end, my_max);
+        }
     }
-    __syncthreads();
-    const int2 range = tile_bins[tile];
-    const int end = min(range.y, s_end + 1);
-
-    Rec<T> pre;
-    int pre_id = -1;
-    if (range.x + tid < end) {
-        pre_id = __ldg(ids + range.x + tid);
-        pre = recs[pre_id];
+    if constexpr (!LEAN) {
+        __syncthreads();
+        end = min(range.y, s_end + 1);
+        if (range.x + tid < end) {
+            pre_id = __ldg(ids + range.x + tid);
+            pre = recs[pre_id];
+        }
     }
     for (int base = range.x; base < end; base += nt) {
         const int cnt = min(nt, end - base);
