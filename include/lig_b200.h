@@ -217,6 +217,13 @@ size_t lig_l2_workspace_bytes(void);
 int lig_l2_clamped_loss(int dtype, int64_t n, const void *img, const void *target, void *loss,
                         void *workspace, size_t workspace_bytes, void *stream);
 
+/* Bounded device-side waits that gave up on the current device since the
+ * library loaded (the backward's optional bulk-copy staging polls an
+ * mbarrier with an iteration limit and abandons the tile rather than hang);
+ * 0 in normal operation, -1 if the query itself failed.  No counterpart in
+ * the reference (its kernels have no device-side waits). */
+int lig_wait_timeouts(void);
+
 /* Sum rasterizer forward that allocates nothing.  No counterpart in the
  * reference.  For callers that cannot allocate device memory when they render
  * (e.g. a plugin running inside a framework that has reserved nearly all GPU

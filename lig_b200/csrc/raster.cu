@@ -1011,6 +1011,53 @@ __device__ __forceinline__ void lean_region_f2(const Rec<float> &g, float clamp,
     }
 }
 
+#ifndef LIG_RASTER_BWD_BULK
+#define LIG_RASTER_BWD_BULK 0  // lean backward (float): records staged by bulk async copies
+#endif
+// Bounded device waits that gave up (a malfunction; read by lig_wait_timeouts).
+__device__ unsigned int g_wait_timeouts;
+constexpr int kWaitLimit = 1 << 22;  // mbarrier polls before a wait is abandoned
+
+// Bulk asynchronous copies of gathered 48-byte records into shared memory,
+// completing on one mbarrier per CTA (cp.async.bulk, this GPU's memory only,
+// no multicast).  Thread 0 announces the batch's bytes; each thread < cnt
+// copies its record.  The transaction count may be completed before it is
+// announced (its range includes negative values), so no barrier is needed
+// between the two.
+__device__ __forceinline__ void bulk_records(uint32_t bar, Rec<float> *s_rec, int32_t *s_ids,
+                                             const int32_t *__restrict__ ids,
+                                             const Rec<float> *__restrict__ recs, int base,
+                                             int cnt) {
+    const int tid = threadIdx.x;
+    if (tid == 0)
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                     "r"(cnt * (int)sizeof(Rec<float>))
+                     : "memory");
+    if (tid < cnt) {
+        const int id = __ldg(ids + base + tid);
+        s_ids[tid] = id;
+        const uint32_t dst = (uint32_t)__cvta_generic_to_shared(s_rec + tid);
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+            "[%3];" ::"r"(dst),
+            "l"(recs + id), "r"((int)sizeof(Rec<float>)), "r"(bar)
+            : "memory");
+    }
+}
+
+// Wait for the mbarrier's current phase with at most kWaitLimit polls.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
+    uint32_t done = 0;
+    for (int it = 0; it < kWaitLimit && !done; ++it)
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; "
+            "selp.u32 %0, 1, 0, p; }"
+            : "=r"(done)
+            : "r"(bar), "r"(phase)
+            : "memory");
+    return done != 0;
+}
+
 // LEAN (sum backward of the fused fit loss, no opacities, no wsum
 // cotangent): only the gradients the fit needs — v_xy, v_conic, v_rgb — are
 // accumulated (no |v_xy| sums, no opacity gradient) and each (Gaussian,
@@ -1023,11 +1070,15 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
                                          const int32_t *__restrict__ final_idx, CotSrc<T> cot,
                                          const T *__restrict__ v_dx, const T *__restrict__ v_dy,
                                          const T *__restrict__ v_dxy, T clamp,
-                                         T *__restrict__ packed, int &s_end) {
+                                         T *__restrict__ packed, int &s_end, uint32_t bar,
+                                         uint32_t &phase) {
     using M = Math<T>;
     // float lean backward: pixel pairs in f32x2 arithmetic (lean_region_f2)
     constexpr bool kPairs = LEAN && !GA && LIG_RASTER_BWD_F2 && sizeof(T) == 4;
     static_assert(!ABS || kPairs, "the |v_xy| sums of the lean walk need its pair form");
+    // records staged by bulk async copies (no register prefetch, no region
+    // masks: the warps test the box and ellipse themselves)
+    constexpr bool kBulk = kPairs && LIG_RASTER_BWD_BULK;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nt = blockDim.x;  // = 32 * regions: region-major pixel slots
     PixRec<T, GA> *s_pix = reinterpret_cast<PixRec<T, GA> *>(smem_raw);
@@ -1051,7 +1102,13 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
     int end = range.y;
     Rec<T> pre;
     int pre_id = -1;
-    if constexpr (LEAN) {
+    if constexpr (kBulk) {
+        // first batch in flight while the pixels are staged
+        if (range.x < end)
+            bulk_records(bar, reinterpret_cast<Rec<float> *>(s_rec), s_ids, ids,
+                         reinterpret_cast<const Rec<float> *>(recs), range.x,
+                         min(nt, end - range.x));
+    } else if constexpr (LEAN) {
         // the lean walk has no final-index test (see lean_region), so the list
         // is not cut at the tile's last final index: the first batch's gather
         // is issued before the pixels are staged and no barrier precedes it
@@ -1113,22 +1170,41 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
     }
     for (int base = range.x; base < end; base += nt) {
         const int cnt = min(nt, end - base);
-        __syncthreads();
-        if (tid < cnt) {
-            s_rec[tid] = pre;
-            s_bits[tid] = region_bits<T, !LIG_RASTER_BWD_LANE_ELLIPSE>(pre, R, tx0, ty0);
-            s_ids[tid] = pre_id;
-        }
-        __syncthreads();
-        if (base + nt + tid < end) {
-            pre_id = __ldg(ids + base + nt + tid);
-            pre = recs[pre_id];
+        if constexpr (kBulk) {
+            if (base != range.x) {  // everyone is done with the previous batch
+                __syncthreads();
+                bulk_records(bar, reinterpret_cast<Rec<float> *>(s_rec), s_ids, ids,
+                             reinterpret_cast<const Rec<float> *>(recs), base, cnt);
+            }
+            const bool ok = mbar_wait(bar, phase);
+            phase ^= 1u;
+            // all threads agree: a wait that gave up counts once, then every
+            // thread lets its copies drain (bounded) and the tile is abandoned
+            if (__syncthreads_or(!ok)) {
+                if (tid == 0) atomicAdd(&g_wait_timeouts, 1u);
+                (void)mbar_wait(bar, phase ^ 1u);
+                return;
+            }
+        } else {
+            __syncthreads();
+            if (tid < cnt) {
+                s_rec[tid] = pre;
+                s_bits[tid] = region_bits<T, !LIG_RASTER_BWD_LANE_ELLIPSE>(pre, R, tx0, ty0);
+                s_ids[tid] = pre_id;
+            }
+            __syncthreads();
+            if (base + nt + tid < end) {
+                pre_id = __ldg(ids + base + nt + tid);
+                pre = recs[pre_id];
+            }
         }
         // compact the batch slots touching this region (ascending)
         int nmine = 0;
         for (int m = 0; m * 32 < cnt; ++m) {
             const int t = m * 32 + lane;
-            bool hit = t < cnt && ((s_bits[t] >> w) & 1u);
+            bool hit;
+            if constexpr (kBulk) hit = t < cnt && region_hit<T, false, false>(s_rec[t], R, w, tx0, ty0);
+            else hit = t < cnt && ((s_bits[t] >> w) & 1u);
             if (LIG_RASTER_BWD_LANE_ELLIPSE && hit) {
                 // exact ellipse test of Gaussian t against this warp's region,
                 // one Gaussian per lane (the staging only tested the box)
@@ -1391,12 +1467,22 @@ raster_bwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work
                   const T *__restrict__ v_dx, const T *__restrict__ v_dy,
                   const T *__restrict__ v_dxy, T clamp, T *__restrict__ packed) {
     __shared__ int s_end, s_slot;
+    __shared__ __align__(8) unsigned long long s_mbar;
+    const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&s_mbar);
+    uint32_t phase = 0;
+    if (LIG_RASTER_BWD_BULK && LEAN && !GA && sizeof(T) == 4) {
+        if (threadIdx.x == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(1));
+            asm volatile("fence.mbarrier_init.release.cluster;");
+        }
+        __syncthreads();
+    }
     const int n_tiles = geo.total_tiles();
     for (int tile = next_tile(work, s_slot, true); tile < n_tiles;
          tile = next_tile(work, s_slot, false)) {
         const TileCtx tc = tile_ctx(geo, cum, d_total, tile);
-        bwd_tile<T, GA, LEAN, ABS>(tc, tile, ids, tile_bins, recs, final_idx, cot, v_dx, v_dy, v_dxy,
-                              clamp, packed, s_end);
+        bwd_tile<T, GA, LEAN, ABS>(tc, tile, ids, tile_bins, recs, final_idx, cot, v_dx, v_dy,
+                                   v_dxy, clamp, packed, s_end, bar, phase);
     }
 }
 
@@ -1741,6 +1827,15 @@ extern "C" int lig_raster_bwd_l2(int dtype, int H, int W, int B, int n, const in
                                   v_con, v_rgb, v_op, s);
     }
     return LIG_ERR_INVALID;
+}
+
+// Number of bounded device-side waits (mbarrier polls of the bulk-staged
+// backward) that gave up on the current device since the library loaded;
+// 0 unless a kernel malfunctioned.
+extern "C" int lig_wait_timeouts(void) {
+    unsigned int v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_wait_timeouts, sizeof(v)) != cudaSuccess) return -1;
+    return (int)v;
 }
 
 // ----------------------------------------------------- allocation-free entry

@@ -194,6 +194,20 @@ def test_dropin_backward_image_loss_matches_reference(H, W, B, n):
     assert rel_err(np_(col.grad), np_(gr["v_rgb"])) <= 1e-4
 
 
+def test_no_device_wait_gave_up():
+    """No bounded device-side wait (bulk-staged backward) has timed out in
+    this process (the counter stays 0 in normal operation)."""
+    from lig_b200 import _lib
+    H, W, B, n = 150, 170, 16, 3000
+    means, L, colors, _ = scene(n, H, W, diag=(0.5, 5.0), seed=21)
+    target = torch.rand(H, W, 3, generator=torch.Generator().manual_seed(22)).cuda()
+    from lig_b200.fused import render_l2_loss
+    p = [t.clone().requires_grad_() for t in (means, L, colors)]
+    render_l2_loss(p[1], p[0], p[2], None, target, H, W, B).backward()
+    torch.cuda.synchronize()
+    assert _lib.lib.lig_wait_timeouts() == 0
+
+
 def test_lig_training_step_decreases_loss():
     H, W, B, n = 96, 96, 16, 2000
     means, L, colors, _ = scene(n, H, W, diag=(0.5, 3.0), seed=2)
