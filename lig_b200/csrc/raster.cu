@@ -667,7 +667,7 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
 // spilled, more warps to hide latency): measured 4% faster at 8192^2 and
 // 1% at 2048^2, but 14% slower at 512^2 (1024 tiles).
 #ifndef LIG_RASTER_BWD_LEAN_MINB_LARGE
-#define LIG_RASTER_BWD_LEAN_MINB_LARGE 5  // with the packed pixel pairs (48 registers)
+#define LIG_RASTER_BWD_LEAN_MINB_LARGE 4  // with the packed pixel pairs (64 registers)
 #endif
 #ifndef LIG_RASTER_BWD_LARGE_MIN_TILES
 #define LIG_RASTER_BWD_LARGE_MIN_TILES 4096
