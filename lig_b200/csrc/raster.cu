@@ -656,6 +656,9 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
 #ifndef LIG_RASTER_FWD_MINB
 #define LIG_RASTER_FWD_MINB 4
 #endif
+#ifndef LIG_RASTER_FWD_MINB64
+#define LIG_RASTER_FWD_MINB64 0  // 0: the 256-thread instantiation's budget (64 registers)
+#endif
 #ifndef LIG_RASTER_BWD_PAIR
 #define LIG_RASTER_BWD_PAIR 1  // lean backward: two pixels per loop iteration (measured faster)
 #endif
@@ -667,7 +670,7 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
 // spilled, more warps to hide latency): measured 4% faster at 8192^2 and
 // 1% at 2048^2, but 14% slower at 512^2 (1024 tiles).
 #ifndef LIG_RASTER_BWD_LEAN_MINB_LARGE
-#define LIG_RASTER_BWD_LEAN_MINB_LARGE 4  // with the packed pixel pairs (64 registers)
+#define LIG_RASTER_BWD_LEAN_MINB_LARGE 5  // pairs + bulk-staged records (48 registers)
 #endif
 #ifndef LIG_RASTER_BWD_LARGE_MIN_TILES
 #define LIG_RASTER_BWD_LARGE_MIN_TILES 4096
@@ -1012,7 +1015,7 @@ __device__ __forceinline__ void lean_region_f2(const Rec<float> &g, float clamp,
 }
 
 #ifndef LIG_RASTER_BWD_BULK
-#define LIG_RASTER_BWD_BULK 0  // lean backward (float): records staged by bulk async copies
+#define LIG_RASTER_BWD_BULK 1  // lean backward (float): records staged by bulk async copies
 #endif
 // Bounded device waits that gave up (a malfunction; read by lig_wait_timeouts).
 __device__ unsigned int g_wait_timeouts;
@@ -1617,10 +1620,16 @@ int raster_fwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
                        L2Fwd<T>);
     const bool small = nt <= 256;
     constexpr int FM = LIG_RASTER_FWD_MINB;
+    // the fused-loss forward with four pixels per lane launches 64-thread
+    // CTAs at B = 16; with LIG_RASTER_FWD_MINB64 > 0 it gets an instantiation
+    // asking for that many resident CTAs per SM (its register budget)
+    constexpr int FM64 = LIG_RASTER_FWD_MINB64 > 0 ? LIG_RASTER_FWD_MINB64 : 16;
     K fn = ga ? (small ? raster_fwd_kernel<T, true, 1, 256, FM>
                        : raster_fwd_kernel<T, true, 1, 1024, 1>)
-         : fl ? (ppl4 ? (small ? raster_fwd_kernel<T, false, 4, 256, FM, true>
-                               : raster_fwd_kernel<T, false, 4, 1024, 1, true>)
+         : fl ? (ppl4 ? ((LIG_RASTER_FWD_MINB64 > 0 && nt <= 64)
+                             ? raster_fwd_kernel<T, false, 4, 64, FM64, true>
+                         : small ? raster_fwd_kernel<T, false, 4, 256, FM, true>
+                                 : raster_fwd_kernel<T, false, 4, 1024, 1, true>)
                  : ppl2 ? (small ? raster_fwd_kernel<T, false, 2, 256, FM, true>
                                  : raster_fwd_kernel<T, false, 2, 1024, 1, true>)
                         : (small ? raster_fwd_kernel<T, false, 1, 256, FM, true>
