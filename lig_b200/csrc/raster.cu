@@ -101,6 +101,72 @@ __global__ void pack_kernel(int n, const T *__restrict__ xys, const T *__restric
     recs[i] = r;
 }
 
+// Bounded device waits that gave up (a malfunction; read by lig_wait_timeouts).
+__device__ unsigned int g_wait_timeouts;
+constexpr int kWaitLimit = 1 << 22;  // mbarrier polls before a wait is abandoned
+
+// Bulk asynchronous copies of gathered 48-byte records into shared memory,
+// completing on one mbarrier per CTA (cp.async.bulk, this GPU's memory only,
+// no multicast).  Thread 0 announces the batch's bytes; each thread < cnt
+// copies its record.  The transaction count may be completed before it is
+// announced (its range includes negative values), so no barrier is needed
+// between the two.
+__device__ __forceinline__ void bulk_records(uint32_t bar, Rec<float> *s_rec, int32_t *s_ids,
+                                             const int32_t *__restrict__ ids,
+                                             const Rec<float> *__restrict__ recs, int base,
+                                             int cnt) {
+    const int tid = threadIdx.x;
+    if (tid == 0)
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                     "r"(cnt * (int)sizeof(Rec<float>))
+                     : "memory");
+    if (tid < cnt) {
+        const int id = __ldg(ids + base + tid);
+        s_ids[tid] = id;
+        const uint32_t dst = (uint32_t)__cvta_generic_to_shared(s_rec + tid);
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+            "[%3];" ::"r"(dst),
+            "l"(recs + id), "r"((int)sizeof(Rec<float>)), "r"(bar)
+            : "memory");
+    }
+}
+
+// Wait for the mbarrier's current phase with at most kWaitLimit polls.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
+    uint32_t done = 0;
+    for (int it = 0; it < kWaitLimit && !done; ++it)
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; "
+            "selp.u32 %0, 1, 0, p; }"
+            : "=r"(done)
+            : "r"(bar), "r"(phase)
+            : "memory");
+    return done != 0;
+}
+
+// One warp's variant: lane 0 announces the chunk's bytes, lanes < cnt copy
+// their record into dst[lane].
+__device__ __forceinline__ void warp_bulk_records(uint32_t bar, Rec<float> *dst,
+                                                  const int32_t *__restrict__ ids,
+                                                  const Rec<float> *__restrict__ recs, int base,
+                                                  int cnt) {
+    const int lane = threadIdx.x & 31;
+    if (lane == 0)
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                     "r"(cnt * (int)sizeof(Rec<float>))
+                     : "memory");
+    if (lane < cnt) {
+        const int id = __ldg(ids + base + lane);
+        const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst + lane);
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+            "[%3];" ::"r"(d),
+            "l"(recs + id), "r"((int)sizeof(Rec<float>)), "r"(bar)
+            : "memory");
+    }
+}
+
 // ---------------------------------------------------------------- regions
 // A tile is split into R <= 32 regions of 32 pixels; warp w of the CTA owns
 // region w and each lane owns PPL pixels of it.
@@ -310,6 +376,9 @@ __device__ __forceinline__ int next_tile(int *work, int &s_slot, bool first) {
 #ifndef LIG_RASTER_FWD_FUSED
 #define LIG_RASTER_FWD_FUSED 1  // specialised fused-loss forward (no opacities)
 #endif
+#ifndef LIG_RASTER_FWD_BULK
+#define LIG_RASTER_FWD_BULK 0  // fused-loss forward (float): records staged by bulk copies
+#endif
 // One CTA per tile, warp w = region w (8x4 pixels), one pixel per lane.
 // Batches of blockDim Gaussians (list order) are staged in shared memory, one
 // record per thread, with the next batch's record fetched into registers
@@ -493,7 +562,8 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
                                          T *__restrict__ wsum, T *__restrict__ odx,
                                          T *__restrict__ ody, T *__restrict__ odxy,
                                          int32_t *__restrict__ final_idx, Rec<T> *s_rec,
-                                         uint32_t *s_bits, const L2Fwd<T> &l2) {
+                                         uint32_t *s_bits, const L2Fwd<T> &l2, uint32_t fbar,
+                                         uint32_t &fphase) {
     const unsigned FULL = 0xffffffffu;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int B = tc.B, tx0 = tc.tx0, ty0 = tc.ty0;
@@ -602,7 +672,44 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
     };
     if (!tc.empty) {
         const int2 range = tile_bins[tile];
-        if constexpr (LIG_RASTER_FWD_WARPS) {
+        if constexpr (FL && PPL == 4 && LIG_RASTER_FWD_WARPS && LIG_RASTER_FWD_BULK &&
+                      sizeof(T) == 4) {
+            // as below, with each warp's chunks of 32 records staged by bulk
+            // asynchronous copies into two buffers (one mbarrier each), the
+            // next two chunks in flight while one is walked
+            Rec<T> *buf0 = s_rec + w * 64, *buf1 = buf0 + 32;
+            const uint32_t bar0 = fbar + 16u * w, bar1 = bar0 + 8u;
+            const int nch = (range.y - range.x + 31) / 32;
+            auto issue = [&](int k) {
+                const int base = range.x + 32 * k;
+                warp_bulk_records((k & 1) ? bar1 : bar0,
+                                  reinterpret_cast<Rec<float> *>((k & 1) ? buf1 : buf0), ids,
+                                  reinterpret_cast<const Rec<float> *>(recs), base,
+                                  min(32, range.y - base));
+            };
+            if (nch > 0) issue(0);
+            if (nch > 1) issue(1);
+            for (int k = 0; k < nch; ++k) {
+                const int base = range.x + 32 * k, b = k & 1;
+                const uint32_t bar = b ? bar1 : bar0;
+                const bool ok = mbar_wait(bar, (fphase >> b) & 1u);
+                fphase ^= 1u << b;
+                if (__any_sync(FULL, !ok)) {
+                    // a wait gave up: count it, let this warp's copies drain
+                    // (bounded) and leave the rest of its list
+                    if (lane == 0) atomicAdd(&g_wait_timeouts, 1u);
+                    (void)mbar_wait(bar, ((fphase >> b) & 1u) ^ 1u);
+                    if (k + 1 < nch) (void)mbar_wait(b ? bar0 : bar1, (fphase >> (b ^ 1)) & 1u);
+                    break;
+                }
+                Rec<T> *rb = b ? buf1 : buf0;
+                const bool hit =
+                    base + lane < range.y && region_hit<T, ELL, FL>(rb[lane], R, w, tx0, ty0);
+                walk(__ballot_sync(FULL, hit), rb, base);
+                __syncwarp();
+                if (k + 2 < nch) issue(k + 2);
+            }
+        } else if constexpr (LIG_RASTER_FWD_WARPS) {
             // each warp streams the tile's list in chunks of 32 on its own
             // (its region's test only, no block barriers: warps whose
             // regions have short lists do not wait for the others)
@@ -705,14 +812,29 @@ raster_fwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work
                   L2Fwd<T> l2) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_slot;
+    // two mbarriers per warp for the bulk-staged fused-loss forward
+    __shared__ __align__(8) unsigned long long s_fbar[2 * 32];
     Rec<T> *s_rec = reinterpret_cast<Rec<T> *>(smem_raw);
-    uint32_t *s_bits = reinterpret_cast<uint32_t *>(s_rec + blockDim.x);
+    constexpr bool kBulk = FL && PPL == 4 && LIG_RASTER_FWD_WARPS && LIG_RASTER_FWD_BULK &&
+                           sizeof(T) == 4;
+    uint32_t *s_bits = reinterpret_cast<uint32_t *>(s_rec + (kBulk ? 2 : 1) * blockDim.x);
+    const uint32_t fbar = (uint32_t)__cvta_generic_to_shared(s_fbar);
+    uint32_t fphase = 0;
+    if (kBulk) {
+        if ((threadIdx.x & 31) == 0) {
+            const uint32_t b = fbar + 16u * (threadIdx.x >> 5);
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(b), "r"(1));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(b + 8u), "r"(1));
+            asm volatile("fence.mbarrier_init.release.cluster;");
+        }
+        __syncthreads();
+    }
     const int n_tiles = geo.total_tiles();
     for (int tile = next_tile(work, s_slot, true); tile < n_tiles;
          tile = next_tile(work, s_slot, false)) {
         const TileCtx tc = tile_ctx(geo, cum, d_total, tile);
         fwd_tile<T, GA, PPL, FL>(tc, tile, ids, tile_bins, recs, img, wsum, odx, ody, odxy,
-                                 final_idx, s_rec, s_bits, l2);
+                                 final_idx, s_rec, s_bits, l2, fbar, fphase);
     }
 }
 
@@ -1017,50 +1139,6 @@ __device__ __forceinline__ void lean_region_f2(const Rec<float> &g, float clamp,
 #ifndef LIG_RASTER_BWD_BULK
 #define LIG_RASTER_BWD_BULK 1  // lean backward (float): records staged by bulk async copies
 #endif
-// Bounded device waits that gave up (a malfunction; read by lig_wait_timeouts).
-__device__ unsigned int g_wait_timeouts;
-constexpr int kWaitLimit = 1 << 22;  // mbarrier polls before a wait is abandoned
-
-// Bulk asynchronous copies of gathered 48-byte records into shared memory,
-// completing on one mbarrier per CTA (cp.async.bulk, this GPU's memory only,
-// no multicast).  Thread 0 announces the batch's bytes; each thread < cnt
-// copies its record.  The transaction count may be completed before it is
-// announced (its range includes negative values), so no barrier is needed
-// between the two.
-__device__ __forceinline__ void bulk_records(uint32_t bar, Rec<float> *s_rec, int32_t *s_ids,
-                                             const int32_t *__restrict__ ids,
-                                             const Rec<float> *__restrict__ recs, int base,
-                                             int cnt) {
-    const int tid = threadIdx.x;
-    if (tid == 0)
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
-                     "r"(cnt * (int)sizeof(Rec<float>))
-                     : "memory");
-    if (tid < cnt) {
-        const int id = __ldg(ids + base + tid);
-        s_ids[tid] = id;
-        const uint32_t dst = (uint32_t)__cvta_generic_to_shared(s_rec + tid);
-        asm volatile(
-            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
-            "[%3];" ::"r"(dst),
-            "l"(recs + id), "r"((int)sizeof(Rec<float>)), "r"(bar)
-            : "memory");
-    }
-}
-
-// Wait for the mbarrier's current phase with at most kWaitLimit polls.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
-    uint32_t done = 0;
-    for (int it = 0; it < kWaitLimit && !done; ++it)
-        asm volatile(
-            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; "
-            "selp.u32 %0, 1, 0, p; }"
-            : "=r"(done)
-            : "r"(bar), "r"(phase)
-            : "memory");
-    return done != 0;
-}
-
 // LEAN (sum backward of the fused fit loss, no opacities, no wsum
 // cotangent): only the gradients the fit needs — v_xy, v_conic, v_rgb — are
 // accumulated (no |v_xy| sums, no opacity gradient) and each (Gaussian,
@@ -1614,7 +1692,9 @@ int raster_fwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
     const bool ppl4 = !ga && geo.total_tiles() >= LIG_RASTER_PPL4_MIN_TILES;
     const bool ppl2 = !ga && !ppl4 && geo.total_tiles() >= LIG_RASTER_PPL2_MIN_TILES;
     const int nt = 32 * Regions::make(ppl4 ? 3 : (ppl2 ? 1 : 0), geo.B).count;
-    const size_t sm = (size_t)nt * (sizeof(Rec<T>) + sizeof(uint32_t));
+    // per thread a record (two: double-buffered bulk staging) and a region mask
+    const bool two = fl && ppl4 && sizeof(T) == 4 && LIG_RASTER_FWD_BULK;
+    const size_t sm = (size_t)nt * ((two ? 2 : 1) * sizeof(Rec<T>) + sizeof(uint32_t));
     using K = void (*)(const BatchGeo, const int32_t *, int *, const int32_t *, const int2 *,
                        const int32_t *, const Rec<T> *, T *, T *, T *, T *, T *, int32_t *,
                        L2Fwd<T>);
