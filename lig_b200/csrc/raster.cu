@@ -379,6 +379,9 @@ __device__ __forceinline__ int next_tile(int *work, int &s_slot, bool first) {
 #ifndef LIG_RASTER_FWD_BULK
 #define LIG_RASTER_FWD_BULK 0  // fused-loss forward (float): records staged by bulk copies
 #endif
+#ifndef LIG_RASTER_FWD_XPREF
+#define LIG_RASTER_FWD_XPREF 0  // fused-loss forward: persistent, next tile's records prefetched
+#endif
 // One CTA per tile, warp w = region w (8x4 pixels), one pixel per lane.
 // Batches of blockDim Gaussians (list order) are staged in shared memory, one
 // record per thread, with the next batch's record fetched into registers
@@ -555,7 +558,7 @@ __device__ __forceinline__ double fwd_write(const FwdAcc<T, GA> &acc, bool insid
 // added in list order either way.
 // FL: the fused-loss forward without opacities (records carry the halved
 // conic; no wsum): per pixel the same alphas and colour sums, fewer operations.
-template <typename T, bool GA, int PPL, bool FL>
+template <typename T, bool GA, int PPL, bool FL, bool XP = false>
 __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int32_t *__restrict__ ids,
                                          const int2 *__restrict__ tile_bins,
                                          const Rec<T> *__restrict__ recs, T *__restrict__ img,
@@ -563,7 +566,8 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
                                          T *__restrict__ ody, T *__restrict__ odxy,
                                          int32_t *__restrict__ final_idx, Rec<T> *s_rec,
                                          uint32_t *s_bits, const L2Fwd<T> &l2, uint32_t fbar,
-                                         uint32_t &fphase) {
+                                         uint32_t &fphase, Rec<T> *xpre = nullptr,
+                                         int2 xrange = int2{0, 0}, int2 xnext = int2{0, 0}) {
     const unsigned FULL = 0xffffffffu;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int B = tc.B, tx0 = tc.tx0, ty0 = tc.ty0;
@@ -671,7 +675,7 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
         }
     };
     if (!tc.empty) {
-        const int2 range = tile_bins[tile];
+        const int2 range = XP ? xrange : tile_bins[tile];
         if constexpr (FL && PPL == 4 && LIG_RASTER_FWD_WARPS && LIG_RASTER_FWD_BULK &&
                       sizeof(T) == 4) {
             // as below, with each warp's chunks of 32 records staged by bulk
@@ -715,15 +719,26 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
             // regions have short lists do not wait for the others)
             Rec<T> *w_rec = s_rec + w * 32;
             Rec<T> pre;
-            if (range.x + lane < range.y) pre = recs[__ldg(ids + range.x + lane)];
+            if constexpr (XP) pre = *xpre;  // fetched while the previous tile was walked
+            else if (range.x + lane < range.y) pre = recs[__ldg(ids + range.x + lane)];
             for (int base = range.x; base < range.y; base += 32) {
                 const bool hit =
                     base + lane < range.y && region_hit<T, ELL, FL>(pre, R, w, tx0, ty0);
                 __syncwarp();
                 w_rec[lane] = pre;
                 __syncwarp();
-                if (base + 32 + lane < range.y) pre = recs[__ldg(ids + base + 32 + lane)];
+                if (base + 32 < range.y) {
+                    if (base + 32 + lane < range.y) pre = recs[__ldg(ids + base + 32 + lane)];
+                } else if constexpr (XP) {
+                    // the last chunk: fetch the next tile's first one instead
+                    if (xnext.x + lane < xnext.y) pre = recs[__ldg(ids + xnext.x + lane)];
+                }
                 walk(__ballot_sync(FULL, hit), w_rec, base);
+            }
+            if constexpr (XP) {
+                if (range.x >= range.y && xnext.x + lane < xnext.y)
+                    pre = recs[__ldg(ids + xnext.x + lane)];
+                *xpre = pre;
             }
         } else {
             const int nt = blockDim.x;
@@ -748,6 +763,8 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
     } else {  // the reference's empty-list branch (rasterize.py:80-90)
 #pragma unroll
         for (int p = 0; p < PPL; ++p) acc[p].r = acc[p].g = acc[p].b = (T)1;
+        if constexpr (XP)
+            if (xnext.x + lane < xnext.y) *xpre = recs[__ldg(ids + xnext.x + lane)];
     }
     double sq = 0.0;
 #pragma unroll
@@ -802,7 +819,7 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
 #define LIG_RASTER_PPL4_MIN_TILES 4096  // measured: faster from 2048^2 up, not at 512^2
 #endif
 
-template <typename T, bool GA, int PPL, int MAXT, int MINB, bool FL = false>
+template <typename T, bool GA, int PPL, int MAXT, int MINB, bool FL = false, bool XP = false>
 __global__ void __launch_bounds__(MAXT, MINB)
 raster_fwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work,
                   const int32_t *__restrict__ ids, const int2 *__restrict__ tile_bins,
@@ -830,11 +847,40 @@ raster_fwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work
         __syncthreads();
     }
     const int n_tiles = geo.total_tiles();
-    for (int tile = next_tile(work, s_slot, true); tile < n_tiles;
-         tile = next_tile(work, s_slot, false)) {
-        const TileCtx tc = tile_ctx(geo, cum, d_total, tile);
-        fwd_tile<T, GA, PPL, FL>(tc, tile, ids, tile_bins, recs, img, wsum, odx, ody, odxy,
-                                 final_idx, s_rec, s_bits, l2, fbar, fphase);
+    if constexpr (XP) {
+        // persistent CTAs with a static schedule (tile, tile + grid, ...): each
+        // warp fetches the next tile's first chunk of records while it walks
+        // the last chunk of the current one
+        int tile = blockIdx.x;
+        if (tile >= n_tiles) return;
+        TileCtx tc = tile_ctx(geo, cum, d_total, tile);
+        int2 range = tc.empty ? make_int2(0, 0) : tile_bins[tile];
+        const int lane = threadIdx.x & 31;
+        Rec<T> pre;
+        if (range.x + lane < range.y) pre = recs[__ldg(ids + range.x + lane)];
+        for (;;) {
+            const int next = tile + (int)gridDim.x;
+            TileCtx ntc = tc;
+            int2 nrange = make_int2(0, 0);
+            if (next < n_tiles) {
+                ntc = tile_ctx(geo, cum, d_total, next);
+                if (!ntc.empty) nrange = tile_bins[next];
+            }
+            fwd_tile<T, GA, PPL, FL, true>(tc, tile, ids, tile_bins, recs, img, wsum, odx, ody,
+                                           odxy, final_idx, s_rec, s_bits, l2, fbar, fphase,
+                                           &pre, range, nrange);
+            if (next >= n_tiles) break;
+            tile = next;
+            tc = ntc;
+            range = nrange;
+        }
+    } else {
+        for (int tile = next_tile(work, s_slot, true); tile < n_tiles;
+             tile = next_tile(work, s_slot, false)) {
+            const TileCtx tc = tile_ctx(geo, cum, d_total, tile);
+            fwd_tile<T, GA, PPL, FL>(tc, tile, ids, tile_bins, recs, img, wsum, odx, ody, odxy,
+                                     final_idx, s_rec, s_bits, l2, fbar, fphase);
+        }
     }
 }
 
@@ -1704,10 +1750,15 @@ int raster_fwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
     // CTAs at B = 16; with LIG_RASTER_FWD_MINB64 > 0 it gets an instantiation
     // asking for that many resident CTAs per SM (its register budget)
     constexpr int FM64 = LIG_RASTER_FWD_MINB64 > 0 ? LIG_RASTER_FWD_MINB64 : 16;
+    // cross-tile prefetch (static persistent schedule) for the fused-loss
+    // forward with four pixels per lane, when no work counter is given
+    const bool xp = fl && ppl4 && small && !walk.work && LIG_RASTER_FWD_XPREF &&
+                    !(LIG_RASTER_FWD_MINB64 > 0 && nt <= 64);
     K fn = ga ? (small ? raster_fwd_kernel<T, true, 1, 256, FM>
                        : raster_fwd_kernel<T, true, 1, 1024, 1>)
          : fl ? (ppl4 ? ((LIG_RASTER_FWD_MINB64 > 0 && nt <= 64)
                              ? raster_fwd_kernel<T, false, 4, 64, FM64, true>
+                         : xp ? raster_fwd_kernel<T, false, 4, 256, FM, true, true>
                          : small ? raster_fwd_kernel<T, false, 4, 256, FM, true>
                                  : raster_fwd_kernel<T, false, 4, 1024, 1, true>)
                  : ppl2 ? (small ? raster_fwd_kernel<T, false, 2, 256, FM, true>
@@ -1722,11 +1773,11 @@ int raster_fwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
                               : raster_fwd_kernel<T, false, 1, 1024, 1>);
     if (!set_dyn_smem((const void *)fn, sm)) return LIG_ERR_LAUNCH;
     int grid = geo.total_tiles();
-    if (walk.work) {
+    if (walk.work || xp) {
         const int pg = persistent_grid((const void *)fn, nt, sm);
         if (pg <= 0) return LIG_ERR_LAUNCH;
         grid = grid < pg ? grid : pg;
-        cudaMemsetAsync(walk.work, 0, sizeof(int), s);
+        if (walk.work) cudaMemsetAsync(walk.work, 0, sizeof(int), s);
     }
     fn<<<grid, nt, sm, s>>>(geo, walk.cum, walk.work, ids, (const int2 *)bins, d_total,
                             (const Rec<T> *)ws, (T *)img, (T *)wsum, ga ? (T *)dx : nullptr,
