@@ -101,72 +101,6 @@ __global__ void pack_kernel(int n, const T *__restrict__ xys, const T *__restric
     recs[i] = r;
 }
 
-// Bounded device waits that gave up (a malfunction; read by lig_wait_timeouts).
-__device__ unsigned int g_wait_timeouts;
-constexpr int kWaitLimit = 1 << 22;  // mbarrier polls before a wait is abandoned
-
-// Bulk asynchronous copies of gathered 48-byte records into shared memory,
-// completing on one mbarrier per CTA (cp.async.bulk, this GPU's memory only,
-// no multicast).  Thread 0 announces the batch's bytes; each thread < cnt
-// copies its record.  The transaction count may be completed before it is
-// announced (its range includes negative values), so no barrier is needed
-// between the two.
-__device__ __forceinline__ void bulk_records(uint32_t bar, Rec<float> *s_rec, int32_t *s_ids,
-                                             const int32_t *__restrict__ ids,
-                                             const Rec<float> *__restrict__ recs, int base,
-                                             int cnt) {
-    const int tid = threadIdx.x;
-    if (tid == 0)
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
-                     "r"(cnt * (int)sizeof(Rec<float>))
-                     : "memory");
-    if (tid < cnt) {
-        const int id = __ldg(ids + base + tid);
-        s_ids[tid] = id;
-        const uint32_t dst = (uint32_t)__cvta_generic_to_shared(s_rec + tid);
-        asm volatile(
-            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
-            "[%3];" ::"r"(dst),
-            "l"(recs + id), "r"((int)sizeof(Rec<float>)), "r"(bar)
-            : "memory");
-    }
-}
-
-// Wait for the mbarrier's current phase with at most kWaitLimit polls.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
-    uint32_t done = 0;
-    for (int it = 0; it < kWaitLimit && !done; ++it)
-        asm volatile(
-            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; "
-            "selp.u32 %0, 1, 0, p; }"
-            : "=r"(done)
-            : "r"(bar), "r"(phase)
-            : "memory");
-    return done != 0;
-}
-
-// One warp's variant: lane 0 announces the chunk's bytes, lanes < cnt copy
-// their record into dst[lane].
-__device__ __forceinline__ void warp_bulk_records(uint32_t bar, Rec<float> *dst,
-                                                  const int32_t *__restrict__ ids,
-                                                  const Rec<float> *__restrict__ recs, int base,
-                                                  int cnt) {
-    const int lane = threadIdx.x & 31;
-    if (lane == 0)
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
-                     "r"(cnt * (int)sizeof(Rec<float>))
-                     : "memory");
-    if (lane < cnt) {
-        const int id = __ldg(ids + base + lane);
-        const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst + lane);
-        asm volatile(
-            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
-            "[%3];" ::"r"(d),
-            "l"(recs + id), "r"((int)sizeof(Rec<float>)), "r"(bar)
-            : "memory");
-    }
-}
-
 // ---------------------------------------------------------------- regions
 // A tile is split into R <= 32 regions of 32 pixels; warp w of the CTA owns
 // region w and each lane owns PPL pixels of it.
@@ -376,12 +310,6 @@ __device__ __forceinline__ int next_tile(int *work, int &s_slot, bool first) {
 #ifndef LIG_RASTER_FWD_FUSED
 #define LIG_RASTER_FWD_FUSED 1  // specialised fused-loss forward (no opacities)
 #endif
-#ifndef LIG_RASTER_FWD_BULK
-#define LIG_RASTER_FWD_BULK 0  // fused-loss forward (float): records staged by bulk copies
-#endif
-#ifndef LIG_RASTER_FWD_XPREF
-#define LIG_RASTER_FWD_XPREF 0  // fused-loss forward: persistent, next tile's records prefetched
-#endif
 // One CTA per tile, warp w = region w (8x4 pixels), one pixel per lane.
 // Batches of blockDim Gaussians (list order) are staged in shared memory, one
 // record per thread, with the next batch's record fetched into registers
@@ -558,16 +486,14 @@ __device__ __forceinline__ double fwd_write(const FwdAcc<T, GA> &acc, bool insid
 // added in list order either way.
 // FL: the fused-loss forward without opacities (records carry the halved
 // conic; no wsum): per pixel the same alphas and colour sums, fewer operations.
-template <typename T, bool GA, int PPL, bool FL, bool XP = false>
+template <typename T, bool GA, int PPL, bool FL>
 __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int32_t *__restrict__ ids,
                                          const int2 *__restrict__ tile_bins,
                                          const Rec<T> *__restrict__ recs, T *__restrict__ img,
                                          T *__restrict__ wsum, T *__restrict__ odx,
                                          T *__restrict__ ody, T *__restrict__ odxy,
                                          int32_t *__restrict__ final_idx, Rec<T> *s_rec,
-                                         uint32_t *s_bits, const L2Fwd<T> &l2, uint32_t fbar,
-                                         uint32_t &fphase, Rec<T> *xpre = nullptr,
-                                         int2 xrange = int2{0, 0}, int2 xnext = int2{0, 0}) {
+                                         uint32_t *s_bits, const L2Fwd<T> &l2) {
     const unsigned FULL = 0xffffffffu;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int B = tc.B, tx0 = tc.tx0, ty0 = tc.ty0;
@@ -675,70 +601,22 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
         }
     };
     if (!tc.empty) {
-        const int2 range = XP ? xrange : tile_bins[tile];
-        if constexpr (FL && PPL == 4 && LIG_RASTER_FWD_WARPS && LIG_RASTER_FWD_BULK &&
-                      sizeof(T) == 4) {
-            // as below, with each warp's chunks of 32 records staged by bulk
-            // asynchronous copies into two buffers (one mbarrier each), the
-            // next two chunks in flight while one is walked
-            Rec<T> *buf0 = s_rec + w * 64, *buf1 = buf0 + 32;
-            const uint32_t bar0 = fbar + 16u * w, bar1 = bar0 + 8u;
-            const int nch = (range.y - range.x + 31) / 32;
-            auto issue = [&](int k) {
-                const int base = range.x + 32 * k;
-                warp_bulk_records((k & 1) ? bar1 : bar0,
-                                  reinterpret_cast<Rec<float> *>((k & 1) ? buf1 : buf0), ids,
-                                  reinterpret_cast<const Rec<float> *>(recs), base,
-                                  min(32, range.y - base));
-            };
-            if (nch > 0) issue(0);
-            if (nch > 1) issue(1);
-            for (int k = 0; k < nch; ++k) {
-                const int base = range.x + 32 * k, b = k & 1;
-                const uint32_t bar = b ? bar1 : bar0;
-                const bool ok = mbar_wait(bar, (fphase >> b) & 1u);
-                fphase ^= 1u << b;
-                if (__any_sync(FULL, !ok)) {
-                    // a wait gave up: count it, let this warp's copies drain
-                    // (bounded) and leave the rest of its list
-                    if (lane == 0) atomicAdd(&g_wait_timeouts, 1u);
-                    (void)mbar_wait(bar, ((fphase >> b) & 1u) ^ 1u);
-                    if (k + 1 < nch) (void)mbar_wait(b ? bar0 : bar1, (fphase >> (b ^ 1)) & 1u);
-                    break;
-                }
-                Rec<T> *rb = b ? buf1 : buf0;
-                const bool hit =
-                    base + lane < range.y && region_hit<T, ELL, FL>(rb[lane], R, w, tx0, ty0);
-                walk(__ballot_sync(FULL, hit), rb, base);
-                __syncwarp();
-                if (k + 2 < nch) issue(k + 2);
-            }
-        } else if constexpr (LIG_RASTER_FWD_WARPS) {
+        const int2 range = tile_bins[tile];
+        if constexpr (LIG_RASTER_FWD_WARPS) {
             // each warp streams the tile's list in chunks of 32 on its own
             // (its region's test only, no block barriers: warps whose
             // regions have short lists do not wait for the others)
             Rec<T> *w_rec = s_rec + w * 32;
             Rec<T> pre;
-            if constexpr (XP) pre = *xpre;  // fetched while the previous tile was walked
-            else if (range.x + lane < range.y) pre = recs[__ldg(ids + range.x + lane)];
+            if (range.x + lane < range.y) pre = recs[__ldg(ids + range.x + lane)];
             for (int base = range.x; base < range.y; base += 32) {
                 const bool hit =
                     base + lane < range.y && region_hit<T, ELL, FL>(pre, R, w, tx0, ty0);
                 __syncwarp();
                 w_rec[lane] = pre;
                 __syncwarp();
-                if (base + 32 < range.y) {
-                    if (base + 32 + lane < range.y) pre = recs[__ldg(ids + base + 32 + lane)];
-                } else if constexpr (XP) {
-                    // the last chunk: fetch the next tile's first one instead
-                    if (xnext.x + lane < xnext.y) pre = recs[__ldg(ids + xnext.x + lane)];
-                }
+                if (base + 32 + lane < range.y) pre = recs[__ldg(ids + base + 32 + lane)];
                 walk(__ballot_sync(FULL, hit), w_rec, base);
-            }
-            if constexpr (XP) {
-                if (range.x >= range.y && xnext.x + lane < xnext.y)
-                    pre = recs[__ldg(ids + xnext.x + lane)];
-                *xpre = pre;
             }
         } else {
             const int nt = blockDim.x;
@@ -763,8 +641,6 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
     } else {  // the reference's empty-list branch (rasterize.py:80-90)
 #pragma unroll
         for (int p = 0; p < PPL; ++p) acc[p].r = acc[p].g = acc[p].b = (T)1;
-        if constexpr (XP)
-            if (xnext.x + lane < xnext.y) *xpre = recs[__ldg(ids + xnext.x + lane)];
     }
     double sq = 0.0;
 #pragma unroll
@@ -779,9 +655,6 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
 // instantiation.
 #ifndef LIG_RASTER_FWD_MINB
 #define LIG_RASTER_FWD_MINB 4
-#endif
-#ifndef LIG_RASTER_FWD_MINB64
-#define LIG_RASTER_FWD_MINB64 0  // 0: the 256-thread instantiation's budget (64 registers)
 #endif
 #ifndef LIG_RASTER_BWD_PAIR
 #define LIG_RASTER_BWD_PAIR 1  // lean backward: two pixels per loop iteration (measured faster)
@@ -819,7 +692,7 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
 #define LIG_RASTER_PPL4_MIN_TILES 4096  // measured: faster from 2048^2 up, not at 512^2
 #endif
 
-template <typename T, bool GA, int PPL, int MAXT, int MINB, bool FL = false, bool XP = false>
+template <typename T, bool GA, int PPL, int MAXT, int MINB, bool FL = false>
 __global__ void __launch_bounds__(MAXT, MINB)
 raster_fwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work,
                   const int32_t *__restrict__ ids, const int2 *__restrict__ tile_bins,
@@ -829,58 +702,14 @@ raster_fwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work
                   L2Fwd<T> l2) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_slot;
-    // two mbarriers per warp for the bulk-staged fused-loss forward
-    __shared__ __align__(8) unsigned long long s_fbar[2 * 32];
     Rec<T> *s_rec = reinterpret_cast<Rec<T> *>(smem_raw);
-    constexpr bool kBulk = FL && PPL == 4 && LIG_RASTER_FWD_WARPS && LIG_RASTER_FWD_BULK &&
-                           sizeof(T) == 4;
-    uint32_t *s_bits = reinterpret_cast<uint32_t *>(s_rec + (kBulk ? 2 : 1) * blockDim.x);
-    const uint32_t fbar = (uint32_t)__cvta_generic_to_shared(s_fbar);
-    uint32_t fphase = 0;
-    if (kBulk) {
-        if ((threadIdx.x & 31) == 0) {
-            const uint32_t b = fbar + 16u * (threadIdx.x >> 5);
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(b), "r"(1));
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(b + 8u), "r"(1));
-            asm volatile("fence.mbarrier_init.release.cluster;");
-        }
-        __syncthreads();
-    }
+    uint32_t *s_bits = reinterpret_cast<uint32_t *>(s_rec + blockDim.x);
     const int n_tiles = geo.total_tiles();
-    if constexpr (XP) {
-        // persistent CTAs with a static schedule (tile, tile + grid, ...): each
-        // warp fetches the next tile's first chunk of records while it walks
-        // the last chunk of the current one
-        int tile = blockIdx.x;
-        if (tile >= n_tiles) return;
-        TileCtx tc = tile_ctx(geo, cum, d_total, tile);
-        int2 range = tc.empty ? make_int2(0, 0) : tile_bins[tile];
-        const int lane = threadIdx.x & 31;
-        Rec<T> pre;
-        if (range.x + lane < range.y) pre = recs[__ldg(ids + range.x + lane)];
-        for (;;) {
-            const int next = tile + (int)gridDim.x;
-            TileCtx ntc = tc;
-            int2 nrange = make_int2(0, 0);
-            if (next < n_tiles) {
-                ntc = tile_ctx(geo, cum, d_total, next);
-                if (!ntc.empty) nrange = tile_bins[next];
-            }
-            fwd_tile<T, GA, PPL, FL, true>(tc, tile, ids, tile_bins, recs, img, wsum, odx, ody,
-                                           odxy, final_idx, s_rec, s_bits, l2, fbar, fphase,
-                                           &pre, range, nrange);
-            if (next >= n_tiles) break;
-            tile = next;
-            tc = ntc;
-            range = nrange;
-        }
-    } else {
-        for (int tile = next_tile(work, s_slot, true); tile < n_tiles;
-             tile = next_tile(work, s_slot, false)) {
-            const TileCtx tc = tile_ctx(geo, cum, d_total, tile);
-            fwd_tile<T, GA, PPL, FL>(tc, tile, ids, tile_bins, recs, img, wsum, odx, ody, odxy,
-                                     final_idx, s_rec, s_bits, l2, fbar, fphase);
-        }
+    for (int tile = next_tile(work, s_slot, true); tile < n_tiles;
+         tile = next_tile(work, s_slot, false)) {
+        const TileCtx tc = tile_ctx(geo, cum, d_total, tile);
+        fwd_tile<T, GA, PPL, FL>(tc, tile, ids, tile_bins, recs, img, wsum, odx, ody, odxy,
+                                 final_idx, s_rec, s_bits, l2);
     }
 }
 
@@ -1185,6 +1014,50 @@ __device__ __forceinline__ void lean_region_f2(const Rec<float> &g, float clamp,
 #ifndef LIG_RASTER_BWD_BULK
 #define LIG_RASTER_BWD_BULK 1  // lean backward (float): records staged by bulk async copies
 #endif
+// Bounded device waits that gave up (a malfunction; read by lig_wait_timeouts).
+__device__ unsigned int g_wait_timeouts;
+constexpr int kWaitLimit = 1 << 22;  // mbarrier polls before a wait is abandoned
+
+// Bulk asynchronous copies of gathered 48-byte records into shared memory,
+// completing on one mbarrier per CTA (cp.async.bulk, this GPU's memory only,
+// no multicast).  Thread 0 announces the batch's bytes; each thread < cnt
+// copies its record.  The transaction count may be completed before it is
+// announced (its range includes negative values), so no barrier is needed
+// between the two.
+__device__ __forceinline__ void bulk_records(uint32_t bar, Rec<float> *s_rec, int32_t *s_ids,
+                                             const int32_t *__restrict__ ids,
+                                             const Rec<float> *__restrict__ recs, int base,
+                                             int cnt) {
+    const int tid = threadIdx.x;
+    if (tid == 0)
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                     "r"(cnt * (int)sizeof(Rec<float>))
+                     : "memory");
+    if (tid < cnt) {
+        const int id = __ldg(ids + base + tid);
+        s_ids[tid] = id;
+        const uint32_t dst = (uint32_t)__cvta_generic_to_shared(s_rec + tid);
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+            "[%3];" ::"r"(dst),
+            "l"(recs + id), "r"((int)sizeof(Rec<float>)), "r"(bar)
+            : "memory");
+    }
+}
+
+// Wait for the mbarrier's current phase with at most kWaitLimit polls.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
+    uint32_t done = 0;
+    for (int it = 0; it < kWaitLimit && !done; ++it)
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; "
+            "selp.u32 %0, 1, 0, p; }"
+            : "=r"(done)
+            : "r"(bar), "r"(phase)
+            : "memory");
+    return done != 0;
+}
+
 // LEAN (sum backward of the fused fit loss, no opacities, no wsum
 // cotangent): only the gradients the fit needs — v_xy, v_conic, v_rgb — are
 // accumulated (no |v_xy| sums, no opacity gradient) and each (Gaussian,
@@ -1738,29 +1611,16 @@ int raster_fwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
     const bool ppl4 = !ga && geo.total_tiles() >= LIG_RASTER_PPL4_MIN_TILES;
     const bool ppl2 = !ga && !ppl4 && geo.total_tiles() >= LIG_RASTER_PPL2_MIN_TILES;
     const int nt = 32 * Regions::make(ppl4 ? 3 : (ppl2 ? 1 : 0), geo.B).count;
-    // per thread a record (two: double-buffered bulk staging) and a region mask
-    const bool two = fl && ppl4 && sizeof(T) == 4 && LIG_RASTER_FWD_BULK;
-    const size_t sm = (size_t)nt * ((two ? 2 : 1) * sizeof(Rec<T>) + sizeof(uint32_t));
+    const size_t sm = (size_t)nt * (sizeof(Rec<T>) + sizeof(uint32_t));
     using K = void (*)(const BatchGeo, const int32_t *, int *, const int32_t *, const int2 *,
                        const int32_t *, const Rec<T> *, T *, T *, T *, T *, T *, int32_t *,
                        L2Fwd<T>);
     const bool small = nt <= 256;
     constexpr int FM = LIG_RASTER_FWD_MINB;
-    // the fused-loss forward with four pixels per lane launches 64-thread
-    // CTAs at B = 16; with LIG_RASTER_FWD_MINB64 > 0 it gets an instantiation
-    // asking for that many resident CTAs per SM (its register budget)
-    constexpr int FM64 = LIG_RASTER_FWD_MINB64 > 0 ? LIG_RASTER_FWD_MINB64 : 16;
-    // cross-tile prefetch (static persistent schedule) for the fused-loss
-    // forward with four pixels per lane, when no work counter is given
-    const bool xp = fl && ppl4 && small && !walk.work && LIG_RASTER_FWD_XPREF &&
-                    !(LIG_RASTER_FWD_MINB64 > 0 && nt <= 64);
     K fn = ga ? (small ? raster_fwd_kernel<T, true, 1, 256, FM>
                        : raster_fwd_kernel<T, true, 1, 1024, 1>)
-         : fl ? (ppl4 ? ((LIG_RASTER_FWD_MINB64 > 0 && nt <= 64)
-                             ? raster_fwd_kernel<T, false, 4, 64, FM64, true>
-                         : xp ? raster_fwd_kernel<T, false, 4, 256, FM, true, true>
-                         : small ? raster_fwd_kernel<T, false, 4, 256, FM, true>
-                                 : raster_fwd_kernel<T, false, 4, 1024, 1, true>)
+         : fl ? (ppl4 ? (small ? raster_fwd_kernel<T, false, 4, 256, FM, true>
+                               : raster_fwd_kernel<T, false, 4, 1024, 1, true>)
                  : ppl2 ? (small ? raster_fwd_kernel<T, false, 2, 256, FM, true>
                                  : raster_fwd_kernel<T, false, 2, 1024, 1, true>)
                         : (small ? raster_fwd_kernel<T, false, 1, 256, FM, true>
@@ -1773,11 +1633,11 @@ int raster_fwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
                               : raster_fwd_kernel<T, false, 1, 1024, 1>);
     if (!set_dyn_smem((const void *)fn, sm)) return LIG_ERR_LAUNCH;
     int grid = geo.total_tiles();
-    if (walk.work || xp) {
+    if (walk.work) {
         const int pg = persistent_grid((const void *)fn, nt, sm);
         if (pg <= 0) return LIG_ERR_LAUNCH;
         grid = grid < pg ? grid : pg;
-        if (walk.work) cudaMemsetAsync(walk.work, 0, sizeof(int), s);
+        cudaMemsetAsync(walk.work, 0, sizeof(int), s);
     }
     fn<<<grid, nt, sm, s>>>(geo, walk.cum, walk.work, ids, (const int2 *)bins, d_total,
                             (const Rec<T> *)ws, (T *)img, (T *)wsum, ga ? (T *)dx : nullptr,
