@@ -8,7 +8,7 @@
 //
 // Ordering (default, LIG_BIN_SCATTER): per-tile counters, their exclusive
 // scan, an atomic scatter of every slot into its tile's range and a per-tile
-// sort by Gaussian index (see "scatter binning" below); workspace: three
+// sort by Gaussian index (see "scatter binning" below); workspace: two
 // counters per tile.  Alternative kept for comparison: keys are 32-bit tile
 // ids (the reference's int64 (tile << 32) | depth keys carry depth 0, so only
 // ceil(log2 T) bits hold information) sorted by a stable LSD radix sort over
@@ -544,16 +544,17 @@ __global__ void tile_count_kernel(int n, const T *__restrict__ xys, const T *__r
                      [&](int, uint32_t key, uint32_t) { atomicAdd(&tcount[key], 1u); });
 }
 
-// 3. scatter into the tile's range (tstart: exclusive scan of the counts)
+// 3. scatter into the tile's range: `cursor` starts as the exclusive scan of
+// the counts (each tile's first position) and one atomic per slot returns
+// the slot's absolute position; afterwards cursor[t] = start + count.
 template <typename T>
 __global__ void tile_scatter_kernel(int n, const T *__restrict__ xys, const T *__restrict__ ext,
                                     const int32_t *__restrict__ cum, BatchGeo geo, int capacity,
-                                    const uint32_t *__restrict__ tstart,
-                                    uint32_t *__restrict__ tfill, uint32_t *__restrict__ out,
+                                    uint32_t *__restrict__ cursor, uint32_t *__restrict__ out,
                                     int64_t *__restrict__ keys64, int32_t *__restrict__ gids) {
     for_each_slot<T>(n, xys, ext, cum, geo, capacity, nullptr,
                      [&](int slot, uint32_t key, uint32_t val) {
-                         out[tstart[key] + atomicAdd(&tfill[key], 1u)] = val;
+                         out[atomicAdd(&cursor[key], 1u)] = val;
                          if (keys64) {  // the reference's emission-order outputs
                              const bool ph = (val & kPhantom) != 0;
                              const int g = (int)(val >> 1);
@@ -635,7 +636,7 @@ __device__ __forceinline__ void sort_segment_regs(uint32_t *seg, int L, int32_t 
 // common short tiles run at full occupancy).
 __global__ void __launch_bounds__(32 * kSegWarps)
 tile_sort_kernel(BatchGeo geo, const uint32_t *__restrict__ tcount,
-                 const uint32_t *__restrict__ tstart, int capacity, uint32_t *__restrict__ vals,
+                 const uint32_t *__restrict__ tend, int capacity, uint32_t *__restrict__ vals,
                  int32_t *__restrict__ ids, int2 *__restrict__ tile_bins,
                  int64_t *__restrict__ isect_sorted, int32_t *__restrict__ long_list) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -643,8 +644,9 @@ tile_sort_kernel(BatchGeo geo, const uint32_t *__restrict__ tcount,
     const int nwarps = gridDim.x * kSegWarps;
     for (int t = blockIdx.x * kSegWarps + w; t < T; t += nwarps) {
         const uint32_t c = tcount[t];
-        const int a = (int)min((uint32_t)capacity, tstart[t]);
-        const int b = (int)min((uint32_t)capacity, tstart[t] + c);
+        const uint32_t e = tend[t];  // start + count after the scatter
+        const int a = (int)min((uint32_t)capacity, e - c);
+        const int b = (int)min((uint32_t)capacity, e);
         if (lane == 0) tile_bins[t] = c ? make_int2(a, b) : make_int2(0, 0);
         const int L = b - a;
         if (L <= 0) continue;
@@ -671,15 +673,15 @@ tile_sort_kernel(BatchGeo geo, const uint32_t *__restrict__ tcount,
 constexpr int kLongThreads = 256;
 __global__ void __launch_bounds__(kLongThreads)
 tile_sort_long_kernel(BatchGeo geo, const uint32_t *__restrict__ tcount,
-                      const uint32_t *__restrict__ tstart, int capacity,
+                      const uint32_t *__restrict__ tend, int capacity,
                       uint32_t *__restrict__ vals, int32_t *__restrict__ ids,
                       const int32_t *__restrict__ long_list) {
     __shared__ uint32_t s_buf[kSegSmem];
     const int nlong = long_list[0];
     for (int q = blockIdx.x; q < nlong; q += gridDim.x) {
         const int t = long_list[1 + q];
-        const int a = (int)min((uint32_t)capacity, tstart[t]);
-        const int b = (int)min((uint32_t)capacity, tstart[t] + tcount[t]);
+        const int a = (int)min((uint32_t)capacity, tend[t] - tcount[t]);
+        const int b = (int)min((uint32_t)capacity, tend[t]);
         const int L = b - a;
         int P = 1;
         while (P < L) P <<= 1;
@@ -748,11 +750,11 @@ inline BinPlan make_plan(int capacity, int num_tiles) {
     return p;
 }
 
-// Workspace of the scatter path: per-tile counts, first positions and
-// cursors, scan partials, the long-tile list.  The sort keys are scattered
+// Workspace of the scatter path: per-tile counts and cursors (the cursors
+// start as the scan of the counts), scan partials, the long-tile list.  The sort keys are scattered
 // into gid_sorted itself and sorted in place there.
 struct ScatterPlan {
-    size_t off_count, off_start, off_fill, off_part, off_long, total;
+    size_t off_count, off_cursor, off_part, off_long, total;
 };
 
 inline ScatterPlan make_scatter_plan(int num_tiles) {
@@ -760,8 +762,7 @@ inline ScatterPlan make_scatter_plan(int num_tiles) {
     size_t t = (size_t)(num_tiles > 0 ? num_tiles : 1);
     size_t off = 0;
     p.off_count = off; off = align_up(off + 4 * t);
-    p.off_start = off; off = align_up(off + 4 * t);
-    p.off_fill = off; off = align_up(off + 4 * t);
+    p.off_cursor = off; off = align_up(off + 4 * t);
     p.off_part = off; off = align_up(off + 4 * ((t + kScanTile - 1) / kScanTile + 1));
     p.off_long = off; off = align_up(off + 4 * (t + 1));
     p.total = off;
@@ -779,8 +780,7 @@ int run_bin_scatter(const BatchGeo &geo, const void *xys, const void *ext, const
     if (ws_bytes < p.total) return LIG_ERR_WORKSPACE;
     char *base = (char *)ws;
     uint32_t *tcount = (uint32_t *)(base + p.off_count);
-    uint32_t *tstart = (uint32_t *)(base + p.off_start);
-    uint32_t *tfill = (uint32_t *)(base + p.off_fill);
+    uint32_t *cursor = (uint32_t *)(base + p.off_cursor);
     uint32_t *part = (uint32_t *)(base + p.off_part);
     int32_t *long_list = (int32_t *)(base + p.off_long);
     cudaMemsetAsync(status, 0, sizeof(int32_t), s);
@@ -792,7 +792,6 @@ int run_bin_scatter(const BatchGeo &geo, const void *xys, const void *ext, const
         return LIG_OK;
     }
     cudaMemsetAsync(tcount, 0, sizeof(uint32_t) * (size_t)T_, s);
-    cudaMemsetAsync(tfill, 0, sizeof(uint32_t) * (size_t)T_, s);
     cudaMemsetAsync(long_list, 0, sizeof(int32_t), s);
     const int warps = (n + 31) / 32;
     const int eblocks = (warps * 32 + 255) / 256;
@@ -801,17 +800,17 @@ int run_bin_scatter(const BatchGeo &geo, const void *xys, const void *ext, const
     flag_overflow_kernel<<<1, 1, 0, s>>>(d_total, capacity, status);
     note_launches(2);
     LIG_LAUNCH_CHECK();
-    int rc = device_scan(tcount, tstart, T_, false, part, nullptr, s);
+    int rc = device_scan(tcount, cursor, T_, false, part, nullptr, s);
     if (rc) return rc;
     uint32_t *vals = (uint32_t *)gid_sorted;
     tile_scatter_kernel<T><<<eblocks, 256, 0, s>>>(n, (const T *)xys, (const T *)ext, cum, geo,
-                                                   capacity, tstart, tfill, vals, isect, gids);
+                                                   capacity, cursor, vals, isect, gids);
     const int sort_blocks = (int)std::min<int64_t>(((int64_t)T_ + kSegWarps - 1) / kSegWarps,
                                                    148 * 32);
-    tile_sort_kernel<<<sort_blocks, 32 * kSegWarps, 0, s>>>(geo, tcount, tstart, capacity, vals,
+    tile_sort_kernel<<<sort_blocks, 32 * kSegWarps, 0, s>>>(geo, tcount, cursor, capacity, vals,
                                                           gid_sorted, (int2 *)tile_bins,
                                                           isect_sorted, long_list);
-    tile_sort_long_kernel<<<148 * 4, kLongThreads, 0, s>>>(geo, tcount, tstart, capacity, vals,
+    tile_sort_long_kernel<<<148 * 4, kLongThreads, 0, s>>>(geo, tcount, cursor, capacity, vals,
                                                            gid_sorted, long_list);
     note_launches(3);
     LIG_LAUNCH_CHECK();
