@@ -1016,7 +1016,10 @@ __device__ __forceinline__ void lean_region_f2(const Rec<float> &g, float clamp,
 #endif
 // Bounded device waits that gave up (a malfunction; read by lig_wait_timeouts).
 __device__ unsigned int g_wait_timeouts;
-constexpr int kWaitLimit = 1 << 22;  // mbarrier polls before a wait is abandoned
+// SM clock cycles (about 1 ms) before an mbarrier wait is abandoned: a
+// normal wait ends within microseconds, and a malfunction then costs a
+// launch at most about a millisecond per wave of CTAs instead of a hang.
+constexpr long long kWaitCycles = 2000000;
 
 // Bulk asynchronous copies of gathered 48-byte records into shared memory,
 // completing on one mbarrier per CTA (cp.async.bulk, this GPU's memory only,
@@ -1045,16 +1048,19 @@ __device__ __forceinline__ void bulk_records(uint32_t bar, Rec<float> *s_rec, in
     }
 }
 
-// Wait for the mbarrier's current phase with at most kWaitLimit polls.
+// Wait for the mbarrier's phase `phase` for at most kWaitCycles.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
     uint32_t done = 0;
-    for (int it = 0; it < kWaitLimit && !done; ++it)
+    const long long t0 = clock64();
+    for (;;) {
         asm volatile(
             "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; "
             "selp.u32 %0, 1, 0, p; }"
             : "=r"(done)
             : "r"(bar), "r"(phase)
             : "memory");
+        if (done || clock64() - t0 > kWaitCycles) break;
+    }
     return done != 0;
 }
 
