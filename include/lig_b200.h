@@ -89,13 +89,16 @@ size_t lig_cumsum_workspace_bytes(int num_points);
 
 /* Inclusive int32 prefix sum of num_tiles_hit; the total (num_intersects) is
  * written to the device word *num_intersects, with no host synchronisation.
+ * One kernel (a single-pass scan with decoupled look-back); num_tiles_hit and
+ * cum_tiles_hit must not overlap and the workspace must be 8-byte aligned
+ * (LIG_ERR_INVALID otherwise).
  * Replaces compute_cumulative_intersects (gsplat2d/gsplat2d/utils.py:61-67). */
 int lig_cumsum_tiles(int num_points, const int32_t *num_tiles_hit, int32_t *cum_tiles_hit,
                      int32_t *num_intersects, void *workspace, size_t workspace_bytes,
                      void *stream);
 
 /* Workspace bytes needed by lig_bin for `capacity` intersections over
- * num_tiles tiles (per-tile counters and scan partials). */
+ * num_tiles tiles (per-tile counters and cursors, the scan state). */
 size_t lig_bin_workspace_bytes(int num_points, int capacity, int num_tiles);
 
 /* Binning by tile in one call: per-tile counts of the emitted (Gaussian,

@@ -57,184 +57,325 @@ __device__ __forceinline__ uint32_t block_incl_scan(uint32_t v, uint32_t &total,
     return v + add;
 }
 
-// Each thread owns kScanItems consecutive elements (loaded warp-striped and
-// transposed through registers via shuffles would save little here: the scan
-// runs on <= a few MB).  Phase 1: per-block sums.
-__global__ void scan_reduce_kernel(const uint32_t *__restrict__ in, int n,
-                                   uint32_t *__restrict__ partials) {
-    __shared__ uint32_t s_warp[32];
-    int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
-    uint32_t acc = 0;
+// Single-pass scan with decoupled look-back.  Each CTA takes a ticket (the
+// order in which CTAs started), scans its kScanTile values and publishes its
+// aggregate in a 64-bit state word (flag in the high half: 1 = aggregate,
+// 2 = inclusive prefix); warp 0 then reads its predecessors' words 32 at a
+// time, nearest first, summing aggregates until it meets an inclusive
+// prefix, and publishes its own inclusive prefix.  A CTA only waits on CTAs
+// holding earlier tickets, which are already running, and each wait is
+// bounded (kScanWaitCycles of SM clock): a CTA that gives up sums its
+// predecessors' inputs directly instead, so the result is exact either way.
+// state: scan_state_words(n) words, zeroed before the launch (the last word
+// holds the ticket counter).
+constexpr uint64_t kScanFlagAgg = 1ull << 32;
+constexpr uint64_t kScanFlagPre = 2ull << 32;
+constexpr long long kScanWaitCycles = 1ll << 20;
+
+__device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t *p) {
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed_u64(uint64_t *p, uint64_t v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Exclusive prefix of CTA `tile` from its predecessors' state words (warp 0,
+// all lanes; the result is uniform).  false: the wait gave up.
+__device__ __forceinline__ bool scan_look_back(const uint64_t *state, int tile,
+                                               uint32_t &excl) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    excl = 0;
+    int p0 = tile - 1;
+    const long long t0 = clock64();
+    for (;;) {
+        const int p = p0 - lane;
+        const uint64_t w = p >= 0 ? ld_relaxed_u64(&state[p]) : kScanFlagPre;
+        const uint32_t flag = (uint32_t)(w >> 32);
+        const unsigned pre = __ballot_sync(FULL, flag == 2u);
+        const unsigned none = __ballot_sync(FULL, flag == 0u);
+        // lanes up to and including the nearest inclusive prefix
+        const unsigned upto = pre ? ((pre & (0u - pre)) << 1) - 1u : FULL;
+        if (none & upto) {
+            if (__any_sync(FULL, clock64() - t0 > kScanWaitCycles)) return false;
+            continue;
+        }
+        uint32_t x = ((upto >> lane) & 1u) ? (uint32_t)w : 0u;
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        int64_t i = base + k;
-        if (i < n) acc += in[i];
-    }
-    uint32_t total;
-    block_incl_scan(acc, total, s_warp);
-    if (threadIdx.x == 0) partials[blockIdx.x] = total;
-}
-
-// Phase 2: exclusive scan of the partials by one block (any count).
-__global__ void scan_partials_kernel(uint32_t *__restrict__ partials, int nparts) {
-    __shared__ uint32_t s_warp[32];
-    uint32_t carry = 0;
-    for (int base = 0; base < nparts; base += blockDim.x) {
-        int i = base + threadIdx.x;
-        uint32_t v = i < nparts ? partials[i] : 0;
-        uint32_t total;
-        uint32_t incl = block_incl_scan(v, total, s_warp);
-        if (i < nparts) partials[i] = carry + incl - v;
-        carry += total;
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(FULL, x, o);
+        excl += x;
+        if (pre) return true;
+        p0 -= 32;
     }
 }
 
-// Phase 3: rescan each block with its carry-in; inclusive or exclusive output.
-// The last element's inclusive value (the grand total) goes to *total_out.
-__global__ void scan_final_kernel(const uint32_t *__restrict__ in, int n,
-                                  const uint32_t *__restrict__ partials, bool inclusive,
-                                  uint32_t *__restrict__ out, int32_t *__restrict__ total_out) {
+__global__ void __launch_bounds__(kScanThreads)
+scan_kernel(const uint32_t *__restrict__ in, int n, uint32_t *__restrict__ out, bool inclusive,
+            int32_t *__restrict__ total_out, uint64_t *__restrict__ state,
+            uint32_t *__restrict__ ticket) {
     __shared__ uint32_t s_warp[32];
-    int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    __shared__ uint32_t s_tile, s_prefix;
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+    __syncthreads();
+    const int tile = (int)s_tile;
+    const int64_t base = (int64_t)tile * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    const bool full = base + kScanItems <= n;
     uint32_t v[kScanItems];
+    if (full && (reinterpret_cast<uintptr_t>(in) & 15) == 0) {
+        const uint4 *q = reinterpret_cast<const uint4 *>(in + base);
+#pragma unroll
+        for (int k = 0; k < kScanItems / 4; ++k) {
+            const uint4 x = q[k];
+            v[4 * k] = x.x;
+            v[4 * k + 1] = x.y;
+            v[4 * k + 2] = x.z;
+            v[4 * k + 3] = x.w;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) v[k] = base + k < n ? in[base + k] : 0u;
+    }
     uint32_t acc = 0;
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        int64_t i = base + k;
-        v[k] = i < n ? in[i] : 0;
-        acc += v[k];
-    }
+    for (int k = 0; k < kScanItems; ++k) acc += v[k];
     uint32_t total;
-    uint32_t incl = block_incl_scan(acc, total, s_warp);
-    uint32_t run = partials[blockIdx.x] + incl - acc;
+    const uint32_t incl = block_incl_scan(acc, total, s_warp);
+    if (threadIdx.x < 32) {
+        uint32_t excl = 0;
+        bool ok = true;
+        if (tile == 0) {
+            if (threadIdx.x == 0) st_relaxed_u64(&state[0], kScanFlagPre | total);
+        } else {
+            if (threadIdx.x == 0) st_relaxed_u64(&state[tile], kScanFlagAgg | total);
+            ok = scan_look_back(state, tile, excl);
+        }
+        if (threadIdx.x == 0) {
+            s_ok = ok;
+            s_prefix = excl;
+        }
+    }
+    __syncthreads();
+    if (!s_ok) {  // the wait gave up: sum the predecessors' inputs here
+        uint32_t part = 0;
+        const int64_t lim = (int64_t)tile * kScanTile;
+        for (int64_t i = threadIdx.x; i < lim; i += blockDim.x) part += in[i];
+        uint32_t sum;
+        block_incl_scan(part, sum, s_warp);
+        if (threadIdx.x == 0) s_prefix = sum;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && tile > 0) st_relaxed_u64(&state[tile], kScanFlagPre | (s_prefix + total));
+    uint32_t run = s_prefix + incl - acc;
+    if (full && (reinterpret_cast<uintptr_t>(out) & 15) == 0) {
+        uint32_t o[kScanItems];
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        int64_t i = base + k;
-        uint32_t nxt = run + v[k];
-        if (i < n) out[i] = inclusive ? nxt : run;
-        if (total_out && i == n - 1) *total_out = (int32_t)nxt;
-        run = nxt;
+        for (int k = 0; k < kScanItems; ++k) {
+            const uint32_t nxt = run + v[k];
+            o[k] = inclusive ? nxt : run;
+            run = nxt;
+        }
+        uint4 *q = reinterpret_cast<uint4 *>(out + base);
+#pragma unroll
+        for (int k = 0; k < kScanItems / 4; ++k)
+            q[k] = make_uint4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
+        if (total_out && base + kScanItems == n) *total_out = (int32_t)run;
+    } else {
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) {
+            const int64_t i = base + k;
+            const uint32_t nxt = run + v[k];
+            if (i < n) out[i] = inclusive ? nxt : run;
+            if (total_out && i == n - 1) *total_out = (int32_t)nxt;
+            run = nxt;
+        }
     }
 }
 
 inline int scan_blocks(int n) { return (n + kScanTile - 1) / kScanTile; }
 
-// Device-wide scan of n u32 values (in may alias out).  partials needs
-// scan_blocks(n) words.
+// 64-bit state words of a scan of n values (one per CTA + the ticket)
+inline size_t scan_state_words(int n) { return (size_t)scan_blocks(n > 0 ? n : 1) + 1; }
+
+// Device-wide scan of n u32 values (in and out must not overlap).  state:
+// scan_state_words(n) words; zeroed here unless the caller already did
+// (`zeroed`, e.g. with a neighbouring buffer in one memset).
 inline int device_scan(const uint32_t *in, uint32_t *out, int n, bool inclusive,
-                       uint32_t *partials, int32_t *total_out, cudaStream_t s) {
+                       uint64_t *state, int32_t *total_out, cudaStream_t s,
+                       bool zeroed = false) {
     if (n <= 0) {
         if (total_out) cudaMemsetAsync(total_out, 0, sizeof(int32_t), s);
         return LIG_OK;
     }
-    int nb = scan_blocks(n);
-    scan_reduce_kernel<<<nb, kScanThreads, 0, s>>>(in, n, partials);
-    scan_partials_kernel<<<1, 1024, 0, s>>>(partials, nb);
-    scan_final_kernel<<<nb, kScanThreads, 0, s>>>(in, n, partials, inclusive, out, total_out);
-    note_launches(3);
+    const int nb = scan_blocks(n);
+    if (!zeroed) cudaMemsetAsync(state, 0, sizeof(uint64_t) * scan_state_words(n), s);
+    scan_kernel<<<nb, kScanThreads, 0, s>>>(in, n, out, inclusive, total_out, state,
+                                            reinterpret_cast<uint32_t *>(state + nb));
+    note_launches(1);
     LIG_LAUNCH_CHECK();
     return LIG_OK;
 }
 
 // -------------------------------------------------------------- emission
-// One warp per 32 consecutive Gaussians.  The warp flattens their tile slots
-// (counts from the inclusive prefix sum) and writes them lane-per-slot, so the
-// stores are coalesced and lanes stay busy whatever the per-Gaussian counts.
-// Slot j of Gaussian g maps to tile (y0 + j / w, x0 + j % w): row-major over
-// the bbox, the emission order of csrc/forward.cu:134-142.  Gaussians whose
-// extent is <= 0 but whose count is non-zero get key 0 / id 0 slots — the
-// values the reference leaves in its zero-initialised buffers.
+// Slot j of Gaussian g (j < num_tiles_hit[g], its slots numbered from
+// cum[g - 1]) maps to tile (y0 + j / w, x0 + j % w): row-major over the
+// bbox, the emission order of csrc/forward.cu:134-142.  A Gaussian whose
+// extent is <= 0 but whose count is non-zero has "phantom" slots: tile 0 of
+// its image and the image's first Gaussian id (0 / 0 for a single image),
+// the values the reference leaves in its zero-initialised buffers.
+//
+// Every slot carries a sort value 2 g + phantom (the scatter path sorts by it
+// within a tile: ascending Gaussian id, phantoms at their Gaussian's place).
+constexpr uint32_t kPhantom = 1u;  // low bit of the sort value
+
+// sort value -> Gaussian id (phantom slots: the image's first Gaussian)
+__device__ __forceinline__ int32_t slot_id(uint32_t v, const BatchGeo &geo) {
+    const int g = (int)(v >> 1);
+    if (!(v & kPhantom)) return (int32_t)g;
+    return geo.g_off[geo.image_of_gauss(g)];
+}
+
+// One warp per 32 consecutive Gaussians hands out their tile slots
+// lane-per-slot: the warp flattens its Gaussians' slots, so lanes stay busy
+// whatever the per-Gaussian counts and consecutive lanes touch neighbouring
+// tiles.  SlotWarp holds each lane's Gaussian (its first slot in the warp's
+// flattened order, slot base, first tile, bbox width, row stride and
+// reciprocal); slot_at(sl) finds the owner of flattened slot sl with a
+// 5-step search over the inclusive count prefix, takes six broadcasts from
+// it, and computes the bbox row as a multiply-high by ceil(2^32 / w) — exact
+// while count * w <= 2^32, an integer division beyond.  A phantom slot is a
+// bbox of width 1 and row stride -1, so its key stays on the first tile.
+struct SlotWarp {
+    int64_t g0;
+    int incl, excl, slot_base, bw, stride, total;
+    uint32_t base, magic;
+};
+
+template <typename T>
+__device__ __forceinline__ bool slot_warp(int n, const T *__restrict__ xys,
+                                          const T *__restrict__ extents,
+                                          const int32_t *__restrict__ cum, const BatchGeo &geo,
+                                          int32_t *__restrict__ status, SlotWarp &sw) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    sw.g0 = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
+    if (sw.g0 >= n) return false;
+    const int g = (int)(sw.g0 + lane);
+    int cnt = 0, start = 0;
+    sw.bw = 1;
+    sw.stride = -1;
+    sw.base = 0;
+    sw.magic = 0;
+    if (g < n) {
+        const int im = geo.image_of_gauss(g);
+        const int tbx = geo.tbx[im];
+        sw.base = (uint32_t)geo.tile_off[im];
+        const int prev = g > 0 ? cum[g - 1] : 0;
+        start = prev;
+        cnt = cum[g] - prev;
+        const T ex = extents[2 * g], ey = extents[2 * g + 1];
+        if (!(ex <= (T)0 || ey <= (T)0) && cnt > 0) {
+            int x0, y0, x1, y1;
+            tile_bbox(xys[2 * g], xys[2 * g + 1], ex, ey, tbx, geo.tby(im), geo.B, x0, y0, x1, y1);
+            const int w = x1 - x0, h = y1 - y0;
+            if (w <= 0 || w * h != cnt) {
+                // inconsistent inputs: emit phantoms (in range) and flag it
+                if (status) atomicOr(status, LIG_STATUS_BADBOX);
+            } else {
+                sw.bw = w;
+                sw.stride = tbx - w;
+                sw.base += (uint32_t)y0 * (uint32_t)tbx + (uint32_t)x0;
+                if (w > 1 && (uint64_t)cnt * (uint64_t)w <= 0xffffffffull)
+                    sw.magic = 0xffffffffu / (uint32_t)w + 1u;
+            }
+        }
+    }
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += t;
+    }
+    sw.incl = incl;
+    sw.total = __shfl_sync(FULL, incl, 31);
+    sw.excl = incl - cnt;
+    sw.slot_base = start - sw.excl;
+    return true;
+}
+
+// Flattened slot sl of the warp (all lanes call it together): false when sl
+// is past the warp's slots; otherwise the slot number, tile key and sort
+// value (2 g + phantom).
+__device__ __forceinline__ bool slot_at(const SlotWarp &sw, int sl, int &slot, uint32_t &key,
+                                        uint32_t &val) {
+    const unsigned FULL = 0xffffffffu;
+    int lo = 0;  // owner = first lane whose inclusive count exceeds sl
+#pragma unroll
+    for (int step = 16; step >= 1; step >>= 1) {
+        const int v = __shfl_sync(FULL, sw.incl, lo + step - 1);
+        if (v <= sl) lo += step;
+    }
+    const int o_excl = __shfl_sync(FULL, sw.excl, lo);
+    const int o_sb = __shfl_sync(FULL, sw.slot_base, lo);
+    const uint32_t o_base = __shfl_sync(FULL, sw.base, lo);
+    const int o_bw = __shfl_sync(FULL, sw.bw, lo);
+    const int o_stride = __shfl_sync(FULL, sw.stride, lo);
+    const uint32_t o_magic = __shfl_sync(FULL, sw.magic, lo);
+    if (sl >= sw.total) return false;
+    slot = sl + o_sb;
+    const uint32_t j = (uint32_t)(sl - o_excl);
+    uint32_t q;  // bbox row of slot j
+    if (o_bw == 1) q = j;
+    else if (o_magic) q = __umulhi(j, o_magic);
+    else q = j / (uint32_t)o_bw;
+    key = o_base + j + q * (uint32_t)o_stride;
+    val = ((uint32_t)(sw.g0 + lo) << 1) | (o_stride < 0 ? kPhantom : 0u);
+    return true;
+}
+
+// f(slot, tile key, sort value) for every slot below `capacity` (slots past
+// it set LIG_STATUS_OVERFLOW).
+template <typename T, typename F>
+__device__ __forceinline__ void for_each_slot(int n, const T *__restrict__ xys,
+                                              const T *__restrict__ extents,
+                                              const int32_t *__restrict__ cum,
+                                              const BatchGeo &geo, int capacity,
+                                              int32_t *__restrict__ status, F f) {
+    SlotWarp sw;
+    if (!slot_warp<T>(n, xys, extents, cum, geo, status, sw)) return;
+    const int lane = threadIdx.x & 31;
+    bool overflow = false;
+    for (int s0 = 0; s0 < sw.total; s0 += 32) {
+        int slot;
+        uint32_t key, val;
+        if (!slot_at(sw, s0 + lane, slot, key, val)) continue;
+        if (slot >= capacity) {
+            overflow = true;
+            continue;
+        }
+        f(slot, key, val);
+    }
+    if (overflow && status) atomicOr(status, LIG_STATUS_OVERFLOW);
+}
+
+// Emission in slot order: 32-bit tile keys and/or Gaussian ids, optionally
+// the reference's int64 keys (tile << 32) and a second copy of the ids.
 template <typename T>
 __global__ void emit_kernel(int n, const T *__restrict__ xys, const T *__restrict__ extents,
                             const int32_t *__restrict__ cum, BatchGeo geo, int capacity,
                             uint32_t *__restrict__ keys,
                             int32_t *__restrict__ vals, int64_t *__restrict__ keys64,
                             int32_t *__restrict__ vals_extra, int32_t *__restrict__ status) {
-    const unsigned FULL = 0xffffffffu;
-    int lane = threadIdx.x & 31;
-    int64_t warp_id = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int64_t g0 = warp_id * 32;
-    if (g0 >= n) return;
-    int g = (int)(g0 + lane);
-    int cnt = 0, start = 0, x0 = 0, y0 = 0, bw = 1, bh = 0;
-    unsigned tbx = 1, toff = 0, g_first = 0;
-    bool valid = false;
-    if (g < n) {
-        const int im = geo.image_of_gauss(g);
-        tbx = geo.tbx[im];
-        toff = (unsigned)geo.tile_off[im];
-        g_first = (unsigned)geo.g_off[im];
-        int prev = g > 0 ? cum[g - 1] : 0;
-        start = prev;
-        cnt = cum[g] - prev;
-        T ex = extents[2 * g], ey = extents[2 * g + 1];
-        valid = !(ex <= (T)0 || ey <= (T)0);
-        if (valid && cnt > 0) {
-            int x1, y1;
-            tile_bbox(xys[2 * g], xys[2 * g + 1], ex, ey, tbx, geo.tby(im), geo.B, x0, y0, x1, y1);
-            bw = x1 - x0;
-            bh = y1 - y0;
-            if (bw <= 0 || bw * bh != cnt) {
-                // inconsistent inputs: keep emission in range and flag it
-                if (status) atomicOr(status, LIG_STATUS_BADBOX);
-                valid = false;
-                bw = 1;
-            }
-        }
-    }
-    // inclusive warp prefix of counts
-    int incl = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        int t = __shfl_up_sync(FULL, incl, o);
-        if (lane >= o) incl += t;
-    }
-    int total = __shfl_sync(FULL, incl, 31);
-    bool overflow = false;
-    for (int s0 = 0; s0 < total; s0 += 32) {
-        int s = s0 + lane;
-        // owner = first lane whose inclusive count exceeds s
-        int lo = 0;
-#pragma unroll
-        for (int step = 16; step >= 1; step >>= 1) {
-            int probe = lo + step - 1;
-            int v = __shfl_sync(FULL, incl, probe);
-            if (v <= s) lo += step;
-        }
-        int owner = lo;
-        int o_incl = __shfl_sync(FULL, incl, owner);
-        int o_cnt = __shfl_sync(FULL, cnt, owner);
-        int o_start = __shfl_sync(FULL, start, owner);
-        int o_x0 = __shfl_sync(FULL, x0, owner);
-        int o_y0 = __shfl_sync(FULL, y0, owner);
-        int o_bw = __shfl_sync(FULL, bw, owner);
-        int o_valid = __shfl_sync(FULL, (int)valid, owner);
-        unsigned o_tbx = __shfl_sync(FULL, tbx, owner);
-        unsigned o_toff = __shfl_sync(FULL, toff, owner);
-        unsigned o_first = __shfl_sync(FULL, g_first, owner);
-        if (s >= total) continue;
-        int j = s - (o_incl - o_cnt);
-        int slot = o_start + j;
-        if (slot >= capacity) {
-            overflow = true;
-            continue;
-        }
-        // phantom slots: the image's first tile and first Gaussian (0 / 0 for
-        // a single image)
-        uint32_t key = o_toff;
-        int32_t gid = (int32_t)o_first;
-        if (o_valid) {
-            int q = j / o_bw;
-            int r = j - q * o_bw;
-            key = o_toff + (uint32_t)(o_y0 + q) * o_tbx + (uint32_t)(o_x0 + r);
-            gid = (int32_t)(g0 + owner);
-        }
-        if (keys) keys[slot] = key;
-        vals[slot] = gid;
-        if (keys64) keys64[slot] = (int64_t)key << 32;
-        if (vals_extra) vals_extra[slot] = gid;
-    }
-    if (overflow && status) atomicOr(status, LIG_STATUS_OVERFLOW);
+    for_each_slot<T>(n, xys, extents, cum, geo, capacity, status,
+                     [&](int slot, uint32_t key, uint32_t v) {
+                         const int32_t gid = slot_id(v, geo);
+                         if (keys) keys[slot] = key;
+                         if (vals) vals[slot] = gid;
+                         if (keys64) keys64[slot] = (int64_t)key << 32;
+                         if (vals_extra) vals_extra[slot] = gid;
+                     });
 }
 
 // ----------------------------------------------------------------- radix
@@ -446,100 +587,18 @@ __global__ void flag_overflow_kernel(const int32_t *d_total, int capacity, int32
 #ifndef LIG_BIN_SCATTER
 #define LIG_BIN_SCATTER 1
 #endif
-constexpr uint32_t kPhantom = 1u;  // low bit of the sort key (key = 2 g + phantom)
 constexpr int kSegSmem = 4096;     // sorted in shared memory up to this length (long tiles)
 constexpr int kSegWarps = 4;       // warps per CTA of the per-tile sort
 
-// The emission enumeration of emit_kernel, calling f(slot, key, sort_value)
-// for every slot below `capacity` (slots past it set overflow).
-template <typename T, typename F>
-__device__ __forceinline__ void for_each_slot(int n, const T *__restrict__ xys,
-                                              const T *__restrict__ extents,
-                                              const int32_t *__restrict__ cum,
-                                              const BatchGeo &geo, int capacity,
-                                              int32_t *__restrict__ status, F f) {
-    const unsigned FULL = 0xffffffffu;
-    int lane = threadIdx.x & 31;
-    int64_t warp_id = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int64_t g0 = warp_id * 32;
-    if (g0 >= n) return;
-    int g = (int)(g0 + lane);
-    int cnt = 0, start = 0, x0 = 0, y0 = 0, bw = 1, bh = 0;
-    unsigned tbx = 1, toff = 0;
-    bool valid = false;
-    if (g < n) {
-        const int im = geo.image_of_gauss(g);
-        tbx = geo.tbx[im];
-        toff = (unsigned)geo.tile_off[im];
-        int prev = g > 0 ? cum[g - 1] : 0;
-        start = prev;
-        cnt = cum[g] - prev;
-        T ex = extents[2 * g], ey = extents[2 * g + 1];
-        valid = !(ex <= (T)0 || ey <= (T)0);
-        if (valid && cnt > 0) {
-            int x1, y1;
-            tile_bbox(xys[2 * g], xys[2 * g + 1], ex, ey, tbx, geo.tby(im), geo.B, x0, y0, x1, y1);
-            bw = x1 - x0;
-            bh = y1 - y0;
-            if (bw <= 0 || bw * bh != cnt) {
-                if (status) atomicOr(status, LIG_STATUS_BADBOX);
-                valid = false;
-                bw = 1;
-            }
-        }
-    }
-    int incl = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        int t = __shfl_up_sync(FULL, incl, o);
-        if (lane >= o) incl += t;
-    }
-    int total = __shfl_sync(FULL, incl, 31);
-    bool overflow = false;
-    for (int s0 = 0; s0 < total; s0 += 32) {
-        int sl = s0 + lane;
-        int lo = 0;
-#pragma unroll
-        for (int step = 16; step >= 1; step >>= 1) {
-            int probe = lo + step - 1;
-            int v = __shfl_sync(FULL, incl, probe);
-            if (v <= sl) lo += step;
-        }
-        int owner = lo;
-        int o_incl = __shfl_sync(FULL, incl, owner);
-        int o_cnt = __shfl_sync(FULL, cnt, owner);
-        int o_start = __shfl_sync(FULL, start, owner);
-        int o_x0 = __shfl_sync(FULL, x0, owner);
-        int o_y0 = __shfl_sync(FULL, y0, owner);
-        int o_bw = __shfl_sync(FULL, bw, owner);
-        int o_valid = __shfl_sync(FULL, (int)valid, owner);
-        unsigned o_tbx = __shfl_sync(FULL, tbx, owner);
-        unsigned o_toff = __shfl_sync(FULL, toff, owner);
-        if (sl >= total) continue;
-        int j = sl - (o_incl - o_cnt);
-        int slot = o_start + j;
-        if (slot >= capacity) {
-            overflow = true;
-            continue;
-        }
-        uint32_t key = o_toff;
-        uint32_t val = ((uint32_t)(g0 + owner) << 1) | kPhantom;
-        if (o_valid) {
-            int q = j / o_bw;
-            int r = j - q * o_bw;
-            key = o_toff + (uint32_t)(o_y0 + q) * o_tbx + (uint32_t)(o_x0 + r);
-            val = (uint32_t)(g0 + owner) << 1;
-        }
-        f(slot, key, val);
-    }
-    if (overflow && status) atomicOr(status, LIG_STATUS_OVERFLOW);
-}
-
-// 1. per-tile counts (slots below capacity; the rest is flagged as overflow)
+// 1. per-tile counts (slots below capacity; the rest is flagged as overflow,
+// as is a total above the capacity)
 template <typename T>
 __global__ void tile_count_kernel(int n, const T *__restrict__ xys, const T *__restrict__ ext,
-                                  const int32_t *__restrict__ cum, BatchGeo geo, int capacity,
-                                  uint32_t *__restrict__ tcount, int32_t *__restrict__ status) {
+                                  const int32_t *__restrict__ cum, const int32_t *d_total,
+                                  BatchGeo geo, int capacity, uint32_t *__restrict__ tcount,
+                                  int32_t *__restrict__ status) {
+    if (blockIdx.x == 0 && threadIdx.x == 0 && *d_total > capacity)
+        atomicOr(status, LIG_STATUS_OVERFLOW);
     for_each_slot<T>(n, xys, ext, cum, geo, capacity, status,
                      [&](int, uint32_t key, uint32_t) { atomicAdd(&tcount[key], 1u); });
 }
@@ -547,30 +606,38 @@ __global__ void tile_count_kernel(int n, const T *__restrict__ xys, const T *__r
 // 3. scatter into the tile's range: `cursor` starts as the exclusive scan of
 // the counts (each tile's first position) and one atomic per slot returns
 // the slot's absolute position; afterwards cursor[t] = start + count.
+// Each lane takes two slots per trip (64 apart) and issues both atomics
+// before either store, so two atomic round trips are in flight per lane.
 template <typename T>
 __global__ void tile_scatter_kernel(int n, const T *__restrict__ xys, const T *__restrict__ ext,
                                     const int32_t *__restrict__ cum, BatchGeo geo, int capacity,
                                     uint32_t *__restrict__ cursor, uint32_t *__restrict__ out,
                                     int64_t *__restrict__ keys64, int32_t *__restrict__ gids) {
-    for_each_slot<T>(n, xys, ext, cum, geo, capacity, nullptr,
-                     [&](int slot, uint32_t key, uint32_t val) {
-                         out[atomicAdd(&cursor[key], 1u)] = val;
-                         if (keys64) {  // the reference's emission-order outputs
-                             const bool ph = (val & kPhantom) != 0;
-                             const int g = (int)(val >> 1);
-                             const int im = geo.image_of_gauss(g);
-                             keys64[slot] = ph ? (int64_t)geo.tile_off[im] << 32
-                                               : (int64_t)key << 32;
-                             gids[slot] = ph ? geo.g_off[im] : g;
-                         }
-                     });
-}
-
-// sort value -> Gaussian id (phantom slots: the image's first Gaussian)
-__device__ __forceinline__ int32_t slot_id(uint32_t v, const BatchGeo &geo) {
-    const int g = (int)(v >> 1);
-    if (!(v & kPhantom)) return (int32_t)g;
-    return geo.g_off[geo.image_of_gauss(g)];
+    SlotWarp sw;
+    if (!slot_warp<T>(n, xys, ext, cum, geo, nullptr, sw)) return;
+    const int lane = threadIdx.x & 31;
+    for (int s0 = 0; s0 < sw.total; s0 += 64) {
+        int sa, sb;
+        uint32_t ka, kb, va, vb;
+        bool oka = slot_at(sw, s0 + lane, sa, ka, va);
+        bool okb = slot_at(sw, s0 + 32 + lane, sb, kb, vb);
+        oka = oka && sa < capacity;
+        okb = okb && sb < capacity;
+        const uint32_t pa = oka ? atomicAdd(&cursor[ka], 1u) : 0u;
+        const uint32_t pb = okb ? atomicAdd(&cursor[kb], 1u) : 0u;
+        if (oka) out[pa] = va;
+        if (okb) out[pb] = vb;
+        if (keys64) {  // the reference's emission-order outputs
+            if (oka) {
+                keys64[sa] = (int64_t)ka << 32;
+                gids[sa] = slot_id(va, geo);
+            }
+            if (okb) {
+                keys64[sb] = (int64_t)kb << 32;
+                gids[sb] = slot_id(vb, geo);
+            }
+        }
+    }
 }
 
 // Bitonic sort of E * 32 values held E per lane (value k of lane l is
@@ -722,7 +789,7 @@ tile_sort_long_kernel(BatchGeo geo, const uint32_t *__restrict__ tcount,
 // ------------------------------------------------------- workspace plan
 struct BinPlan {
     int bits, passes, dbits, bins, nblk;
-    size_t off_k0, off_v0, off_k1, off_hist, off_part, total;
+    size_t off_k0, off_v0, off_k1, off_hist, off_hscan, off_part, total;
 };
 
 inline size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -744,17 +811,19 @@ inline BinPlan make_plan(int capacity, int num_tiles) {
     p.off_k1 = off; off = align_up(off + 4 * cap);
     size_t hist_n = (size_t)p.bins * p.nblk;
     p.off_hist = off; off = align_up(off + 4 * hist_n);
-    size_t nparts = (hist_n + kScanTile - 1) / kScanTile + 1;
-    p.off_part = off; off = align_up(off + 4 * nparts);
+    p.off_hscan = off; off = align_up(off + 4 * hist_n);
+    p.off_part = off; off = align_up(off + 8 * scan_state_words((int)hist_n));
     p.total = off;
     return p;
 }
 
-// Workspace of the scatter path: per-tile counts and cursors (the cursors
-// start as the scan of the counts), scan partials, the long-tile list.  The sort keys are scattered
-// into gid_sorted itself and sorted in place there.
+// Workspace of the scatter path: per-tile counts, the scan state, the
+// long-tile list (its first word is the length) and the per-tile cursors
+// (they start as the scan of the counts).  The first three are adjacent so
+// that one memset clears the counts, the scan state and the list length.
+// The sort keys are scattered into gid_sorted itself and sorted in place.
 struct ScatterPlan {
-    size_t off_count, off_cursor, off_part, off_long, total;
+    size_t off_count, off_part, off_long, off_cursor, total;
 };
 
 inline ScatterPlan make_scatter_plan(int num_tiles) {
@@ -762,9 +831,9 @@ inline ScatterPlan make_scatter_plan(int num_tiles) {
     size_t t = (size_t)(num_tiles > 0 ? num_tiles : 1);
     size_t off = 0;
     p.off_count = off; off = align_up(off + 4 * t);
-    p.off_cursor = off; off = align_up(off + 4 * t);
-    p.off_part = off; off = align_up(off + 4 * ((t + kScanTile - 1) / kScanTile + 1));
+    p.off_part = off; off = align_up(off + 8 * scan_state_words((int)t));
     p.off_long = off; off = align_up(off + 4 * (t + 1));
+    p.off_cursor = off; off = align_up(off + 4 * t);
     p.total = off;
     return p;
 }
@@ -781,7 +850,7 @@ int run_bin_scatter(const BatchGeo &geo, const void *xys, const void *ext, const
     char *base = (char *)ws;
     uint32_t *tcount = (uint32_t *)(base + p.off_count);
     uint32_t *cursor = (uint32_t *)(base + p.off_cursor);
-    uint32_t *part = (uint32_t *)(base + p.off_part);
+    uint64_t *part = (uint64_t *)(base + p.off_part);
     int32_t *long_list = (int32_t *)(base + p.off_long);
     cudaMemsetAsync(status, 0, sizeof(int32_t), s);
     if (n == 0 || capacity == 0) {
@@ -791,16 +860,15 @@ int run_bin_scatter(const BatchGeo &geo, const void *xys, const void *ext, const
         LIG_LAUNCH_CHECK();
         return LIG_OK;
     }
-    cudaMemsetAsync(tcount, 0, sizeof(uint32_t) * (size_t)T_, s);
-    cudaMemsetAsync(long_list, 0, sizeof(int32_t), s);
+    // counts, scan state and the long-list length in one memset
+    cudaMemsetAsync(tcount, 0, p.off_long + sizeof(int32_t) - p.off_count, s);
     const int warps = (n + 31) / 32;
     const int eblocks = (warps * 32 + 255) / 256;
-    tile_count_kernel<T><<<eblocks, 256, 0, s>>>(n, (const T *)xys, (const T *)ext, cum, geo,
-                                                 capacity, tcount, status);
-    flag_overflow_kernel<<<1, 1, 0, s>>>(d_total, capacity, status);
-    note_launches(2);
+    tile_count_kernel<T><<<eblocks, 256, 0, s>>>(n, (const T *)xys, (const T *)ext, cum, d_total,
+                                                 geo, capacity, tcount, status);
+    note_launches(1);
     LIG_LAUNCH_CHECK();
-    int rc = device_scan(tcount, cursor, T_, false, part, nullptr, s);
+    int rc = device_scan(tcount, cursor, T_, false, part, nullptr, s, /*zeroed=*/true);
     if (rc) return rc;
     uint32_t *vals = (uint32_t *)gid_sorted;
     tile_scatter_kernel<T><<<eblocks, 256, 0, s>>>(n, (const T *)xys, (const T *)ext, cum, geo,
@@ -810,7 +878,7 @@ int run_bin_scatter(const BatchGeo &geo, const void *xys, const void *ext, const
     tile_sort_kernel<<<sort_blocks, 32 * kSegWarps, 0, s>>>(geo, tcount, cursor, capacity, vals,
                                                           gid_sorted, (int2 *)tile_bins,
                                                           isect_sorted, long_list);
-    tile_sort_long_kernel<<<148 * 4, kLongThreads, 0, s>>>(geo, tcount, cursor, capacity, vals,
+    tile_sort_long_kernel<<<148 * 2, kLongThreads, 0, s>>>(geo, tcount, cursor, capacity, vals,
                                                            gid_sorted, long_list);
     note_launches(3);
     LIG_LAUNCH_CHECK();
@@ -834,7 +902,8 @@ int run_bin(const BatchGeo &geo, const void *xys, const void *ext, const int32_t
     int32_t *v0 = (int32_t *)(base + p.off_v0);
     uint32_t *k1 = (uint32_t *)(base + p.off_k1);
     uint32_t *hist = (uint32_t *)(base + p.off_hist);
-    uint32_t *part = (uint32_t *)(base + p.off_part);
+    uint32_t *hscan = (uint32_t *)(base + p.off_hscan);
+    uint64_t *part = (uint64_t *)(base + p.off_part);
 
     cudaMemsetAsync(status, 0, sizeof(int32_t), s);
     cudaMemsetAsync(tile_bins, 0, sizeof(int32_t) * 2 * (size_t)T_, s);
@@ -882,10 +951,10 @@ int run_bin(const BatchGeo &geo, const void *xys, const void *ext, const int32_t
         int shift = pass * p.dbits;
         radix_upsweep_kernel<<<p.nblk, kSortThreads, sizeof(uint32_t) * p.bins, s>>>(
             ka, d_total, capacity, shift, p.bins, hist, p.nblk);
-        int rc = device_scan(hist, hist, hist_n, false, part, nullptr, s);
+        int rc = device_scan(hist, hscan, hist_n, false, part, nullptr, s);
         if (rc) return rc;
         radix_downsweep_kernel<<<p.nblk, kSortThreads, dsm, s>>>(
-            ka, va, kb, vb, d_total, capacity, shift, p.bins, hist, p.nblk);
+            ka, va, kb, vb, d_total, capacity, shift, p.bins, hscan, p.nblk);
         note_launches(2);
         LIG_LAUNCH_CHECK();
         uint32_t *tk = ka; ka = kb; kb = tk;
@@ -908,12 +977,17 @@ int run_bin(const BatchGeo &geo, const void *xys, const void *ext, const int32_t
 using namespace lig;
 
 extern "C" size_t lig_cumsum_workspace_bytes(int n) {
-    return sizeof(uint32_t) * ((size_t)scan_blocks(n > 0 ? n : 1) + 1);
+    return sizeof(uint64_t) * scan_state_words(n);
 }
 
 extern "C" int lig_cumsum_tiles(int n, const int32_t *counts, int32_t *cum, int32_t *total,
                                 void *workspace, size_t workspace_bytes, void *stream) {
     if (n < 0 || !total || (n > 0 && (!counts || !cum || !workspace))) return LIG_ERR_INVALID;
+    // the scan reads its predecessors' inputs when a wait gives up: no aliasing
+    if (n > 0 && (const char *)counts < (const char *)(cum + n) &&
+        (const char *)cum < (const char *)(counts + n))
+        return LIG_ERR_INVALID;
+    if ((reinterpret_cast<uintptr_t>(workspace) & 7) != 0) return LIG_ERR_INVALID;
     if (workspace_bytes < lig_cumsum_workspace_bytes(n)) return LIG_ERR_WORKSPACE;
     cudaStream_t s = (cudaStream_t)stream;
     if (n == 0) {
@@ -921,7 +995,7 @@ extern "C" int lig_cumsum_tiles(int n, const int32_t *counts, int32_t *cum, int3
         LIG_LAUNCH_CHECK();
         return LIG_OK;
     }
-    return device_scan((const uint32_t *)counts, (uint32_t *)cum, n, true, (uint32_t *)workspace,
+    return device_scan((const uint32_t *)counts, (uint32_t *)cum, n, true, (uint64_t *)workspace,
                        total, s);
 }
 
