@@ -675,6 +675,9 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
 #ifndef LIG_RASTER_BWD_SPLIT
 #define LIG_RASTER_BWD_SPLIT 1  // split a short list's Gaussians across lanes (measured faster)
 #endif
+#ifndef LIG_RASTER_BWD_SPLIT1
+#define LIG_RASTER_BWD_SPLIT1 20  // with up to this many Gaussians left, 2 lanes take one
+#endif
 #ifndef LIG_RASTER_BWD_LANE_ELLIPSE
 #define LIG_RASTER_BWD_LANE_ELLIPSE 1  // ellipse culling by the warp's lanes (measured faster)
 #endif
@@ -1226,15 +1229,16 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
             nmine += __popc(mask);
         }
         __syncwarp();
-        for (int g0 = 0; g0 < nmine; g0 += 32) {
-            // lanes per Gaussian: with fewer than 17 / 9 / 5 Gaussians left,
-            // 2 / 4 / 8 lanes share one Gaussian, lane part p taking pixels
+        for (int g0 = 0, lsplit = 0; g0 < nmine; g0 += 32 >> lsplit) {
+            // lanes per Gaussian: with at most 4 / 8 / LIG_RASTER_BWD_SPLIT1
+            // Gaussians left, 8 / 4 / 2 lanes share one Gaussian (a round
+            // then takes 4 / 8 / 16 of them), lane part p taking pixels
             // p, p + 2^lsplit, ... of the region (interleaved, so the group's
             // pixel records sit in different shared-memory banks); their
             // sums are combined below
             const int left = min(32, nmine - g0);
-            const int lsplit = !LIG_RASTER_BWD_SPLIT ? 0 : left <= 4 ? 3 : left <= 8 ? 2
-                                                             : left <= 16 ? 1 : 0;
+            lsplit = !LIG_RASTER_BWD_SPLIT ? 0 : left <= 4 ? 3 : left <= 8 ? 2
+                                                 : left <= LIG_RASTER_BWD_SPLIT1 ? 1 : 0;
             const int gi = lane >> lsplit, part = lane & ((1 << lsplit) - 1);
             const int jstep = 1 << lsplit;
             const int slot = gi < left ? (int)my_list[g0 + gi] : -1;

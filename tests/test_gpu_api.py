@@ -319,6 +319,29 @@ def test_fused_l2_forward_diff_and_loss(H, W, B, n):
         assert rel_err(np_(gb[i]), np_(full[i])) <= 1e-5
 
 
+@pytest.mark.parametrize("seed,diag,offdiag", [(21, (0.3, 8.0), 4.0),    # thin, tilted
+                                              (22, (0.2, 1.0), 0.05),   # small, axis-aligned
+                                              (23, (2.0, 20.0), 8.0)])  # large, tilted
+def test_fused_l2_forward_row_blocks_exact(seed, diag, offdiag):
+    """The fused forward with four pixels per lane (>= 4096 tiles) evaluates
+    only the 4-row blocks of its 8x16 region that a Gaussian can reach; on
+    thin, small and large tilted Gaussians the masked difference and the
+    final indices stay equal to the plain forward's, bit for bit."""
+    H, W, B, n = 1024, 1040, 16, 12000
+    means, L, colors, _ = scene(n, H, W, diag=diag, seed=seed, offdiag_std=offdiag)
+    g = torch.Generator().manual_seed(seed)
+    target = torch.rand(H, W, 3, generator=g).cuda()
+    xys, ext, con, cnt = ops.project_fwd(L, means, None, H, W, B, True)
+    b = ops.bin_gaussians(xys, ext, cnt, H, W, B)
+    img, _, _, _, _, fin = ops.raster_fwd(H, W, B, b.gaussian_ids_sorted, b.tile_bins, b.total,
+                                          xys, con, colors, None, False)
+    diff, fin2, _ = ops.raster_fwd_l2(H, W, B, b.gaussian_ids_sorted, b.tile_bins, b.total,
+                                      xys, con, colors, None, target)
+    exp = torch.where((img >= 0) & (img <= 1), torch.clamp(img, 0, 1) - target,
+                      torch.zeros_like(img))
+    assert torch.equal(diff, exp) and torch.equal(fin2, fin)
+
+
 def test_binning_grows_sort_shared_memory_between_calls():
     """A process whose first binning needs 9-bit radix digits and whose next
     one needs 10-bit digits (more shared memory in the downsweep) must opt
