@@ -2,16 +2,18 @@
 
 Workload (one "step"): one fit iteration of LIG's full-resolution level —
 2M Cholesky Gaussians (means U[0,8192)^2, diagonals U[0.5,6], off-diagonal
-N(0,0.5), colours U(0,1)) on an 8192x8192 RGB fp32 target (a render of 2M
-seeded teacher Gaussians plus 1/f^2 noise of std 0.03, clipped): project ->
+N(0,0.5), colours U(0,1)) on an 8192x8192 RGB target (a render of 2M
+seeded teacher Gaussians plus 1/f^2 noise of std 0.03, clipped and stored as
+8-bit RGB, the form of the PNG images LIG's train.py reads and converts with
+ToTensor; the loss kernel reads each byte as byte / 255): project ->
 bin -> raster forward with the clamped L2 loss fused in -> raster backward
 -> projection backward -> Adam, as lig_b200.fit.LevelFit.step runs it (its
 CUDA-graph engine: one graph replay per iteration).  Synthetic data stands
 in for the DIV2K/STimage images (not available offline).
 
   value  device-timed iterations/s, target resident in HBM (inputs > L2).
-  e2e    same loop through LevelFit.step with the step's input (the target
-         image) copied host->device from pinned memory every step (double
+  e2e    same loop through LevelFit.step with the step's input (the 8-bit
+         target image) copied host->device from pinned memory every step (double
          buffered on a copy stream, overlapping the previous step) and the
          loss copied back to pinned host memory every step.
   roofline  the dominant kernel's algorithmic rate (reference-defined
@@ -157,9 +159,15 @@ def make_workload(size: int, n: int, device):
     n_teacher = max(1, int(N_TEACHER * (size / H) ** 2))
     target = make_target(size, size, n_teacher, DIAG, noise="spectral", noise_std=0.03,
                          device=device, block=BLOCK)
+    target = torch.round(target * 255).clamp_(0, 255).to(torch.uint8)  # 8-bit RGB image
     fit = LevelFit(n, size, size, device=device, lr=1e-3, block=BLOCK, diag=DIAG,
                    seed=synthetic.SEED_INIT)
     return target, fit
+
+
+def workload_name(size: int, n: int) -> str:
+    return (f"LIG level-2 fit step, {size}x{size} RGB (8-bit target), {n} Gaussians "
+            f"(diag U[0.5,6]), 16x16 tiles, L2 + Adam")
 
 
 def evaluations(fit) -> tuple[int, int]:
@@ -222,7 +230,7 @@ def cpu_band_sample(size, n, target_secs, steps, diag=DIAG):
     def band_step(rows):
         sel = (means[:, 1] >= -32) & (means[:, 1] < rows + 32)
         m, L, c = means[sel], chol[sel], colors[sel]
-        tgt = rng.uniform(0, 1, (rows, size, 3)).astype(np.float32)
+        tgt = (rng.integers(0, 256, (rows, size, 3)) / 255).astype(np.float32)
         state = {}
         t0 = time.perf_counter()
         xys, ext, con, cnt = O.project_fwd(L, m, None, rows, size, BLOCK, chol=True)
@@ -263,8 +271,7 @@ def run_reference(args, rank, world):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": f"LIG level-2 fit step, {size}x{size} RGB, {n} Gaussians, "
-                                   f"16x16 tiles (CPU: band sample)",
+            "config": {"workload": workload_name(size, n),
                        "global_batch": 1, "parallelism": "replicas"},
             "cpu_baseline": {"value": val, "unit": "iters/s", "cores": cores, "kind": "port",
                              "sample": desc},
@@ -401,6 +408,8 @@ def run_lig(args, rank, world, local_rank):
     else:
         roof = {"bound": "hbm", "achieved": None, "peak": None, "unit": "GB/s", "frac": None,
                 "traffic": None, "kernel": dom}
+    tbytes = int(target.numel() * target.element_size())
+    diff_bytes = int(target.numel() * 4)
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         v, cores, desc, _, _ = cpu_band_sample(size, n, args.cpu_seconds, 1)
@@ -409,14 +418,15 @@ def run_lig(args, rank, world, local_rank):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": f"LIG level-2 fit step, {size}x{size} RGB fp32, {n} "
-                                   f"Gaussians (diag U[0.5,6]), 16x16 tiles, L2 + Adam",
+            "config": {"workload": workload_name(size, n),
                        "global_batch": world, "seq_len": None,
                        "parallelism": f"replicas{world}",
-                       "l2": "inputs > L2 (805 MB image per step)",
+                       "l2": f"inputs > L2 ({tbytes / 1e6:.0f} MB target read and "
+                             f"{diff_bytes / 1e6:.0f} MB masked difference written and read "
+                             f"per step)",
                        "intersections": m_isect, "evaluations": evals},
             "e2e": {"value": e2e, "unit": "iters/s",
-                    "h2d_bytes_per_step": int(target.numel() * 4), "d2h_bytes_per_step": 4},
+                    "h2d_bytes_per_step": tbytes, "d2h_bytes_per_step": 4},
             "gpu_launches": launches, "gpu_launches_per_step": launches_per_step,
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
             "kernels": kernels}

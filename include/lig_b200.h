@@ -134,7 +134,8 @@ int lig_tile_bin_edges(int num_intersects, const int64_t *isect_ids_sorted, int 
 
 /* ---------------------------------------------------------- rasterization */
 
-/* Workspace bytes for lig_raster_fwd / lig_raster_bwd (packed records). */
+/* Workspace bytes for lig_raster_fwd / lig_raster_bwd (packed records; the
+ * workspace must be 16-byte aligned, LIG_ERR_INVALID otherwise). */
 size_t lig_raster_workspace_bytes(int dtype, int num_points);
 
 /* Weighted-sum rasterizer forward.  out_dx/out_dy/out_dxy == NULL selects the
@@ -369,6 +370,23 @@ int lig_raster_fwd_l2_batch(int dtype, int n_img, const int32_t *heights, const 
                             const void *target, int persistent, int32_t *work, void *workspace,
                             size_t workspace_bytes, double *tile_partials, void *diff,
                             int32_t *final_idx, void *loss, void *per_image, void *stream);
+
+/* lig_raster_fwd_l2_batch with an 8-bit target [sum_i H_i W_i, 3] (RGB
+ * images as stored): each byte t counts as t / 255 rounded to nearest — the
+ * float torchvision's ToTensor gives, which train.py's image loading uses
+ * (train.py:30, 209-214) — so every output equals
+ * lig_raster_fwd_l2_batch's with that float target, for a quarter of the
+ * target's bytes.  No reference counterpart (the reference keeps the target
+ * as fp32 on the device). */
+int lig_raster_fwd_l2_u8_batch(int dtype, int n_img, const int32_t *heights,
+                               const int32_t *widths, const int32_t *counts, int block_width,
+                               const int32_t *gaussian_ids_sorted, const int32_t *tile_bins,
+                               const int32_t *num_intersects, const int32_t *cum,
+                               const void *xys, const void *conics, const void *colors,
+                               const void *opacities, const uint8_t *target, int persistent,
+                               int32_t *work, void *workspace, size_t workspace_bytes,
+                               double *tile_partials, void *diff, int32_t *final_idx, void *loss,
+                               void *per_image, void *stream);
 
 /* Batched lig_raster_bwd_diff (per-image scale 2 / (3 H_i W_i)). */
 int lig_raster_bwd_diff_batch(int dtype, int n_img, const int32_t *heights,

@@ -82,6 +82,8 @@ SIGNATURES = {
                                 P, P, P]),
     "lig_raster_fwd_l2_batch": (I, [I, I, P, P, P, I, P, P, P, P, P, P, P, P, P, I, P, P, SZ,
                                     P, P, P, P, P, P]),
+    "lig_raster_fwd_l2_u8_batch": (I, [I, I, P, P, P, I, P, P, P, P, P, P, P, P, P, I, P, P, SZ,
+                                    P, P, P, P, P, P]),
     "lig_raster_bwd_diff_batch": (I, [I, I, P, P, P, I, P, P, P, P, P, P, P, P, P, P, P, D, I,
                                       P, P, SZ, P, P, P, P, P, P]),
     "lig_adam_scratch_bytes": (SZ, []),

@@ -132,7 +132,9 @@ class BatchStats:
 class BatchedFit:
     """Fits one Gaussian set per target image, all images per launch.
 
-    targets: list of [H_i, W_i, 3] fp32 CUDA tensors; counts: Gaussians per
+    targets: list of [H_i, W_i, 3] CUDA tensors, all fp32 or all uint8 (RGB
+    images as stored, read as byte / 255 like torchvision's ToTensor, for a
+    quarter of the bytes to upload and read); counts: Gaussians per
     image; init: optional list per image of (means, cholesky, colors) or of
     a FitState (parameters plus Adam moments and step, to resume a fit); else
     seeded synthetic Gaussians, seed seed_base + i; block: tile size;
@@ -181,7 +183,9 @@ class BatchedFit:
                 L.points_of(self.means, i).copy_(mu)
                 L.points_of(self.chol, i).copy_(ch)
                 L.points_of(self.rgbs, i).copy_(co)
-            self.target = torch.cat([t.reshape(-1, 3).to(f32) for t in targets]).contiguous()
+            u8 = all(t.dtype == torch.uint8 for t in targets)
+            tdt = torch.uint8 if u8 else f32
+            self.target = torch.cat([t.reshape(-1, 3).to(tdt) for t in targets]).contiguous()
         # per-step buffers
         self.xys = torch.empty(N, 2, dtype=f32, **kw)
         self.ext = torch.empty(N, 2, dtype=f32, **kw)
@@ -300,7 +304,8 @@ class BatchedFit:
         st = self._stream()
         tgt = self.target if target is None else target
         self._bin(st)
-        call("lig_raster_fwd_l2_batch", _lib.LIG_F32, *L.args(), L.block, _p(self.gids),
+        fwd = "lig_raster_fwd_l2_u8_batch" if tgt.dtype == torch.uint8 else "lig_raster_fwd_l2_batch"
+        call(fwd, _lib.LIG_F32, *L.args(), L.block, _p(self.gids),
              _p(self.bins), _p(self.total), _p(self.cum), _p(self.xys), _p(self.con),
              _p(self.rgbs), None, _p(tgt), int(self.persistent), _p(self.work),
              _p(self.r_ws), self.r_ws.numel(), _p(self.partials), _p(self.img), _p(self.fin),
@@ -353,10 +358,10 @@ class BatchedFit:
         if target is None:
             return None
         t = target.reshape(-1, 3)
-        if (t.dtype != torch.float32 or t.device != self.dev or not t.is_contiguous()
-                or t.shape[0] != self.L.pixels):
-            raise ValueError("target must be a contiguous float32 CUDA tensor with the batch's "
-                             "[pixels, 3] values")
+        if (t.dtype not in (torch.float32, torch.uint8) or t.device != self.dev
+                or not t.is_contiguous() or t.shape[0] != self.L.pixels):
+            raise ValueError("target must be a contiguous float32 or uint8 CUDA tensor with the "
+                             "batch's [pixels, 3] values")
         return t
 
     def step(self, target: Optional[torch.Tensor] = None):
@@ -431,6 +436,8 @@ class BatchedFit:
         for i in range(self.L.n):
             a = torch.clamp(self.L.image(self.img, i), 0, 1)
             b = self.L.image(self.target, i)
+            if b.dtype == torch.uint8:
+                b = b.float() / 255
             mse = torch.mean((a - b) ** 2).item()
             out.append(10 * math.log10(1.0 / max(mse, 1e-20)))
         return out

@@ -58,12 +58,19 @@ template <typename T> struct alignas(16) Rec {
 // where the reference's per-pixel tests must run everywhere in the tile.
 // HALF: the record carries a/2 and c/2 in place of a and c (the fused-loss
 // forward, see sigma_half); the cull data are computed from the full conic.
+// zero (backward): also clears the Gaussian's zero_stride accumulators there
+// (zero_stride * sizeof(T) a multiple of 16 bytes, 16-byte aligned).
 template <typename T, bool HALF>
 __global__ void pack_kernel(int n, const T *__restrict__ xys, const T *__restrict__ conics,
                             const T *__restrict__ colors, const T *__restrict__ opac,
-                            Rec<T> *__restrict__ recs) {
+                            Rec<T> *__restrict__ recs, T *__restrict__ zero, int zero_stride) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    if (zero) {
+        float4 *z = reinterpret_cast<float4 *>(zero + (size_t)i * zero_stride);
+        const int nv = zero_stride * (int)sizeof(T) / 16;
+        for (int k = 0; k < nv; ++k) z[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
     Rec<T> r;
     r.x = xys[2 * i];
     r.y = xys[2 * i + 1];
@@ -420,11 +427,31 @@ struct FwdAcc {
 // forward writes the masked difference diff = (0 <= x <= 1) ? clamp(x) - t : 0
 // (what the loss gradient needs per pixel) and each tile adds
 // (clamp(x) - t)^2 over its pixels into one fp64 partial (fixed-order block
-// reduction, so the loss is deterministic).  target == null: plain forward.
+// reduction, so the loss is deterministic).  No target: plain forward.
+// An 8-bit target (an RGB image as stored) is read as t = byte / 255 rounded
+// to nearest: the float value torchvision's ToTensor gives (train.py's image
+// loading), so the result equals the fp32 path fed that float target.  In
+// float the quotient is q = b * r (r = 1/255 rounded) refined by one
+// residual-correction step (Markstein): e = fma(-q, 255, b), t = fma(e, r, q)
+// — equal to the correctly rounded b / 255 for every byte b (checked against
+// the host's division for all 256 values), with no division.
 template <typename T> struct L2Fwd {
     const T *target;
     double *tile_partial;  // [total tiles]
+    const uint8_t *target_u8 = nullptr;
+    __device__ __forceinline__ bool on() const { return target || target_u8; }
+    __device__ __forceinline__ T at(int i) const;
 };
+template <> __device__ __forceinline__ float L2Fwd<float>::at(int i) const {
+    if (!target_u8) return target[i];
+    constexpr float r = 0.003921568859368563f;  // 1/255 rounded to nearest (0x3b808081)
+    const float b = (float)target_u8[i];
+    const float q = __fmul_rn(b, r);
+    return __fmaf_rn(__fmaf_rn(-q, 255.0f, b), r, q);
+}
+template <> __device__ __forceinline__ double L2Fwd<double>::at(int i) const {
+    return target_u8 ? __ddiv_rn((double)target_u8[i], 255.0) : target[i];
+}
 
 template <typename T>
 __device__ __forceinline__ void block_sum_to(double v, double *dst) {
@@ -453,12 +480,12 @@ __device__ __forceinline__ double fwd_write(const FwdAcc<T, GA> &acc, bool insid
                                             const L2Fwd<T> &l2) {
     if (!inside) return 0.0;
     final_idx[pix] = acc.cur;
-    if (l2.target) {
+    if (l2.on()) {
         double sq = 0;
         const T x[3] = {acc.r, acc.g, acc.b};
 #pragma unroll
         for (int ch = 0; ch < 3; ++ch) {
-            const T d = min(max(x[ch], (T)0), (T)1) - l2.target[3 * pix + ch];
+            const T d = min(max(x[ch], (T)0), (T)1) - l2.at(3 * pix + ch);
             sq += (double)(d * d);
             img[3 * pix + ch] = (x[ch] >= (T)0 && x[ch] <= (T)1) ? d : (T)0;
         }
@@ -646,7 +673,7 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
 #pragma unroll
     for (int p = 0; p < PPL; ++p)
         sq += fwd_write<T, GA>(acc[p], inside[p], pix[p], img, wsum, odx, ody, odxy, final_idx, l2);
-    if (l2.target) block_sum_to<T>(sq, l2.tile_partial + tile);
+    if (l2.on()) block_sum_to<T>(sq, l2.tile_partial + tile);
 }
 
 // Launch bounds: tiles of B <= 16 launch <= 256 threads, and their
@@ -1535,12 +1562,14 @@ __global__ void unpack_grads_kernel(int n, const T *__restrict__ packed, Grads<T
 // ------------------------------------------------------------------ host
 template <typename T>
 int pack(int n, const void *xys, const void *con, const void *col, const void *op, void *ws,
-         size_t ws_bytes, cudaStream_t s, bool half = false) {
+         size_t ws_bytes, cudaStream_t s, bool half = false, T *zero = nullptr,
+         int zero_stride = 0) {
     if (ws_bytes < sizeof(Rec<T>) * (size_t)n) return LIG_ERR_WORKSPACE;
+    if ((reinterpret_cast<uintptr_t>(ws) & 15) != 0) return LIG_ERR_INVALID;  // 16-byte records
     if (n > 0) {
         auto k = half ? pack_kernel<T, true> : pack_kernel<T, false>;
         k<<<(n + 255) / 256, 256, 0, s>>>(n, (const T *)xys, (const T *)con, (const T *)col,
-                                          (const T *)op, (Rec<T> *)ws);
+                                          (const T *)op, (Rec<T> *)ws, zero, zero_stride);
     }
     note_launches(n > 0 ? 1 : 0);
     LIG_LAUNCH_CHECK();
@@ -1601,7 +1630,7 @@ struct TileWalk {
     int *work = nullptr;           // persistent: global work counter; null: CTA per tile
 };
 
-// Loss outputs of the fused-L2 forward (l2.target != null).
+// Loss outputs of the fused-L2 forward (with a target).
 template <typename T> struct L2Out {
     T *loss = nullptr, *per_image = nullptr;
 };
@@ -1615,7 +1644,7 @@ int raster_fwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
     const int n = geo.total_points();
     const bool ga = dx != nullptr;
     // fused loss without opacities: the specialised forward (halved conic)
-    const bool fl = !ga && l2.target && !op && LIG_RASTER_FWD_FUSED;
+    const bool fl = !ga && (l2.target || l2.target_u8) && !op && LIG_RASTER_FWD_FUSED;
     int rc = pack<T>(n, xys, con, col, op, ws, ws_bytes, s, fl);
     if (rc) return rc;
     const bool ppl4 = !ga && geo.total_tiles() >= LIG_RASTER_PPL4_MIN_TILES;
@@ -1653,7 +1682,7 @@ int raster_fwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
                             (const Rec<T> *)ws, (T *)img, (T *)wsum, ga ? (T *)dx : nullptr,
                             ga ? (T *)dy : nullptr, ga ? (T *)dxy : nullptr, fin, l2);
     int launches = 1;
-    if (l2.target) {
+    if (l2.target || l2.target_u8) {
         const TileChunks ch = tile_chunks(geo);
         double *chunk_sum = l2.tile_partial + geo.total_tiles();
         if (ch.chunk_off[geo.n_img] > 0)
@@ -1693,8 +1722,8 @@ int raster_bwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
                           sizeof(T) == 4 && LIG_RASTER_BWD_F2;
     const int stride = lean ? 8 : 12;
     T *packed = reinterpret_cast<T *>((char *)ws + goff);
-    cudaMemsetAsync(packed, 0, sizeof(T) * stride * (size_t)n, s);
-    int rc = pack<T>(n, xys, con, col, op, ws, goff, s);
+    // records, and the packed gradients cleared in the same pass
+    int rc = pack<T>(n, xys, con, col, op, ws, goff, s, false, packed, stride);
     if (rc) return rc;
     const T cl = (T)(clamp > 0 ? clamp : (ga ? 0.999 : 0.99));
     const int nt = 32 * Regions::make(ga ? 2 : 0, geo.B).count;
@@ -2006,14 +2035,17 @@ extern "C" size_t lig_l2_tile_partials_bytes(int num_tiles) {
 }
 
 namespace lig {
+// target: T values, or bytes when u8
 template <typename T>
 int fwd_l2(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int32_t *bins,
            const int32_t *d_total, const void *xys, const void *con, const void *col,
            const void *op, const void *target, void *ws, size_t ws_bytes, double *partials,
-           void *diff, int32_t *fin, void *loss, void *per_image, cudaStream_t s) {
+           void *diff, int32_t *fin, void *loss, void *per_image, cudaStream_t s,
+           bool u8 = false) {
+    const L2Fwd<T> l2 = u8 ? L2Fwd<T>{nullptr, partials, (const uint8_t *)target}
+                           : L2Fwd<T>{(const T *)target, partials};
     return raster_fwd<T>(geo, walk, ids, bins, d_total, xys, con, col, op, ws, ws_bytes, diff,
-                         nullptr, nullptr, nullptr, nullptr, fin, s,
-                         L2Fwd<T>{(const T *)target, partials},
+                         nullptr, nullptr, nullptr, nullptr, fin, s, l2,
                          L2Out<T>{(T *)loss, (T *)per_image});
 }
 
@@ -2098,6 +2130,32 @@ extern "C" int lig_raster_fwd_l2_batch(int dtype, int n_img, const int32_t *heig
     if (dtype == LIG_F64)
         return fwd_l2<double>(geo, walk, ids, bins, d_total, xys, con, col, op, target, ws,
                               ws_bytes, tile_partials, diff, fin, loss, per_image, s);
+    return LIG_ERR_INVALID;
+}
+
+extern "C" int lig_raster_fwd_l2_u8_batch(int dtype, int n_img, const int32_t *heights,
+                                          const int32_t *widths, const int32_t *counts, int B,
+                                          const int32_t *ids, const int32_t *bins,
+                                          const int32_t *d_total, const int32_t *cum,
+                                          const void *xys, const void *con, const void *col,
+                                          const void *op, const uint8_t *target, int persistent,
+                                          int32_t *work, void *ws, size_t ws_bytes,
+                                          double *tile_partials, void *diff, int32_t *fin,
+                                          void *loss, void *per_image, void *stream) {
+    BatchGeo geo;
+    if (!batch_geo(n_img, heights, widths, counts, B, geo)) return LIG_ERR_INVALID;
+    const int n = geo.total_points();
+    if (!bins || !d_total || !target || !ws || !tile_partials || !diff || !fin || !loss ||
+        (persistent && !work) || (n > 0 && (!xys || !con || !col || !cum)))
+        return LIG_ERR_INVALID;
+    TileWalk walk{n > 0 ? cum : nullptr, persistent ? work : nullptr};
+    cudaStream_t s = (cudaStream_t)stream;
+    if (dtype == LIG_F32)
+        return fwd_l2<float>(geo, walk, ids, bins, d_total, xys, con, col, op, target, ws,
+                             ws_bytes, tile_partials, diff, fin, loss, per_image, s, true);
+    if (dtype == LIG_F64)
+        return fwd_l2<double>(geo, walk, ids, bins, d_total, xys, con, col, op, target, ws,
+                              ws_bytes, tile_partials, diff, fin, loss, per_image, s, true);
     return LIG_ERR_INVALID;
 }
 

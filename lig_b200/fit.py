@@ -25,7 +25,11 @@ from .gsplat2d import gradient_aware_upscale, project_gaussians_cholesky, raster
 
 
 class LevelFit:
-    """One LIG level: N Gaussians fitted to an [H, W, 3] target.
+    """One LIG level: N Gaussians fitted to an [H, W, 3] target — fp32, or
+    uint8 (an RGB image as stored, read as byte / 255 the way torchvision's
+    ToTensor converts it in train.py; the graph engine reads the bytes in the
+    loss kernel, so uploading a new target each step moves a quarter of the
+    bytes).
 
     rgb_init "uniform" draws colours U(0,1) (the fit configurations);
     "zeros" starts them at zero as gaussianlig.py:57 does.
@@ -89,6 +93,8 @@ class LevelFit:
         buffer that the next step overwrites)."""
         if self.engine == "graph":
             return self._graph_step(target_hwc.contiguous())
+        if target_hwc.dtype == torch.uint8:  # an 8-bit image, read as ToTensor does
+            target_hwc = target_hwc.float() / 255
         if self.fused_loss:
             loss = render_l2_loss(self.chol, self.means, self.rgbs, None, target_hwc, self.H,
                                   self.W, self.block)

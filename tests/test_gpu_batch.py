@@ -298,3 +298,64 @@ def test_levelfit_graph_engine_matches_autograd_engine():
     for p, q in zip((a.means, a.chol, a.rgbs), (c.means, c.chol, c.rgbs)):
         d = (p - q).abs()
         assert float((d > 1e-4).float().mean()) < 0.01 and float(d.median()) <= 1e-6
+
+
+def test_uint8_targets_equal_their_float_conversion():
+    """A batch fitted to 8-bit targets (lig_raster_fwd_l2_u8_batch) sees
+    exactly the masked difference, final indices and losses of the same batch
+    fitted to the float targets byte / 255 (torchvision's ToTensor division,
+    done on the host as train.py's image loading does); the fits then follow
+    each other (the backward's atomic sums differ only in order)."""
+    counts = [900, 1200, 0, 3000, 700]
+    g = torch.Generator().manual_seed(12)
+    u8 = [torch.randint(0, 256, (h, w, 3), generator=g, dtype=torch.uint8) for h, w in SHAPES]
+    f32 = [(t.float() / 255).cuda() for t in u8]
+    a = BatchedFit([t.cuda() for t in u8], counts, graph=False, diag=(0.5, 5.0))
+    b = BatchedFit(f32, counts, graph=False, diag=(0.5, 5.0))
+    assert a.target.dtype == torch.uint8 and b.target.dtype == torch.float32
+    a.step()
+    b.step()
+    torch.cuda.synchronize()
+    assert torch.equal(a.img, b.img) and torch.equal(a.fin, b.fin)
+    assert torch.equal(a.loss, b.loss) and torch.equal(a.per_image, b.per_image)
+    a.fit(5)
+    b.fit(5)
+    assert rel_err(np_(a.flat), np_(b.flat)) <= 1e-5
+    pa, pb = a.psnr(), b.psnr()
+    assert all(abs(x - y) <= 1e-4 for x, y in zip(pa, pb))
+
+
+def test_levelfit_uint8_upload_buffers():
+    """LevelFit.step on 8-bit target buffers (the per-step upload of the
+    end-to-end bench) equals the step on their float conversion, for the
+    graph engine (bytes read in the loss kernel) and the autograd engine
+    (converted before the drop-in call)."""
+    from lig_b200.fit import LevelFit
+    H, W, n = 96, 112, 1500
+    g = torch.Generator().manual_seed(13)
+    u8 = torch.randint(0, 256, (H, W, 3), generator=g, dtype=torch.uint8)
+    f32 = (u8.float() / 255).cuda()
+    bufs = [u8.cuda(), u8.cuda()]
+    for engine in ("graph", "autograd"):
+        a = LevelFit(n, H, W, lr=1e-2, diag=(0.5, 4.0), engine=engine)
+        b = LevelFit(n, H, W, lr=1e-2, diag=(0.5, 4.0), engine=engine)
+        la = [float(a.step(bufs[k % 2])) for k in range(4)]
+        lb = [float(b.step(f32)) for _ in range(4)]
+        assert la[0] == lb[0], engine
+        for x, y in zip(la, lb):
+            assert abs(x - y) <= 1e-5 * abs(y), engine
+
+
+def test_uint8_target_every_byte_value():
+    """Every byte value b reads as the correctly rounded b / 255 (the host's
+    division, as ToTensor): with no Gaussians the render is white, so the
+    masked difference is exactly 1 - t."""
+    g = torch.Generator().manual_seed(14)
+    vals = torch.stack([torch.randperm(256, generator=g) for _ in range(3)], 1).to(torch.uint8)
+    u8 = vals.reshape(16, 16, 3)
+    ref = 1 - u8.float() / 255
+    other = torch.randint(0, 256, (64, 64, 3), generator=g, dtype=torch.uint8)
+    a = BatchedFit([u8.cuda(), other.cuda()], [0, 200], graph=False)  # image 0: no Gaussians
+    a.step()
+    torch.cuda.synchronize()
+    assert torch.equal(a.L.image(a.img, 0).cpu(), ref)
