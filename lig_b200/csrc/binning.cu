@@ -2,14 +2,15 @@
 // of the emitted (Gaussian, tile) slots by tile.
 //
 // The intersection count lives in a device word written by
-// lig_cumsum_tiles; every kernel here reads it and bounds its work by the
-// caller's capacity, so the whole chain runs without a host round trip (the
-// reference reads it back with .item(), gsplat2d/gsplat2d/utils.py:66).
+// lig_cumsum_tiles (one single-pass look-back scan kernel); every kernel here
+// reads it and bounds its work by the caller's capacity, so the whole chain
+// runs without a host round trip (the reference reads it back with .item(),
+// gsplat2d/gsplat2d/utils.py:66).
 //
 // Ordering (default, LIG_BIN_SCATTER): per-tile counters, their exclusive
 // scan, an atomic scatter of every slot into its tile's range and a per-tile
 // sort by Gaussian index (see "scatter binning" below); workspace: two
-// counters per tile.  Alternative kept for comparison: keys are 32-bit tile
+// counters per tile, the scan state and the long-tile list.  Alternative kept for comparison: keys are 32-bit tile
 // ids (the reference's int64 (tile << 32) | depth keys carry depth 0, so only
 // ceil(log2 T) bits hold information) sorted by a stable LSD radix sort over
 // exactly those bits with <= 10-bit digits, then tile ranges from the
