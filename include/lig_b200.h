@@ -371,6 +371,15 @@ int lig_raster_fwd_l2_batch(int dtype, int n_img, const int32_t *heights, const 
                             size_t workspace_bytes, double *tile_partials, void *diff,
                             int32_t *final_idx, void *loss, void *per_image, void *stream);
 
+/* lig_raster_fwd_l2 with an 8-bit target [H,W,3] (as lig_raster_fwd_l2_u8_batch
+ * below: each byte counts as byte / 255 rounded to nearest). */
+int lig_raster_fwd_l2_u8(int dtype, int img_h, int img_w, int block_width, int num_points,
+                         const int32_t *gaussian_ids_sorted, const int32_t *tile_bins,
+                         const int32_t *num_intersects, const void *xys, const void *conics,
+                         const void *colors, const void *opacities, const uint8_t *target,
+                         void *workspace, size_t workspace_bytes, double *tile_partials,
+                         void *diff, int32_t *final_idx, void *loss, void *stream);
+
 /* lig_raster_fwd_l2_batch with an 8-bit target [sum_i H_i W_i, 3] (RGB
  * images as stored): each byte t counts as t / 255 rounded to nearest — the
  * float torchvision's ToTensor gives, which train.py's image loading uses

@@ -78,6 +78,7 @@ SIGNATURES = {
     "lig_l2_clamped_loss_batch": (I, [I, I, P, P, P, P, P, P, P, SZ, P]),
     "lig_l2_tile_partials_bytes": (SZ, [I]),
     "lig_raster_fwd_l2": (I, [I, I, I, I, I, P, P, P, P, P, P, P, P, P, SZ, P, P, P, P, P]),
+    "lig_raster_fwd_l2_u8": (I, [I, I, I, I, I, P, P, P, P, P, P, P, P, P, SZ, P, P, P, P, P]),
     "lig_raster_bwd_diff": (I, [I, I, I, I, I, P, P, P, P, P, P, P, P, P, P, D, P, SZ, P, P, P,
                                 P, P, P]),
     "lig_raster_fwd_l2_batch": (I, [I, I, P, P, P, I, P, P, P, P, P, P, P, P, P, I, P, P, SZ,

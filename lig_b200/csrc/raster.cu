@@ -2084,6 +2084,26 @@ extern "C" int lig_raster_fwd_l2(int dtype, int H, int W, int B, int n, const in
     return LIG_ERR_INVALID;
 }
 
+extern "C" int lig_raster_fwd_l2_u8(int dtype, int H, int W, int B, int n, const int32_t *ids,
+                                    const int32_t *bins, const int32_t *d_total, const void *xys,
+                                    const void *con, const void *col, const void *op,
+                                    const uint8_t *target, void *ws, size_t ws_bytes,
+                                    double *tile_partials, void *diff, int32_t *fin, void *loss,
+                                    void *stream) {
+    if (!raster_args_ok(H, W, B, n) || !bins || !d_total || !target || !ws || !tile_partials ||
+        !diff || !fin || !loss || (n > 0 && (!xys || !con || !col)))
+        return LIG_ERR_INVALID;
+    const BatchGeo geo = BatchGeo::single(H, W, B, n);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (dtype == LIG_F32)
+        return fwd_l2<float>(geo, TileWalk{}, ids, bins, d_total, xys, con, col, op, target, ws,
+                             ws_bytes, tile_partials, diff, fin, loss, nullptr, s, true);
+    if (dtype == LIG_F64)
+        return fwd_l2<double>(geo, TileWalk{}, ids, bins, d_total, xys, con, col, op, target, ws,
+                              ws_bytes, tile_partials, diff, fin, loss, nullptr, s, true);
+    return LIG_ERR_INVALID;
+}
+
 extern "C" int lig_raster_bwd_diff(int dtype, int H, int W, int B, int n, const int32_t *ids,
                                    const int32_t *bins, const int32_t *d_total, const void *xys,
                                    const void *con, const void *col, const void *op,

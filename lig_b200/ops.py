@@ -425,12 +425,15 @@ def raster_fwd_l2(img_h, img_w, block, gaussian_ids_sorted, tile_bins, total, xy
                   colors, opacities, target):
     """Fit-loop forward with the clamped-L2 loss fused in.  Returns
     (diff [H,W,3], final_idx [H,W], loss 0-d): diff = (0 <= x <= 1) ?
-    clamp(x) - target : 0 for the render x, loss = mean((clamp(x) - target)^2)."""
+    clamp(x) - target : 0 for the render x, loss = mean((clamp(x) - target)^2).
+    A uint8 target (an RGB image as stored) is read as byte / 255, the value
+    torchvision's ToTensor gives."""
     _check_cuda(xys, conics, colors, opacities, tile_bins, total, target)
     xys = _c(xys)
     dt = xys.dtype
     conics, colors, opacities = _c(conics, dt), _c(colors, dt), _c(opacities, dt)
-    target = _c(target, dt)
+    u8 = target.dtype == torch.uint8
+    target = target.contiguous() if u8 else _c(target, dt)
     n = xys.shape[0]
     dev = xys.device
     code = _dt(xys)
@@ -441,7 +444,8 @@ def raster_fwd_l2(img_h, img_w, block, gaussian_ids_sorted, tile_bins, total, xy
     diff = torch.empty((img_h, img_w, 3), dtype=dt, device=dev)
     fin = torch.empty((img_h, img_w), dtype=torch.int32, device=dev)
     loss = torch.empty((), dtype=dt, device=dev)
-    call("lig_raster_fwd_l2", code, int(img_h), int(img_w), int(block), n,
+    call("lig_raster_fwd_l2_u8" if u8 else "lig_raster_fwd_l2", code, int(img_h), int(img_w),
+         int(block), n,
          _p(gaussian_ids_sorted), _p(tile_bins), _p(total), _p(xys), _p(conics), _p(colors),
          _p(opacities), _p(target), _p(ws), wsb, _p(part), _p(diff), _p(fin), _p(loss),
          _stream(dev))

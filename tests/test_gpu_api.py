@@ -342,6 +342,26 @@ def test_fused_l2_forward_row_blocks_exact(seed, diag, offdiag):
     assert torch.equal(diff, exp) and torch.equal(fin2, fin)
 
 
+@pytest.mark.parametrize("H,W,B,n,dtype", [(150, 170, 16, 3000, torch.float32),
+                                           (1024, 1040, 16, 12000, torch.float32),
+                                           (97, 130, 12, 1500, torch.float64)])
+def test_fused_l2_forward_uint8_target(H, W, B, n, dtype):
+    """lig_raster_fwd_l2_u8: an 8-bit target gives the masked difference,
+    final indices and loss of the float target byte / 255 (ToTensor's
+    division on the host), bit for bit, in float and double."""
+    means, L, colors, _ = scene(n, H, W, diag=(0.5, 5.0), seed=8, dtype=dtype)
+    g = torch.Generator().manual_seed(18)
+    u8 = torch.randint(0, 256, (H, W, 3), generator=g, dtype=torch.uint8)
+    tf = (u8.to(dtype) / 255).cuda()
+    xys, ext, con, cnt = ops.project_fwd(L, means, None, H, W, B, True)
+    b = ops.bin_gaussians(xys, ext, cnt, H, W, B)
+    args = (H, W, B, b.gaussian_ids_sorted, b.tile_bins, b.total, xys, con, colors, None)
+    d1, f1, l1 = ops.raster_fwd_l2(*args, u8.cuda())
+    d2, f2, l2 = ops.raster_fwd_l2(*args, tf)
+    assert d1.dtype == dtype
+    assert torch.equal(d1, d2) and torch.equal(f1, f2) and torch.equal(l1, l2)
+
+
 def test_binning_grows_sort_shared_memory_between_calls():
     """A process whose first binning needs 9-bit radix digits and whose next
     one needs 10-bit digits (more shared memory in the downsweep) must opt
