@@ -2,7 +2,8 @@
 
 oracle/compile_callers.py compiles the reference's gaussianlig.py, train.py,
 minimal_trainer_upscale.py (and utils.py, optimizer.py, upscaler_torch.py
-they import) and its gsplat2d package to bytecode under oracle/_ref/py.
+they import) and its gsplat2d package to bytecode in two zip archives under
+oracle/_ref/py (imported through zipimport).
 `bound(arm)` imports those modules with `gsplat2d` / `upscaler_torch`
 resolving to
 
@@ -33,17 +34,25 @@ import torch
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PYDIR = os.path.join(ROOT, "oracle", "_ref", "py")
-CALLERS = os.path.join(PYDIR, "callers")
-REF_PKG = os.path.join(PYDIR, "pkg")
+CALLERS = os.path.join(PYDIR, "callers.zip")
+REF_PKG = os.path.join(PYDIR, "pkg.zip")
 
 _OWNED = ("gaussianlig", "utils", "optimizer", "train", "minimal_trainer_upscale",
           "upscaler_torch", "pytorch_msssim", "gsplat2d")
 
 
+def _has(archive: str, member: str) -> bool:
+    import zipfile
+    try:
+        with zipfile.ZipFile(archive) as z:
+            return member in z.namelist()
+    except (OSError, zipfile.BadZipFile):
+        return False
+
+
 def available() -> bool:
     from oracle import ref
-    return (os.path.exists(os.path.join(CALLERS, "gaussianlig.pyc"))
-            and os.path.exists(os.path.join(REF_PKG, "gsplat2d", "__init__.pyc"))
+    return (_has(CALLERS, "gaussianlig.pyc") and _has(REF_PKG, "gsplat2d/__init__.pyc")
             and ref.available())
 
 

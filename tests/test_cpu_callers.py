@@ -50,13 +50,14 @@ def test_bytecode_is_of_the_unmodified_reference_files():
         import compile_callers
     finally:
         sys.path.pop(0)
+    import zipfile
     n = 0
-    for src, rel in compile_callers.sources(REF):
-        with open(os.path.join(_callers.PYDIR, rel), "rb") as f:
-            header = f.read(16)
+    for src, archive, member in compile_callers.sources(REF):
+        with zipfile.ZipFile(os.path.join(_callers.PYDIR, archive)) as z:
+            header = z.read(member)[:16]
         flags = int.from_bytes(header[4:8], "little")
-        assert flags & 1, rel                       # hash-based pyc
+        assert flags & 1, member                    # hash-based pyc
         with open(src, "rb") as f:
-            assert header[8:16] == importlib.util.source_hash(f.read()), rel
+            assert header[8:16] == importlib.util.source_hash(f.read()), member
         n += 1
     assert n == 14
