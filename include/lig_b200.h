@@ -228,6 +228,18 @@ int lig_l2_clamped_loss(int dtype, int64_t n, const void *img, const void *targe
  * the reference (its kernels have no device-side waits). */
 int lig_wait_timeouts(void);
 
+/* Check of the alpha cut (no counterpart in the reference).  The fused-loss
+ * forward and the lean backward decide a pixel's alpha >= 1/255 test (the
+ * reference's `sigma < 0 || alpha < 1/255` rejection, csrc/forward.cu:255-258)
+ * for Gaussians with culling data by one unsigned compare of sigma's bit
+ * pattern with a cut that the pack step finds on the device.  This entry
+ * point writes into out[0..2] (device memory, three uint32, on `stream`): the
+ * cut found by that search, and the first failing and last passing bit
+ * pattern of a scan of the decision over every non-negative float up to
+ * +inf (about a millisecond).  out[0] == out[1] == out[2] + 1 shows the
+ * decision is a step at the cut. */
+int lig_alpha_cut(uint32_t *out, void *stream);
+
 /* Sum rasterizer forward that allocates nothing.  No counterpart in the
  * reference.  For callers that cannot allocate device memory when they render
  * (e.g. a plugin running inside a framework that has reserved nearly all GPU

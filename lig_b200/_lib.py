@@ -62,6 +62,7 @@ SIGNATURES = {
     "lig_upscale_bwd_nc": (I, [I, I, I, I, I, I, I, D, D, D, D, P, P, P, P, P, P]),
     "lig_probe_fp32": (I, [I, I, P, P]),
     "lig_wait_timeouts": (I, []),
+    "lig_alpha_cut": (I, [P, P]),
     "lig_raster_fwd_noalloc": (I, [I, I, I, I, P, P, P, P, P, P, P, P, P, P, P]),
     "lig_raster_bwd_l2": (I, [I, I, I, I, I, P, P, P, P, P, P, P, P, P, P, P, D, P, SZ, P, P, P,
                               P, P, P]),

@@ -31,6 +31,7 @@
 // terms in list order.
 #include <mutex>
 #include <tuple>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -46,6 +47,44 @@ template <typename T> struct alignas(16) Rec {
     T o, wx, wy, thr;  // opacity, cull half-widths (negative: never cull), sigma threshold
 };
 
+// ------------------------------------------------------------ alpha cut
+// The reference's per-pixel test rejects a term when sigma < 0 or
+// min(clamp, __expf(-sigma)) < 1/255 (csrc/forward.cu:255-258,
+// csrc/backward.cu:104-111); for clamp >= 1/255 the second half depends on
+// __expf(-sigma) alone.  Over the non-negative floats that decision is a step
+// in sigma's bit pattern: it passes below one pattern (the cut) and fails from
+// it on, and every negative sigma (sign bit set) fails.  So for a sigma that
+// is neither NaN nor -0, the whole test is one unsigned compare,
+//   pass  <=>  bits(sigma) < cut.
+// The cut is found on the device by the same expression: between 5.5
+// (__expf(-5.5) = 0.00409, 4% above 1/255 — far beyond __expf's error) and 5.6
+// (6% below) a warp narrows the bracket 32 ways per round (five rounds).
+// lig_alpha_cut scans every non-negative float to show the decision is that
+// step and that the search finds its edge (a GPU test).
+__device__ __forceinline__ bool alpha_passes(float s) {
+    return !(s < 0.f || fminf(0.999f, __expf(-s)) < 1.f / 255.f);
+}
+
+// One full warp; returns the cut (the first failing bit pattern) in every lane.
+__device__ __forceinline__ uint32_t alpha_cut_search() {
+    uint32_t lo = __float_as_uint(5.5f), hi = __float_as_uint(5.6f);  // pass(lo), fail(hi)
+    const int lane = threadIdx.x & 31;
+    while (hi - lo > 1) {
+        const uint32_t step = (hi - lo + 31) / 32;
+        const uint32_t cand = min(lo + (uint32_t)(lane + 1) * step, hi);
+        const uint32_t fails = __ballot_sync(0xffffffffu, !alpha_passes(__uint_as_float(cand)));
+        const int f = __ffs(fails) - 1;  // hi itself fails, so some lane does
+        const uint32_t new_hi = __shfl_sync(0xffffffffu, cand, f);
+        if (f > 0) lo = __shfl_sync(0xffffffffu, cand, f - 1);
+        hi = new_hi;
+    }
+    return hi;
+}
+
+// The cut on this device, written by every float pack launch (always the same
+// value) and read by the rasterizers launched after it on the same stream.
+__device__ uint32_t g_alpha_cut;
+
 // ------------------------------------------------------------------ pack
 // Culling data: the alpha >= 1/255 region of a positive-definite conic is the
 // ellipse sigma <= t/2, t = 2 ln(255 o), whose x half-extent is sqrt(t Sxx).
@@ -55,15 +94,27 @@ template <typename T> struct alignas(16) Rec {
 // alpha < exp(-0.02)/255, i.e. 2% below the reference's 1/255 cut, far beyond
 // the rounding of sigma and __expf, so skipping it changes nothing.  No culling (w < 0) for non-finite inputs, non-positive
 // opacity, non-positive-definite or nearly degenerate conics (b^2 > 0.999 ac),
-// where the reference's per-pixel tests must run everywhere in the tile.
+// where the reference's per-pixel tests must run everywhere in the tile, nor
+// where a conic entry times the squared reach of the box (plus a 16-pixel
+// region) could approach the float range.  A record with culling data
+// (w >= 0) therefore has a finite positive-definite conic and finite sigma
+// terms, so at every pixel it is evaluated on, sigma is finite and not -0
+// (every term of sigma_ref / sigma_half is >= +0 except b dx dy, and their
+// sum is +0 or a positive normal or negative float): the alpha cut's compare
+// applies.
 // HALF: the record carries a/2 and c/2 in place of a and c (the fused-loss
 // forward, see sigma_half); the cull data are computed from the full conic.
 // zero (backward): also clears the Gaussian's zero_stride accumulators there
 // (zero_stride * sizeof(T) a multiple of 16 bytes, 16-byte aligned).
+// Block 0's first warp (float) also publishes the alpha cut.
 template <typename T, bool HALF>
 __global__ void pack_kernel(int n, const T *__restrict__ xys, const T *__restrict__ conics,
                             const T *__restrict__ colors, const T *__restrict__ opac,
                             Rec<T> *__restrict__ recs, T *__restrict__ zero, int zero_stride) {
+    if (sizeof(T) == 4 && blockIdx.x == 0 && threadIdx.x < 32) {
+        const uint32_t cut = alpha_cut_search();
+        if (threadIdx.x == 0) g_alpha_cut = cut;
+    }
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (zero) {
@@ -93,7 +144,8 @@ __global__ void pack_kernel(int n, const T *__restrict__ xys, const T *__restric
         double tc = t > 0.01 ? t : 0.01;
         double sxx = c / det, syy = a / det;
         double hx = 1.001 * sqrt(tc * sxx) + 2.0, hy = 1.001 * sqrt(tc * syy) + 2.0;
-        if (hx < 1e7 && hy < 1e7) {
+        const double reach = fmax(hx, hy) + 16.0;
+        if (hx < 1e7 && hy < 1e7 && fmax(fmax(a, c), fabs(b)) * reach * reach < 1e36) {
             wx = (T)hx;
             wy = (T)hy;
             r.thr = (T)(0.5 * tc * 1.001 + 0.02);
@@ -317,6 +369,9 @@ __device__ __forceinline__ int next_tile(int *work, int &s_slot, bool first) {
 #ifndef LIG_RASTER_FWD_FUSED
 #define LIG_RASTER_FWD_FUSED 1  // specialised fused-loss forward (no opacities)
 #endif
+#ifndef LIG_RASTER_ALPHA_CUT
+#define LIG_RASTER_ALPHA_CUT 1  // fused forward / lean backward: alpha test by the cut's compare
+#endif
 // One CTA per tile, warp w = region w (8x4 pixels), one pixel per lane.
 // Batches of blockDim Gaussians (list order) are staged in shared memory, one
 // record per thread, with the next batch's record fetched into registers
@@ -520,7 +575,9 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
                                          T *__restrict__ wsum, T *__restrict__ odx,
                                          T *__restrict__ ody, T *__restrict__ odxy,
                                          int32_t *__restrict__ final_idx, Rec<T> *s_rec,
-                                         uint32_t *s_bits, const L2Fwd<T> &l2) {
+                                         uint32_t *s_bits, const L2Fwd<T> &l2, uint32_t cut) {
+    // the alpha cut's compare: the fused forward's pixel pairs (float)
+    constexpr bool kCut = FL && PPL > 1 && sizeof(T) == 4 && LIG_RASTER_ALPHA_CUT;
     const unsigned FULL = 0xffffffffu;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int B = tc.B, tx0 = tc.tx0, ty0 = tc.ty0;
@@ -545,8 +602,10 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
 
     FwdAcc<T, GA> acc[PPL];
     // walk the Gaussians of `mask` (bits of the 32 records at rb, list
-    // indices ib + bit) in list order
-    auto walk = [&](uint32_t mask, const Rec<T> *rb, int ib) {
+    // indices ib + bit) in list order; fast_tag true: every record has
+    // culling data, so the fused forward tests alpha by the cut's compare
+    auto walk = [&](uint32_t mask, const Rec<T> *rb, int ib, auto fast_tag) {
+        [[maybe_unused]] constexpr bool FAST = decltype(fast_tag)::value;
         if constexpr (FL && PPL == 1) {
             while (mask) {
                 const int b1 = __ffs(mask) - 1;
@@ -583,7 +642,8 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
                     const T dy = g1.y - py[p];
                     const T sg = fma_rn(bdx, dy, fma_rn(hadx, dx, mul_rn(mul_rn(g1.c, dy), dy)));
                     ap[p] = M::min_((T)0.999, M::exp_(-sg));
-                    okp[p] = !(sg < (T)0 || ap[p] < (T)1 / (T)255);
+                    if constexpr (FAST) okp[p] = __float_as_uint((float)sg) < cut;
+                    else okp[p] = !(sg < (T)0 || ap[p] < (T)1 / (T)255);
                 }
 #pragma unroll
                 for (int p = 0; p < PPL; ++p)
@@ -639,11 +699,17 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
             for (int base = range.x; base < range.y; base += 32) {
                 const bool hit =
                     base + lane < range.y && region_hit<T, ELL, FL>(pre, R, w, tx0, ty0);
+                // a chunk whose records all carry culling data takes the cut
+                bool fast = false;
+                if constexpr (kCut)
+                    fast = !__any_sync(FULL, base + lane < range.y && !(pre.wx >= (T)0));
                 __syncwarp();
                 w_rec[lane] = pre;
                 __syncwarp();
                 if (base + 32 + lane < range.y) pre = recs[__ldg(ids + base + 32 + lane)];
-                walk(__ballot_sync(FULL, hit), w_rec, base);
+                const uint32_t mask = __ballot_sync(FULL, hit);
+                if (fast) walk(mask, w_rec, base, std::true_type{});
+                else walk(mask, w_rec, base, std::false_type{});
             }
         } else {
             const int nt = blockDim.x;
@@ -661,7 +727,7 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
                 for (int m = 0; m * 32 < cnt; ++m) {
                     const int t = m * 32 + lane;
                     walk(__ballot_sync(FULL, t < cnt && ((s_bits[t] >> w) & 1u)), s_rec + m * 32,
-                         base + m * 32);
+                         base + m * 32, std::false_type{});
                 }
             }
         }
@@ -682,9 +748,6 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
 // instantiation.
 #ifndef LIG_RASTER_FWD_MINB
 #define LIG_RASTER_FWD_MINB 4
-#endif
-#ifndef LIG_RASTER_BWD_PAIR
-#define LIG_RASTER_BWD_PAIR 1  // lean backward: two pixels per loop iteration (measured faster)
 #endif
 #ifndef LIG_RASTER_BWD_LEAN_MINB
 #define LIG_RASTER_BWD_LEAN_MINB 4  // the paired loop wants the larger register budget
@@ -735,11 +798,12 @@ raster_fwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work
     Rec<T> *s_rec = reinterpret_cast<Rec<T> *>(smem_raw);
     uint32_t *s_bits = reinterpret_cast<uint32_t *>(s_rec + blockDim.x);
     const int n_tiles = geo.total_tiles();
+    const uint32_t cut = FL && sizeof(T) == 4 ? g_alpha_cut : 0u;
     for (int tile = next_tile(work, s_slot, true); tile < n_tiles;
          tile = next_tile(work, s_slot, false)) {
         const TileCtx tc = tile_ctx(geo, cum, d_total, tile);
         fwd_tile<T, GA, PPL, FL>(tc, tile, ids, tile_bins, recs, img, wsum, odx, ody, odxy,
-                                 final_idx, s_rec, s_bits, l2);
+                                 final_idx, s_rec, s_bits, l2, cut);
     }
 }
 
@@ -966,8 +1030,11 @@ struct alignas(16) PixPair {
 // ABS: also the per-pixel absolute values of the mean gradient summed over
 // the pixels (the reference's v_xy_abs, csrc/backward.cu:146-150), in acc[2],
 // acc[3]: per pixel v_sigma (a dx + b dy) and v_sigma (b dx + c dy).
-template <int NCP, int CSTEP, int NR, bool ABS = false>
-__device__ __forceinline__ void lean_region_f2(const Rec<float> &g, float clamp,
+// FAST: the Gaussian carries culling data and clamp >= 1/255 (or cut = 0 for
+// a clamp below it: nothing passes), so the test is the alpha cut's compare
+// and alpha = min(pass ? clamp : 0, exp(-sigma)) — the same value.
+template <int NCP, int CSTEP, int NR, bool ABS = false, bool FAST = false>
+__device__ __forceinline__ void lean_region_f2(const Rec<float> &g, float clamp, uint32_t cut,
                                                const PixPair *__restrict__ pp, int c0, int r0,
                                                float px0, float py0, float (&acc)[11]) {
     const float ha = 0.5f * g.a, hc = 0.5f * g.c;
@@ -1005,9 +1072,15 @@ __device__ __forceinline__ void lean_region_f2(const Rec<float> &g, float clamp,
             const f2 S = f2_fma(BDX, DY[r], f2_fma(HADX, DX, CDD[r]));
             float s0, s1;
             f2_unpack(S, s0, s1);
-            const float al0 = fminf(clamp, __expf(-s0)), al1 = fminf(clamp, __expf(-s1));
-            const float a0 = (s0 < 0.f || al0 < 1.f / 255.f) ? 0.f : al0;
-            const float a1 = (s1 < 0.f || al1 < 1.f / 255.f) ? 0.f : al1;
+            float a0, a1;
+            if constexpr (FAST) {
+                a0 = fminf(__float_as_uint(s0) < cut ? clamp : 0.f, __expf(-s0));
+                a1 = fminf(__float_as_uint(s1) < cut ? clamp : 0.f, __expf(-s1));
+            } else {
+                const float al0 = fminf(clamp, __expf(-s0)), al1 = fminf(clamp, __expf(-s1));
+                a0 = (s0 < 0.f || al0 < 1.f / 255.f) ? 0.f : al0;
+                a1 = (s1 < 0.f || al1 < 1.f / 255.f) ? 0.f : al1;
+            }
             const f2 A = f2_pack(a0, a1);
             sr = f2_fma(A, V0, sr);
             sg = f2_fma(A, V1, sg);
@@ -1105,7 +1178,7 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
                                          const Rec<T> *__restrict__ recs,
                                          const int32_t *__restrict__ final_idx, CotSrc<T> cot,
                                          const T *__restrict__ v_dx, const T *__restrict__ v_dy,
-                                         const T *__restrict__ v_dxy, T clamp,
+                                         const T *__restrict__ v_dxy, T clamp, uint32_t cut,
                                          T *__restrict__ packed, int &s_end, uint32_t bar,
                                          uint32_t &phase) {
     using M = Math<T>;
@@ -1115,6 +1188,8 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
     // records staged by bulk async copies (no register prefetch, no region
     // masks: the warps test the box and ellipse themselves)
     constexpr bool kBulk = kPairs && LIG_RASTER_BWD_BULK;
+    // the alpha cut's compare in the pair walk (float)
+    constexpr bool kCut = kPairs && LIG_RASTER_ALPHA_CUT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nt = blockDim.x;  // = 32 * regions: region-major pixel slots
     PixRec<T, GA> *s_pix = reinterpret_cast<PixRec<T, GA> *>(smem_raw);
@@ -1236,11 +1311,13 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
         }
         // compact the batch slots touching this region (ascending)
         int nmine = 0;
+        bool exact = false;  // a listed Gaussian without culling data
         for (int m = 0; m * 32 < cnt; ++m) {
             const int t = m * 32 + lane;
             bool hit;
             if constexpr (kBulk) hit = t < cnt && region_hit<T, false, false>(s_rec[t], R, w, tx0, ty0);
             else hit = t < cnt && ((s_bits[t] >> w) & 1u);
+            if constexpr (kCut) exact = exact || (hit && !(s_rec[t].wx >= (T)0));
             if (LIG_RASTER_BWD_LANE_ELLIPSE && hit) {
                 // exact ellipse test of Gaussian t against this warp's region,
                 // one Gaussian per lane (the staging only tested the box)
@@ -1256,6 +1333,11 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
             nmine += __popc(mask);
         }
         __syncwarp();
+        // the alpha cut's compare when every Gaussian this warp lists has
+        // culling data (warp-uniform)
+        const bool fast = kCut && !__any_sync(FULL, exact);
+        auto run_list = [&](auto fast_tag) {
+        constexpr bool FAST = decltype(fast_tag)::value;
         for (int g0 = 0, lsplit = 0; g0 < nmine; g0 += 32 >> lsplit) {
             // lanes per Gaussian: with at most 4 / 8 / LIG_RASTER_BWD_SPLIT1
             // Gaussians left, 8 / 4 / 2 lanes share one Gaussian (a round
@@ -1284,20 +1366,38 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
                 const float px0 = (float)(tx0 + (w % R.nbx) * 8) + 0.5f;
                 const float py0 = (float)(ty0 + (w / R.nbx) * 4) + 0.5f;
                 const PixPair *pp = reinterpret_cast<const PixPair *>(smem_raw) + w * 16;
-                if (act) {
+                if (act && FAST) {
                     switch (lsplit) {
                     case 0:
-                        lean_region_f2<4, 1, 4, ABS>(g, clamp, pp, 0, 0, px0, py0, acc);
+                        lean_region_f2<4, 1, 4, ABS, true>(g, clamp, cut, pp, 0, 0, px0, py0, acc);
                         break;
                     case 1:
-                        lean_region_f2<2, 2, 4, ABS>(g, clamp, pp, part, 0, px0, py0, acc);
+                        lean_region_f2<2, 2, 4, ABS, true>(g, clamp, cut, pp, part, 0, px0, py0,
+                                                           acc);
                         break;
                     case 2:
-                        lean_region_f2<1, 1, 4, ABS>(g, clamp, pp, part, 0, px0, py0, acc);
+                        lean_region_f2<1, 1, 4, ABS, true>(g, clamp, cut, pp, part, 0, px0, py0,
+                                                           acc);
                         break;
                     default:
-                        lean_region_f2<1, 1, 2, ABS>(g, clamp, pp, part & 3, 2 * (part >> 2),
-                                                     px0, py0, acc);
+                        lean_region_f2<1, 1, 2, ABS, true>(g, clamp, cut, pp, part & 3,
+                                                           2 * (part >> 2), px0, py0, acc);
+                        break;
+                    }
+                } else if (act) {
+                    switch (lsplit) {
+                    case 0:
+                        lean_region_f2<4, 1, 4, ABS>(g, clamp, cut, pp, 0, 0, px0, py0, acc);
+                        break;
+                    case 1:
+                        lean_region_f2<2, 2, 4, ABS>(g, clamp, cut, pp, part, 0, px0, py0, acc);
+                        break;
+                    case 2:
+                        lean_region_f2<1, 1, 4, ABS>(g, clamp, cut, pp, part, 0, px0, py0, acc);
+                        break;
+                    default:
+                        lean_region_f2<1, 1, 2, ABS>(g, clamp, cut, pp, part & 3,
+                                                     2 * (part >> 2), px0, py0, acc);
                         break;
                     }
                 }
@@ -1315,41 +1415,7 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
                     default: lean_region<T, 3>(g, clamp, my_pix, part, px0, py0, acc); break;
                     }
                 }
-            } else if constexpr (LEAN && !GA && LIG_RASTER_BWD_PAIR) {
-                // two of the lane's pixels per iteration: their sigma / alpha
-                // chains overlap; accumulation stays in pixel order
-                auto body = [&](const PixRec<T, GA> &c, T alpha, T dx, T dy) {
-                    touched = true;
-                    acc[7] += alpha * c.vo0;
-                    acc[8] += alpha * c.vo1;
-                    acc[9] += alpha * c.vo2;
-                    T v_alpha = 0;
-                    v_alpha += g.r * c.vo0;
-                    v_alpha += g.g * c.vo1;
-                    v_alpha += g.bl * c.vo2;
-                    const T v_sigma = -alpha * v_alpha;
-                    const T tx = v_sigma * dx, ty = v_sigma * dy;
-                    acc[0] += tx;
-                    acc[1] += ty;
-                    acc[4] += tx * dx;
-                    acc[5] += tx * dy;
-                    acc[6] += ty * dy;
-                };
-                for (int j = part; j < 32; j += 2 * jstep) {
-                    const PixRec<T, GA> &c0 = my_pix[j];
-                    const PixRec<T, GA> &c1 = my_pix[j + jstep];
-                    const T dx0 = g.x - c0.px, dy0 = g.y - c0.py;
-                    const T dx1 = g.x - c1.px, dy1 = g.y - c1.py;
-                    const T s0 = sigma_ref<T>(g.a, g.b, g.c, dx0, dy0);
-                    const T s1 = sigma_ref<T>(g.a, g.b, g.c, dx1, dy1);
-                    const T a0 = M::min_(clamp, g.o * M::exp_(-s0));
-                    const T a1 = M::min_(clamp, g.o * M::exp_(-s1));
-                    const bool ok0 = k <= c0.fin && !(s0 < (T)0 || a0 < (T)1 / (T)255);
-                    const bool ok1 = k <= c1.fin && !(s1 < (T)0 || a1 < (T)1 / (T)255);
-                    if (ok0) body(c0, a0, dx0, dy0);
-                    if (ok1) body(c1, a1, dx1, dy1);
-                }
-            } else
+            } else {
             for (int j = part; j < 32; j += jstep) {
                 const PixRec<T, GA> &c = my_pix[j];
                 if (k > c.fin) continue;
@@ -1438,6 +1504,7 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
                     acc[10] += vis * va;
                 }
             }
+            }
             for (int o = 1; o < (1 << lsplit); o <<= 1) {  // combine the lane group
 #pragma unroll
                 for (int q = 0; q < 11; ++q) {
@@ -1492,6 +1559,9 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
                 }
             }
         }
+        };
+        if (fast) run_list(std::true_type{});
+        else run_list(std::false_type{});
     }
 }
 
@@ -1515,11 +1585,15 @@ raster_bwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work
         __syncthreads();
     }
     const int n_tiles = geo.total_tiles();
+    // the alpha cut (pack_kernel wrote it before this launch); a clamp below
+    // 1/255 rejects every term, which cut = 0 says
+    uint32_t cut = 0;
+    if (LEAN && !GA && sizeof(T) == 4 && (float)clamp >= 1.f / 255.f) cut = g_alpha_cut;
     for (int tile = next_tile(work, s_slot, true); tile < n_tiles;
          tile = next_tile(work, s_slot, false)) {
         const TileCtx tc = tile_ctx(geo, cum, d_total, tile);
         bwd_tile<T, GA, LEAN, ABS>(tc, tile, ids, tile_bins, recs, final_idx, cot, v_dx, v_dy,
-                                   v_dxy, clamp, packed, s_end, bar, phase);
+                                   v_dxy, clamp, cut, packed, s_end, bar, phase);
     }
 }
 
@@ -1875,6 +1949,51 @@ extern "C" int lig_wait_timeouts(void) {
     unsigned int v = 0;
     if (cudaMemcpyFromSymbol(&v, g_wait_timeouts, sizeof(v)) != cudaSuccess) return -1;
     return (int)v;
+}
+
+// ------------------------------------------------------ alpha cut check
+namespace lig {
+// out[0] = the warp search's cut; out[1] = first failing, out[2] = last
+// passing bit pattern of the scan below (initial values for its atomics).
+__global__ void alpha_cut_init_kernel(uint32_t *out) {
+    const uint32_t cut = alpha_cut_search();
+    if (threadIdx.x == 0) {
+        out[0] = cut;
+        out[1] = 0xffffffffu;
+        out[2] = 0u;
+    }
+}
+
+// The rasterizers' alpha decision at every non-negative float up to +inf
+// (bit patterns 0 .. 0x7f800000): the decision is a step with its edge at the
+// cut exactly when out[2] + 1 == out[1] == out[0].
+__global__ void alpha_cut_scan_kernel(uint32_t *out) {
+    constexpr uint32_t kLast = 0x7f800000u;
+    uint32_t first_fail = 0xffffffffu, last_pass = 0u;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u <= kLast; u += stride) {
+        if (alpha_passes(__uint_as_float(u))) last_pass = max(last_pass, u);
+        else first_fail = min(first_fail, u);
+    }
+    first_fail = __reduce_min_sync(0xffffffffu, first_fail);
+    last_pass = __reduce_max_sync(0xffffffffu, last_pass);
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(out + 1, first_fail);
+        atomicMax(out + 2, last_pass);
+    }
+}
+}  // namespace lig
+
+// Writes the alpha cut and the full scan's step edges into out[0..2] (device
+// memory, three uint32) on `stream`.
+extern "C" int lig_alpha_cut(uint32_t *out, void *stream) {
+    if (!out) return LIG_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    alpha_cut_init_kernel<<<1, 32, 0, s>>>(out);
+    alpha_cut_scan_kernel<<<148 * 8, 256, 0, s>>>(out);
+    note_launches(2);
+    LIG_LAUNCH_CHECK();
+    return LIG_OK;
 }
 
 // ----------------------------------------------------- allocation-free entry

@@ -385,3 +385,66 @@ print("ok")
     r = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True,
                        timeout=300)
     assert r.returncode == 0 and "ok" in r.stdout, r.stderr[-2000:]
+
+
+def test_alpha_cut_is_the_step_of_the_alpha_test():
+    """Over every non-negative float sigma (bit patterns up to +inf) the
+    rasterizers' alpha >= 1/255 decision is one step in sigma's bit pattern,
+    and the warp search the pack kernel runs finds its edge:
+    out = [search cut, first failing pattern, last passing pattern]."""
+    from lig_b200 import _lib
+    out = torch.zeros(3, dtype=torch.int32, device="cuda")
+    assert _lib.lib.lig_alpha_cut(ops._p(out), ops._stream(out.device)) == _lib.LIG_OK
+    o = out.cpu().numpy().view(np.uint32)
+    assert o[0] == o[1] and o[2] + 1 == o[1], o
+    cut = float(o[:1].view(np.float32)[0])
+    assert 5.5 < cut < 5.6 and abs(cut - np.log(255.0)) < 1e-5
+
+
+@pytest.mark.parametrize("H,W,B,n", [(150, 170, 16, 3000),
+                                     (1040, 1100, 16, 20000)])  # four pixels per lane
+def test_alpha_cut_paths_with_degenerate_gaussians(H, W, B, n):
+    """Chunks that hold a Gaussian without culling data take the float alpha
+    test, the rest the cut's compare.  Mixed in: non-positive-definite
+    conics; negative-definite ones centred exactly on a pixel centre (sigma
+    is -0 there: the reference passes it with alpha = clamp); conics whose
+    entries times the squared cull reach come near the float range (no
+    culling data by that guard); NaN conics (sigma is NaN: the reference
+    passes it with alpha = clamp).  The
+    fused forward's masked difference and final indices equal the plain
+    forward's bit for bit, and the lean backward's colour gradients (an
+    all-positive cotangent, so one flipped alpha decision would move a
+    Gaussian's sum by at least 0.5 / 255) equal the general backward's per
+    Gaussian."""
+    means, L, colors, _ = scene(n, H, W, diag=(0.5, 5.0), seed=31)
+    xys, ext, con, cnt = ops.project_fwd(L, means, None, H, W, B, True)
+    xys, con = xys.clone(), con.clone()
+    idx = torch.arange(7, n, 53, device="cuda")
+    kind = torch.arange(idx.numel(), device="cuda") % 4
+    bad = {0: [1.0, 2.0, 1.0], 1: [-0.3, -0.1, -0.5], 2: [1e35, -0.99e35, 1e35],
+           3: [float("nan"), 0.0, 1.0]}
+    for k, v in bad.items():
+        sel = idx[kind == k]
+        con[sel] = torch.tensor(v, device="cuda")
+        if k == 1:
+            xys[sel] = torch.floor(xys[sel]) + 0.5
+    g = torch.Generator().manual_seed(32)
+    target = torch.rand(H, W, 3, generator=g).cuda()
+    b = ops.bin_gaussians(xys, ext, cnt, H, W, B)
+    img, _, _, _, _, fin = ops.raster_fwd(H, W, B, b.gaussian_ids_sorted, b.tile_bins, b.total,
+                                          xys, con, colors, None, False)
+    diff, fin2, _ = ops.raster_fwd_l2(H, W, B, b.gaussian_ids_sorted, b.tile_bins, b.total,
+                                      xys, con, colors, None, target)
+    assert torch.isfinite(img).all()
+    exp = torch.where((img >= 0) & (img <= 1), torch.clamp(img, 0, 1) - target,
+                      torch.zeros_like(img))
+    assert torch.equal(diff, exp) and torch.equal(fin2, fin)
+    v = 0.5 + 0.5 * torch.rand(H, W, 3, generator=g).cuda()
+    lean = ops.raster_bwd(H, W, B, b.gaussian_ids_sorted, b.tile_bins, b.total, xys, con,
+                          colors, None, fin, v, None)
+    full = ops.raster_bwd(H, W, B, b.gaussian_ids_sorted, b.tile_bins, b.total, xys, con,
+                          colors, None, fin, v, torch.zeros(H, W, device="cuda"))
+    a, r = np_(lean[3]).astype(np.float64), np_(full[3]).astype(np.float64)
+    assert np.isfinite(r).all()
+    assert (np.abs(a - r) <= 1e-6 * np.abs(r) + 1e-5).all()
+    assert (r[np_(idx)].sum(1) > 0).any()   # the planted Gaussians were rendered

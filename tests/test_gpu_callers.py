@@ -7,7 +7,9 @@ tests/_callers.py) twice in this process: once with `gsplat2d` /
 lig_b200.install_gsplat2d(), once with them resolving to the reference's own
 gsplat2d package on the reference's kernels.  Same seeds, same target; the
 comparison is on what LIG's code computes: renders (1e-5), gradients
-(1e-4 relative), parameter updates (1e-4 relative) and PSNR (0.05 dB).
+(1e-4 relative) and the optimizer's moments (5e-4 relative), with the two
+arms in lockstep (each iteration starts both from the reference arm's
+parameters and optimizer state), and the PSNR of free-running fits (0.05 dB).
 
   * Gaussian2D.train_iter (gaussianlig.py:70-111): cov2d parameterisation,
     rgbs initialised to zeros, torch Adam at train.py's default lr 0.018.
@@ -52,52 +54,100 @@ def _psnr(a, b):
     return 10 * math.log10(1.0 / F.mse_loss(a.float(), b.float()).item())
 
 
+# ------------------------------------------------------------------- lockstep
+# A fit's trajectory is chaotic under Adam / Adan: their first steps move each
+# parameter by about lr * sign(gradient), so a gradient at rounding-noise
+# level (the backward's float atomics add in a run-dependent order, in the
+# reference as here) can take either sign and the two runs part ways.  The
+# per-iteration comparisons therefore run the two arms in lockstep: before
+# each iteration this library's model takes the reference model's parameters
+# and optimizer state (by value), then both run the same unmodified step.
+# End-of-fit agreement of free-running fits is the PSNR test on train.py.
+
+def _sync(dst_params, dst_opt, src_params, src_opt):
+    """dst takes src's parameters and optimizer state, by value."""
+    with torch.no_grad():
+        for a, b in zip(dst_params, src_params):
+            a.copy_(b)
+            st = src_opt.state.get(b, {})
+            dst_opt.state[a] = {k: (v.clone() if torch.is_tensor(v) else v)
+                                for k, v in st.items()}
+
+
+def _opt_state(opt, params):
+    return [{k: v.detach().clone() for k, v in opt.state[p].items()
+             if torch.is_tensor(v) and v.numel() > 1} for p in params]
+
+
+def _assert_opt_state_close(sa, sb, tol):
+    for da, db in zip(sa, sb):
+        assert set(da) == set(db)
+        for k in da:
+            assert rel_err(da[k].cpu(), db[k].cpu()) < tol, k
+
+
 # ----------------------------------------------------------------- gaussianlig.py
 
-def _gaussianlig_run(arm, gt, n, iters):
-    H, W = gt.shape[2], gt.shape[3]
+def _gaussianlig_model(arm, H, W, n):
     with _callers.bound(arm):
         import gaussianlig
         torch.manual_seed(0)
         m = gaussianlig.Gaussian2D(loss_type="L2", opt_type="adam", num_points=n, H=H, W=W,
                                    BLOCK_H=16, BLOCK_W=16, device=DEV, lr=0.018)
-        params = (m.means, m.cov2d, m.rgbs)
-        init = [p.detach().clone() for p in params]
-        grads, losses, psnrs = [], [], []
-        step = m.optimizer.step
+        return m, _callers.module_origin("gsplat2d")
 
-        def recording_step(*a, **k):
-            grads.append([p.grad.detach().clone() for p in params])
-            return step(*a, **k)
 
-        m.optimizer.step = recording_step
-        for _ in range(iters):
+def _gaussianlig_step(arm, m, gt):
+    """One Gaussian2D.train_iter (gaussianlig.py:99-111), recording the
+    gradients the optimizer sees and its state after the step."""
+    params = (m.means, m.cov2d, m.rgbs)
+    rec = {}
+    step = m.optimizer.step
+
+    def recording_step(*a, **k):
+        rec["grads"] = [p.grad.detach().clone() for p in params]
+        out = step(*a, **k)
+        rec["state"] = _opt_state(m.optimizer, params)
+        return out
+
+    m.optimizer.step = recording_step
+    try:
+        with _callers.bound(arm):
             loss, psnr = m.train_iter(gt)
-            losses.append(float(loss))
-            psnrs.append(psnr)
-        with torch.no_grad():
-            render = m.forward()["render"].detach().clone()
-        return dict(init=init, grads=grads, losses=losses, psnrs=psnrs, render=render,
-                    delta=[p.detach() - i for p, i in zip(params, init)],
-                    origin=_callers.module_origin("gsplat2d"))
+    finally:
+        m.optimizer.step = step
+    rec["loss"], rec["psnr"] = float(loss), psnr
+    return rec
 
 
 def test_gaussianlig_train_iter_matches_reference():
-    gt = _target(96, 128)
-    mine = _gaussianlig_run("lig", gt, 3000, 10)
-    ref = _gaussianlig_run("ref", gt, 3000, 10)
-    assert "lig_b200" in mine["origin"] and "_ref" in ref["origin"]
-    for a, b in zip(mine["init"], ref["init"]):
+    H, W, n = 96, 128, 3000
+    gt = _target(H, W)
+    mine, o_mine = _gaussianlig_model("lig", H, W, n)
+    ref, o_ref = _gaussianlig_model("ref", H, W, n)
+    assert "lig_b200" in o_mine and "_ref" in o_ref
+    pm, pr = (mine.means, mine.cov2d, mine.rgbs), (ref.means, ref.cov2d, ref.rgbs)
+    for a, b in zip(pm, pr):
         assert torch.equal(a, b)
-    for it, (ga, gb) in enumerate(zip(mine["grads"], ref["grads"])):
-        for name, a, b in zip(("means", "cov2d", "rgbs"), ga, gb):
-            assert rel_err(a.cpu(), b.cpu()) < 1e-4, (it, name)
-    np.testing.assert_allclose(mine["losses"], ref["losses"], rtol=1e-5)
-    np.testing.assert_allclose(mine["psnrs"], ref["psnrs"], atol=1e-4)
-    assert (mine["render"] - ref["render"]).abs().max().item() < 1e-5
-    for name, a, b in zip(("means", "cov2d", "rgbs"), mine["delta"], ref["delta"]):
-        assert rel_err(a.cpu(), b.cpu()) < 1e-4, name
-    assert mine["psnrs"][-1] > mine["psnrs"][0] + 1.0   # the fit learns
+    psnrs = []
+    for it in range(10):
+        _sync(pm, mine.optimizer, pr, ref.optimizer)
+        a = _gaussianlig_step("lig", mine, gt)
+        b = _gaussianlig_step("ref", ref, gt)
+        for name, ga, gb in zip(("means", "cov2d", "rgbs"), a["grads"], b["grads"]):
+            assert rel_err(ga.cpu(), gb.cpu()) < 1e-4, (it, name)
+        assert abs(a["loss"] - b["loss"]) <= 1e-5 * abs(b["loss"]), it
+        assert abs(a["psnr"] - b["psnr"]) <= 1e-4, it
+        _assert_opt_state_close(a["state"], b["state"], 5e-4)   # Adam's moments
+        psnrs.append(b["psnr"])
+    _sync(pm, mine.optimizer, pr, ref.optimizer)
+    with torch.no_grad():
+        with _callers.bound("lig"):
+            r_mine = mine.forward()["render"].detach().clone()
+        with _callers.bound("ref"):
+            r_ref = ref.forward()["render"].detach().clone()
+    assert (r_mine - r_ref).abs().max().item() < 1e-5
+    assert psnrs[-1] > psnrs[0] + 1.0   # the fit learns
 
 
 # ----------------------------------------------------------------------- train.py
@@ -145,8 +195,7 @@ def test_train_py_two_level_psnr_matches_reference(tmp_path):
 
 # ------------------------------------------------------- minimal_trainer_upscale.py
 
-def _minimal_run(arm, gt, h, w, n, iters, use_torch_upscale):
-    H, W = gt.shape[2], gt.shape[3]
+def _minimal_setup(arm, gt, h, w, n):
     with _callers.bound(arm):
         import minimal_trainer_upscale as mtu
         from optimizer import Adan
@@ -161,39 +210,55 @@ def _minimal_run(arm, gt, h, w, n, iters, use_torch_upscale):
                     {"params": model._cholesky, "lr": lr * pos_scale},
                     {"params": model._opacity_logits, "lr": lr}],
                    betas=(0.98, 0.92, 0.99), fused=False)
-        gt_hwc = gt.squeeze(0).permute(1, 2, 0)
         params = (model.means, model._cholesky, model._rgb_logits, model._opacity_logits)
-        first, losses = None, []
-        for it in range(iters):
-            out = model()
-            img = mtu.upscale_fn(out, H, W, use_torch_upscale)
-            loss = F.mse_loss(img, gt_hwc)
-            opt.zero_grad(set_to_none=True)
-            loss.backward()
-            if first is None:
-                first = dict(img=img.detach().clone(), dx=out["dx"].detach().clone(),
-                             wsum=out["wsum"].detach().clone(),
-                             grads=[p.grad.detach().clone() for p in params])
-            opt.step()
-            losses.append(loss.item())
-        with torch.no_grad():
-            model.scale_to(2 * h, 2 * w)   # render the fitted set at twice the model size
-            big = model()["render_hwc"].detach().clone()
-        return dict(first=first, losses=losses, big=big,
+        return dict(mtu=mtu, model=model, opt=opt, params=params,
                     origin=_callers.module_origin("gsplat2d"))
+
+
+def _minimal_step(arm, run, gt, use_torch_upscale):
+    """Gaussian2DMinimal.forward + upscale_fn (minimal_trainer_upscale.py:
+    124-170), the L2 loss, backward and one Adan step."""
+    H, W = gt.shape[2], gt.shape[3]
+    gt_hwc = gt.squeeze(0).permute(1, 2, 0)
+    model, opt, params = run["model"], run["opt"], run["params"]
+    with _callers.bound(arm):
+        out = model()
+        img = run["mtu"].upscale_fn(out, H, W, use_torch_upscale)
+        loss = F.mse_loss(img, gt_hwc)
+        opt.zero_grad(set_to_none=True)
+        loss.backward()
+        rec = dict(img=img.detach().clone(), dx=out["dx"].detach().clone(),
+                   wsum=out["wsum"].detach().clone(),
+                   grads=[p.grad.detach().clone() for p in params], loss=loss.item())
+        opt.step()
+    rec["state"] = _opt_state(opt, params)
+    return rec
 
 
 @pytest.mark.parametrize("use_torch_upscale", [False, True])
 def test_minimal_trainer_upscale_matches_reference(use_torch_upscale):
     gt = _target(160, 192, seed=7)
-    mine = _minimal_run("lig", gt, 80, 96, 2000, 8, use_torch_upscale)
-    ref = _minimal_run("ref", gt, 80, 96, 2000, 8, use_torch_upscale)
+    h, w, n = 80, 96, 2000
+    mine = _minimal_setup("lig", gt, h, w, n)
+    ref = _minimal_setup("ref", gt, h, w, n)
     assert "lig_b200" in mine["origin"] and "_ref" in ref["origin"]
-    a, b = mine["first"], ref["first"]
-    for k in ("img", "dx", "wsum"):
-        assert (a[k] - b[k]).abs().max().item() < 1e-5, k
-    for name, ga, gb in zip(("means", "cholesky", "rgb", "opacity"), a["grads"], b["grads"]):
-        assert rel_err(ga.cpu(), gb.cpu()) < 1e-4, name
-    np.testing.assert_allclose(mine["losses"], ref["losses"], rtol=1e-4)
-    assert (mine["big"] - ref["big"]).abs().max().item() < 1e-4
-    assert mine["losses"][-1] < mine["losses"][0]
+    losses = []
+    for it in range(8):
+        _sync(mine["params"], mine["opt"], ref["params"], ref["opt"])
+        a = _minimal_step("lig", mine, gt, use_torch_upscale)
+        b = _minimal_step("ref", ref, gt, use_torch_upscale)
+        for k in ("img", "dx", "wsum"):
+            assert (a[k] - b[k]).abs().max().item() < 1e-5, (it, k)
+        for name, ga, gb in zip(("means", "cholesky", "rgb", "opacity"), a["grads"], b["grads"]):
+            assert rel_err(ga.cpu(), gb.cpu()) < 1e-4, (it, name)
+        assert abs(a["loss"] - b["loss"]) <= 1e-5 * abs(b["loss"]), it
+        _assert_opt_state_close(a["state"], b["state"], 5e-4)   # Adan's moments
+        losses.append(b["loss"])
+    _sync(mine["params"], mine["opt"], ref["params"], ref["opt"])
+    big = []
+    for arm, run in (("lig", mine), ("ref", ref)):
+        with torch.no_grad(), _callers.bound(arm):
+            run["model"].scale_to(2 * h, 2 * w)   # the fitted set at twice the model size
+            big.append(run["model"]()["render_hwc"].detach().clone())
+    assert (big[0] - big[1]).abs().max().item() < 1e-5
+    assert losses[-1] < losses[0]
