@@ -229,10 +229,10 @@ int lig_l2_clamped_loss(int dtype, int64_t n, const void *img, const void *targe
 int lig_wait_timeouts(void);
 
 /* Check of the alpha cut (no counterpart in the reference).  The fused-loss
- * forward and the lean backward decide a pixel's alpha >= 1/255 test (the
- * reference's `sigma < 0 || alpha < 1/255` rejection, csrc/forward.cu:255-258)
- * for Gaussians with culling data by one unsigned compare of sigma's bit
- * pattern with a cut that the pack step finds on the device.  This entry
+ * forward decides a pixel's alpha >= 1/255 test (the reference's
+ * `sigma < 0 || alpha < 1/255` rejection, csrc/forward.cu:255-258) for
+ * Gaussians with culling data by one unsigned compare of sigma's bit pattern
+ * with a cut that the pack step finds on the device.  This entry
  * point writes into out[0..2] (device memory, three uint32, on `stream`): the
  * cut found by that search, and the first failing and last passing bit
  * pattern of a scan of the decision over every non-negative float up to

@@ -370,7 +370,7 @@ __device__ __forceinline__ int next_tile(int *work, int &s_slot, bool first) {
 #define LIG_RASTER_FWD_FUSED 1  // specialised fused-loss forward (no opacities)
 #endif
 #ifndef LIG_RASTER_ALPHA_CUT
-#define LIG_RASTER_ALPHA_CUT 1  // fused forward / lean backward: alpha test by the cut's compare
+#define LIG_RASTER_ALPHA_CUT 1  // fused forward: alpha test by the cut's compare
 #endif
 // One CTA per tile, warp w = region w (8x4 pixels), one pixel per lane.
 // Batches of blockDim Gaussians (list order) are staged in shared memory, one
@@ -1030,11 +1030,8 @@ struct alignas(16) PixPair {
 // ABS: also the per-pixel absolute values of the mean gradient summed over
 // the pixels (the reference's v_xy_abs, csrc/backward.cu:146-150), in acc[2],
 // acc[3]: per pixel v_sigma (a dx + b dy) and v_sigma (b dx + c dy).
-// FAST: the Gaussian carries culling data and clamp >= 1/255 (or cut = 0 for
-// a clamp below it: nothing passes), so the test is the alpha cut's compare
-// and alpha = min(pass ? clamp : 0, exp(-sigma)) — the same value.
-template <int NCP, int CSTEP, int NR, bool ABS = false, bool FAST = false>
-__device__ __forceinline__ void lean_region_f2(const Rec<float> &g, float clamp, uint32_t cut,
+template <int NCP, int CSTEP, int NR, bool ABS = false>
+__device__ __forceinline__ void lean_region_f2(const Rec<float> &g, float clamp,
                                                const PixPair *__restrict__ pp, int c0, int r0,
                                                float px0, float py0, float (&acc)[11]) {
     const float ha = 0.5f * g.a, hc = 0.5f * g.c;
@@ -1072,15 +1069,9 @@ __device__ __forceinline__ void lean_region_f2(const Rec<float> &g, float clamp,
             const f2 S = f2_fma(BDX, DY[r], f2_fma(HADX, DX, CDD[r]));
             float s0, s1;
             f2_unpack(S, s0, s1);
-            float a0, a1;
-            if constexpr (FAST) {
-                a0 = fminf(__float_as_uint(s0) < cut ? clamp : 0.f, __expf(-s0));
-                a1 = fminf(__float_as_uint(s1) < cut ? clamp : 0.f, __expf(-s1));
-            } else {
-                const float al0 = fminf(clamp, __expf(-s0)), al1 = fminf(clamp, __expf(-s1));
-                a0 = (s0 < 0.f || al0 < 1.f / 255.f) ? 0.f : al0;
-                a1 = (s1 < 0.f || al1 < 1.f / 255.f) ? 0.f : al1;
-            }
+            const float al0 = fminf(clamp, __expf(-s0)), al1 = fminf(clamp, __expf(-s1));
+            const float a0 = (s0 < 0.f || al0 < 1.f / 255.f) ? 0.f : al0;
+            const float a1 = (s1 < 0.f || al1 < 1.f / 255.f) ? 0.f : al1;
             const f2 A = f2_pack(a0, a1);
             sr = f2_fma(A, V0, sr);
             sg = f2_fma(A, V1, sg);
@@ -1178,7 +1169,7 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
                                          const Rec<T> *__restrict__ recs,
                                          const int32_t *__restrict__ final_idx, CotSrc<T> cot,
                                          const T *__restrict__ v_dx, const T *__restrict__ v_dy,
-                                         const T *__restrict__ v_dxy, T clamp, uint32_t cut,
+                                         const T *__restrict__ v_dxy, T clamp,
                                          T *__restrict__ packed, int &s_end, uint32_t bar,
                                          uint32_t &phase) {
     using M = Math<T>;
@@ -1188,8 +1179,6 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
     // records staged by bulk async copies (no register prefetch, no region
     // masks: the warps test the box and ellipse themselves)
     constexpr bool kBulk = kPairs && LIG_RASTER_BWD_BULK;
-    // the alpha cut's compare in the pair walk (float)
-    constexpr bool kCut = kPairs && LIG_RASTER_ALPHA_CUT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nt = blockDim.x;  // = 32 * regions: region-major pixel slots
     PixRec<T, GA> *s_pix = reinterpret_cast<PixRec<T, GA> *>(smem_raw);
@@ -1311,13 +1300,11 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
         }
         // compact the batch slots touching this region (ascending)
         int nmine = 0;
-        bool exact = false;  // a listed Gaussian without culling data
         for (int m = 0; m * 32 < cnt; ++m) {
             const int t = m * 32 + lane;
             bool hit;
             if constexpr (kBulk) hit = t < cnt && region_hit<T, false, false>(s_rec[t], R, w, tx0, ty0);
             else hit = t < cnt && ((s_bits[t] >> w) & 1u);
-            if constexpr (kCut) exact = exact || (hit && !(s_rec[t].wx >= (T)0));
             if (LIG_RASTER_BWD_LANE_ELLIPSE && hit) {
                 // exact ellipse test of Gaussian t against this warp's region,
                 // one Gaussian per lane (the staging only tested the box)
@@ -1333,11 +1320,6 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
             nmine += __popc(mask);
         }
         __syncwarp();
-        // the alpha cut's compare when every Gaussian this warp lists has
-        // culling data (warp-uniform)
-        const bool fast = kCut && !__any_sync(FULL, exact);
-        auto run_list = [&](auto fast_tag) {
-        constexpr bool FAST = decltype(fast_tag)::value;
         for (int g0 = 0, lsplit = 0; g0 < nmine; g0 += 32 >> lsplit) {
             // lanes per Gaussian: with at most 4 / 8 / LIG_RASTER_BWD_SPLIT1
             // Gaussians left, 8 / 4 / 2 lanes share one Gaussian (a round
@@ -1366,38 +1348,20 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
                 const float px0 = (float)(tx0 + (w % R.nbx) * 8) + 0.5f;
                 const float py0 = (float)(ty0 + (w / R.nbx) * 4) + 0.5f;
                 const PixPair *pp = reinterpret_cast<const PixPair *>(smem_raw) + w * 16;
-                if (act && FAST) {
+                if (act) {
                     switch (lsplit) {
                     case 0:
-                        lean_region_f2<4, 1, 4, ABS, true>(g, clamp, cut, pp, 0, 0, px0, py0, acc);
+                        lean_region_f2<4, 1, 4, ABS>(g, clamp, pp, 0, 0, px0, py0, acc);
                         break;
                     case 1:
-                        lean_region_f2<2, 2, 4, ABS, true>(g, clamp, cut, pp, part, 0, px0, py0,
-                                                           acc);
+                        lean_region_f2<2, 2, 4, ABS>(g, clamp, pp, part, 0, px0, py0, acc);
                         break;
                     case 2:
-                        lean_region_f2<1, 1, 4, ABS, true>(g, clamp, cut, pp, part, 0, px0, py0,
-                                                           acc);
+                        lean_region_f2<1, 1, 4, ABS>(g, clamp, pp, part, 0, px0, py0, acc);
                         break;
                     default:
-                        lean_region_f2<1, 1, 2, ABS, true>(g, clamp, cut, pp, part & 3,
-                                                           2 * (part >> 2), px0, py0, acc);
-                        break;
-                    }
-                } else if (act) {
-                    switch (lsplit) {
-                    case 0:
-                        lean_region_f2<4, 1, 4, ABS>(g, clamp, cut, pp, 0, 0, px0, py0, acc);
-                        break;
-                    case 1:
-                        lean_region_f2<2, 2, 4, ABS>(g, clamp, cut, pp, part, 0, px0, py0, acc);
-                        break;
-                    case 2:
-                        lean_region_f2<1, 1, 4, ABS>(g, clamp, cut, pp, part, 0, px0, py0, acc);
-                        break;
-                    default:
-                        lean_region_f2<1, 1, 2, ABS>(g, clamp, cut, pp, part & 3,
-                                                     2 * (part >> 2), px0, py0, acc);
+                        lean_region_f2<1, 1, 2, ABS>(g, clamp, pp, part & 3, 2 * (part >> 2),
+                                                     px0, py0, acc);
                         break;
                     }
                 }
@@ -1559,9 +1523,6 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
                 }
             }
         }
-        };
-        if (fast) run_list(std::true_type{});
-        else run_list(std::false_type{});
     }
 }
 
@@ -1585,15 +1546,11 @@ raster_bwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work
         __syncthreads();
     }
     const int n_tiles = geo.total_tiles();
-    // the alpha cut (pack_kernel wrote it before this launch); a clamp below
-    // 1/255 rejects every term, which cut = 0 says
-    uint32_t cut = 0;
-    if (LEAN && !GA && sizeof(T) == 4 && (float)clamp >= 1.f / 255.f) cut = g_alpha_cut;
     for (int tile = next_tile(work, s_slot, true); tile < n_tiles;
          tile = next_tile(work, s_slot, false)) {
         const TileCtx tc = tile_ctx(geo, cum, d_total, tile);
         bwd_tile<T, GA, LEAN, ABS>(tc, tile, ids, tile_bins, recs, final_idx, cot, v_dx, v_dy,
-                                   v_dxy, clamp, cut, packed, s_end, bar, phase);
+                                   v_dxy, clamp, packed, s_end, bar, phase);
     }
 }
 

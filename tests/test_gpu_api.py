@@ -404,8 +404,9 @@ def test_alpha_cut_is_the_step_of_the_alpha_test():
 @pytest.mark.parametrize("H,W,B,n", [(150, 170, 16, 3000),
                                      (1040, 1100, 16, 20000)])  # four pixels per lane
 def test_alpha_cut_paths_with_degenerate_gaussians(H, W, B, n):
-    """Chunks that hold a Gaussian without culling data take the float alpha
-    test, the rest the cut's compare.  Mixed in: non-positive-definite
+    """In the fused forward, chunks that hold a Gaussian without culling data
+    take the float alpha test, the rest the cut's compare.  Mixed in:
+    non-positive-definite
     conics; negative-definite ones centred exactly on a pixel centre (sigma
     is -0 there: the reference passes it with alpha = clamp); conics whose
     entries times the squared cull reach come near the float range (no
