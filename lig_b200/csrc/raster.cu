@@ -251,19 +251,25 @@ struct Regions {
 // [dx0, dx1] x [dy0, dy1] (positive-definite conic): zero if the rectangle
 // holds the origin, else the least of the four edge minima (each a clamped
 // 1-D quadratic minimum).
+// With the centre outside the rectangle the minimum lies on an edge that
+// faces the centre (at the minimiser every active bound's inward move must
+// not decrease sigma, while the direction to the centre does; that direction
+// points outward only across facing edges), so at most one vertical and one
+// horizontal edge are evaluated: x = dx0 when dx0 > 0, x = dx1 when dx1 < 0,
+// and likewise in y.
 template <typename T>
 __device__ __forceinline__ T sigma_min_rect(T a, T b, T c, T dx0, T dx1, T dy0, T dy1) {
-    if (dx0 <= (T)0 && dx1 >= (T)0 && dy0 <= (T)0 && dy1 >= (T)0) return (T)0;
-    const T ia = (T)1 / a, ic = (T)1 / c;
+    const bool ox = dx0 > (T)0 || dx1 < (T)0, oy = dy0 > (T)0 || dy1 < (T)0;
+    if (!ox && !oy) return (T)0;
     T best = (T)3.0e38;
-    const T xs[2] = {dx0, dx1}, ys[2] = {dy0, dy1};
-#pragma unroll
-    for (int e = 0; e < 2; ++e) {
-        T dx = xs[e];
-        T dy = min(max(-b * dx * ic, dy0), dy1);
-        best = min(best, (T)0.5 * (a * dx * dx + c * dy * dy) + b * dx * dy);
-        dy = ys[e];
-        dx = min(max(-b * dy * ia, dx0), dx1);
+    if (ox) {
+        const T dx = dx0 > (T)0 ? dx0 : dx1;
+        const T dy = min(max(-b * dx / c, dy0), dy1);
+        best = (T)0.5 * (a * dx * dx + c * dy * dy) + b * dx * dy;
+    }
+    if (oy) {
+        const T dy = dy0 > (T)0 ? dy0 : dy1;
+        const T dx = min(max(-b * dy / a, dx0), dx1);
         best = min(best, (T)0.5 * (a * dx * dx + c * dy * dy) + b * dx * dy);
     }
     return best;
