@@ -54,12 +54,13 @@ DIAG = (0.5, 6.0)
 BLOCK = 16
 FLOP_PER_EVAL = {"lig_raster_fwd": 20.0, "lig_raster_bwd": 40.0, "lig_raster_bwd_l2": 40.0,
                  "lig_raster_fwd_l2": 20.0, "lig_raster_bwd_diff": 40.0,
-                 "lig_raster_fwd_l2_batch": 20.0, "lig_raster_bwd_diff_batch": 40.0}
+                 "lig_raster_fwd_l2_batch": 20.0, "lig_raster_fwd_l2_u8_batch": 20.0,
+                 "lig_raster_bwd_diff_batch": 40.0}
 # DRAM bytes (read + write) per launch measured by an ncu capture of the same
 # kernels on the 2048^2 / 125k-Gaussian step (same density); traffic grows
 # with pixels and Gaussians, so a size-S launch is scaled by (S / 2048)^2.
-DRAM_BYTES_2048 = {"lig_raster_fwd_l2_batch": 59.8e6 + 23.2e6,
-                   "lig_raster_bwd_diff_batch": 80.9e6 + 3.6e6}
+DRAM_BYTES_2048 = {"lig_raster_fwd_l2_u8_batch": 21.7e6 + 15.3e6,
+                   "lig_raster_bwd_diff_batch": 63.9e6 + 2.0e6}
 CLOCK_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
