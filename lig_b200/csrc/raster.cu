@@ -81,8 +81,9 @@ __device__ __forceinline__ uint32_t alpha_cut_search() {
     return hi;
 }
 
-// The cut on this device, written by every float pack launch (always the same
-// value) and read by the rasterizers launched after it on the same stream.
+// The cut on this device, written by every pack launch for the fused forward
+// (always the same value) and read by that forward, launched after it on the
+// same stream.
 __device__ uint32_t g_alpha_cut;
 
 // ------------------------------------------------------------------ pack
@@ -106,12 +107,12 @@ __device__ uint32_t g_alpha_cut;
 // forward, see sigma_half); the cull data are computed from the full conic.
 // zero (backward): also clears the Gaussian's zero_stride accumulators there
 // (zero_stride * sizeof(T) a multiple of 16 bytes, 16-byte aligned).
-// Block 0's first warp (float) also publishes the alpha cut.
+// HALF (float): block 0's first warp also publishes the alpha cut.
 template <typename T, bool HALF>
 __global__ void pack_kernel(int n, const T *__restrict__ xys, const T *__restrict__ conics,
                             const T *__restrict__ colors, const T *__restrict__ opac,
                             Rec<T> *__restrict__ recs, T *__restrict__ zero, int zero_stride) {
-    if (sizeof(T) == 4 && blockIdx.x == 0 && threadIdx.x < 32) {
+    if (HALF && sizeof(T) == 4 && blockIdx.x == 0 && threadIdx.x < 32) {
         const uint32_t cut = alpha_cut_search();
         if (threadIdx.x == 0) g_alpha_cut = cut;
     }
@@ -144,8 +145,9 @@ __global__ void pack_kernel(int n, const T *__restrict__ xys, const T *__restric
         double tc = t > 0.01 ? t : 0.01;
         double sxx = c / det, syy = a / det;
         double hx = 1.001 * sqrt(tc * sxx) + 2.0, hy = 1.001 * sqrt(tc * syy) + 2.0;
-        const double reach = fmax(hx, hy) + 16.0;
-        if (hx < 1e7 && hy < 1e7 && fmax(fmax(a, c), fabs(b)) * reach * reach < 1e36) {
+        const float reach = (float)fmax(hx, hy) + 16.f;
+        if (hx < 1e7 && hy < 1e7 &&
+            fmaxf(fmaxf((float)r.a, (float)r.c), fabsf((float)r.b)) * reach * reach < 1e36f) {
             wx = (T)hx;
             wy = (T)hy;
             r.thr = (T)(0.5 * tc * 1.001 + 0.02);
