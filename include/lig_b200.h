@@ -192,7 +192,10 @@ size_t lig_l2_tile_partials_bytes(int num_tiles);
  * (0 <= x <= 1) ? clamp(x, 0, 1) - target : 0 instead of the image x, and
  * *loss = mean((clamp(x, 0, 1) - target)^2) (gaussianlig.py:95-102) is reduced
  * deterministically from per-tile fp64 partials.  final_idx as
- * lig_raster_fwd.  Workspace: lig_raster_workspace_bytes. */
+ * lig_raster_fwd, or NULL: the fit loop's backward without opacities never
+ * reads it, and without it the forward neither tracks nor writes the
+ * per-pixel last index (4 bytes a pixel).  The same holds for the _u8 and
+ * batched forms below.  Workspace: lig_raster_workspace_bytes. */
 int lig_raster_fwd_l2(int dtype, int img_h, int img_w, int block_width, int num_points,
                       const int32_t *gaussian_ids_sorted, const int32_t *tile_bins,
                       const int32_t *num_intersects, const void *xys, const void *conics,
@@ -203,7 +206,8 @@ int lig_raster_fwd_l2(int dtype, int img_h, int img_w, int block_width, int num_
 /* Sum backward of that loss from the forward's diff: pixel cotangent
  * diff * 2 / (3 H W) * grad_loss (equal to lig_raster_bwd_l2's).  As in
  * lig_raster_bwd_l2, with opacities == NULL the fit needs neither |v_xy| nor
- * an opacity gradient: v_xy_abs is written as zeros and not accumulated. */
+ * an opacity gradient: v_xy_abs is written as zeros and not accumulated;
+ * final_idx is then not read and may be NULL (also in the batched form). */
 int lig_raster_bwd_diff(int dtype, int img_h, int img_w, int block_width, int num_points,
                         const int32_t *gaussian_ids_sorted, const int32_t *tile_bins,
                         const int32_t *num_intersects, const void *xys, const void *conics,

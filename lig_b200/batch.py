@@ -308,11 +308,13 @@ class BatchedFit:
         call(fwd, _lib.LIG_F32, *L.args(), L.block, _p(self.gids),
              _p(self.bins), _p(self.total), _p(self.cum), _p(self.xys), _p(self.con),
              _p(self.rgbs), None, _p(tgt), int(self.persistent), _p(self.work),
-             _p(self.r_ws), self.r_ws.numel(), _p(self.partials), _p(self.img), _p(self.fin),
+             _p(self.r_ws), self.r_ws.numel(), _p(self.partials), _p(self.img), None,
              _p(self.loss), _p(self.per_image), st)
+        # no opacities: the backward reads no final indices, so the forward
+        # neither tracks nor writes them
         call("lig_raster_bwd_diff_batch", _lib.LIG_F32, *L.args(), L.block, _p(self.gids),
              _p(self.bins), _p(self.total), _p(self.cum), _p(self.xys), _p(self.con),
-             _p(self.rgbs), None, _p(self.fin), _p(self.img), _p(self.one), 0.0,
+             _p(self.rgbs), None, None, _p(self.img), _p(self.one), 0.0,
              int(self.persistent), _p(self.work), _p(self.r_ws), self.r_ws.numel(),
              _p(self.v_xy), _p(self.v_abs), _p(self.v_con), _p(self.g_rgbs), None, st)
         call("lig_project_bwd_batch", _lib.LIG_F32, *L.args(), 1, _p(self.chol), _p(self.means),

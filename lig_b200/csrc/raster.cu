@@ -458,12 +458,13 @@ struct FwdAcc {
     T r = 0, g = 0, b = 0, w = 0;
     T dx[GA ? 3 : 1] = {}, dy[GA ? 3 : 1] = {}, dxy[GA ? 3 : 1] = {};
     int cur = 0;
-    // fused-loss forward: colour and final index only (no wsum, not GA)
+    // fused-loss forward: colour and, with FIN, the final index (no wsum, not GA)
+    template <bool FIN = true>
     __device__ __forceinline__ void add_fused(const Rec<T> &q, T a, int idx) {
         r += q.r * a;
         g += q.g * a;
         b += q.bl * a;
-        cur = idx;
+        if constexpr (FIN) cur = idx;
     }
     __device__ __forceinline__ void add(const Rec<T> &q, T dxp, T dyp, T a, int idx) {
         // csrc/forward.cu:264-269, csrc/gradient_aware_rasterizer.cu:451-482
@@ -542,7 +543,7 @@ __device__ __forceinline__ double fwd_write(const FwdAcc<T, GA> &acc, bool insid
                                             int32_t *__restrict__ final_idx,
                                             const L2Fwd<T> &l2) {
     if (!inside) return 0.0;
-    final_idx[pix] = acc.cur;
+    if (final_idx) final_idx[pix] = acc.cur;
     if (l2.on()) {
         double sq = 0;
         const T x[3] = {acc.r, acc.g, acc.b};
@@ -576,7 +577,7 @@ __device__ __forceinline__ double fwd_write(const FwdAcc<T, GA> &acc, bool insid
 // added in list order either way.
 // FL: the fused-loss forward without opacities (records carry the halved
 // conic; no wsum): per pixel the same alphas and colour sums, fewer operations.
-template <typename T, bool GA, int PPL, bool FL>
+template <typename T, bool GA, int PPL, bool FL, bool FIN = true>
 __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int32_t *__restrict__ ids,
                                          const int2 *__restrict__ tile_bins,
                                          const Rec<T> *__restrict__ recs, T *__restrict__ img,
@@ -627,10 +628,10 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
                     const Rec<T> g2 = rb[b2];
                     T a2;
                     const bool ok2 = PixelEval<T>::alpha_fused(g2, px[0], py[0], a2);
-                    if (ok1) acc[0].add_fused(g1, a1, ib + b1);
-                    if (ok2) acc[0].add_fused(g2, a2, ib + b2);
+                    if (ok1) acc[0].template add_fused<FIN>(g1, a1, ib + b1);
+                    if (ok2) acc[0].template add_fused<FIN>(g2, a2, ib + b2);
                 } else if (ok1) {
-                    acc[0].add_fused(g1, a1, ib + b1);
+                    acc[0].template add_fused<FIN>(g1, a1, ib + b1);
                 }
             }
         } else if constexpr (FL) {
@@ -655,7 +656,7 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
                 }
 #pragma unroll
                 for (int p = 0; p < PPL; ++p)
-                    if (okp[p]) acc[p].add_fused(g1, ap[p], ib + b1);
+                    if (okp[p]) acc[p].template add_fused<FIN>(g1, ap[p], ib + b1);
             }
         } else if constexpr (PPL == 1) {
             while (mask) {
@@ -793,7 +794,7 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
 #define LIG_RASTER_PPL4_MIN_TILES 4096  // measured: faster from 2048^2 up, not at 512^2
 #endif
 
-template <typename T, bool GA, int PPL, int MAXT, int MINB, bool FL = false>
+template <typename T, bool GA, int PPL, int MAXT, int MINB, bool FL = false, bool FIN = true>
 __global__ void __launch_bounds__(MAXT, MINB)
 raster_fwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work,
                   const int32_t *__restrict__ ids, const int2 *__restrict__ tile_bins,
@@ -810,8 +811,8 @@ raster_fwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work
     for (int tile = next_tile(work, s_slot, true); tile < n_tiles;
          tile = next_tile(work, s_slot, false)) {
         const TileCtx tc = tile_ctx(geo, cum, d_total, tile);
-        fwd_tile<T, GA, PPL, FL>(tc, tile, ids, tile_bins, recs, img, wsum, odx, ody, odxy,
-                                 final_idx, s_rec, s_bits, l2, cut);
+        fwd_tile<T, GA, PPL, FL, FIN>(tc, tile, ids, tile_bins, recs, img, wsum, odx, ody, odxy,
+                                      final_idx, s_rec, s_bits, l2, cut);
     }
 }
 
@@ -1697,12 +1698,18 @@ int raster_fwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
     constexpr int FM = LIG_RASTER_FWD_MINB;
     K fn = ga ? (small ? raster_fwd_kernel<T, true, 1, 256, FM>
                        : raster_fwd_kernel<T, true, 1, 1024, 1>)
-         : fl ? (ppl4 ? (small ? raster_fwd_kernel<T, false, 4, 256, FM, true>
-                               : raster_fwd_kernel<T, false, 4, 1024, 1, true>)
-                 : ppl2 ? (small ? raster_fwd_kernel<T, false, 2, 256, FM, true>
-                                 : raster_fwd_kernel<T, false, 2, 1024, 1, true>)
-                        : (small ? raster_fwd_kernel<T, false, 1, 256, FM, true>
-                                 : raster_fwd_kernel<T, false, 1, 1024, 1, true>))
+         : fl && fin ? (ppl4 ? (small ? raster_fwd_kernel<T, false, 4, 256, FM, true>
+                                      : raster_fwd_kernel<T, false, 4, 1024, 1, true>)
+                        : ppl2 ? (small ? raster_fwd_kernel<T, false, 2, 256, FM, true>
+                                        : raster_fwd_kernel<T, false, 2, 1024, 1, true>)
+                               : (small ? raster_fwd_kernel<T, false, 1, 256, FM, true>
+                                        : raster_fwd_kernel<T, false, 1, 1024, 1, true>))
+         : fl ? (ppl4 ? (small ? raster_fwd_kernel<T, false, 4, 256, FM, true, false>
+                               : raster_fwd_kernel<T, false, 4, 1024, 1, true, false>)
+                 : ppl2 ? (small ? raster_fwd_kernel<T, false, 2, 256, FM, true, false>
+                                 : raster_fwd_kernel<T, false, 2, 1024, 1, true, false>)
+                        : (small ? raster_fwd_kernel<T, false, 1, 256, FM, true, false>
+                                 : raster_fwd_kernel<T, false, 1, 1024, 1, true, false>))
               : ppl4 ? (small ? raster_fwd_kernel<T, false, 4, 256, LIG_RASTER_FWD_MINB>
                               : raster_fwd_kernel<T, false, 4, 1024, 1>)
               : ppl2 ? (small ? raster_fwd_kernel<T, false, 2, 256, LIG_RASTER_FWD_MINB>
@@ -2155,7 +2162,7 @@ extern "C" int lig_raster_fwd_l2(int dtype, int H, int W, int B, int n, const in
                                  double *tile_partials, void *diff, int32_t *fin, void *loss,
                                  void *stream) {
     if (!raster_args_ok(H, W, B, n) || !bins || !d_total || !target || !ws || !tile_partials ||
-        !diff || !fin || !loss || (n > 0 && (!xys || !con || !col)))
+        !diff || !loss || (n > 0 && (!xys || !con || !col)))
         return LIG_ERR_INVALID;
     const BatchGeo geo = BatchGeo::single(H, W, B, n);
     cudaStream_t s = (cudaStream_t)stream;
@@ -2175,7 +2182,7 @@ extern "C" int lig_raster_fwd_l2_u8(int dtype, int H, int W, int B, int n, const
                                     double *tile_partials, void *diff, int32_t *fin, void *loss,
                                     void *stream) {
     if (!raster_args_ok(H, W, B, n) || !bins || !d_total || !target || !ws || !tile_partials ||
-        !diff || !fin || !loss || (n > 0 && (!xys || !con || !col)))
+        !diff || !loss || (n > 0 && (!xys || !con || !col)))
         return LIG_ERR_INVALID;
     const BatchGeo geo = BatchGeo::single(H, W, B, n);
     cudaStream_t s = (cudaStream_t)stream;
@@ -2195,8 +2202,8 @@ extern "C" int lig_raster_bwd_diff(int dtype, int H, int W, int B, int n, const 
                                    double clamp, void *ws, size_t ws_bytes, void *v_xy,
                                    void *v_abs, void *v_con, void *v_rgb, void *v_op,
                                    void *stream) {
-    if (!raster_args_ok(H, W, B, n) || !bins || !d_total || !fin || !diff || !grad_loss || !ws ||
-        (n > 0 && (!xys || !con || !col || !v_xy || !v_abs || !v_con || !v_rgb)))
+    if (!raster_args_ok(H, W, B, n) || !bins || !d_total || (!fin && op) || !diff ||
+        !grad_loss || !ws || (n > 0 && (!xys || !con || !col || !v_xy || !v_abs || !v_con || !v_rgb)))
         return LIG_ERR_INVALID;
     if (n == 0) return LIG_OK;
     const BatchGeo geo = BatchGeo::single(H, W, B, n);
@@ -2223,7 +2230,7 @@ extern "C" int lig_raster_fwd_l2_batch(int dtype, int n_img, const int32_t *heig
     BatchGeo geo;
     if (!batch_geo(n_img, heights, widths, counts, B, geo)) return LIG_ERR_INVALID;
     const int n = geo.total_points();
-    if (!bins || !d_total || !target || !ws || !tile_partials || !diff || !fin || !loss ||
+    if (!bins || !d_total || !target || !ws || !tile_partials || !diff || !loss ||
         (persistent && !work) || (n > 0 && (!xys || !con || !col || !cum)))
         return LIG_ERR_INVALID;
     TileWalk walk{n > 0 ? cum : nullptr, persistent ? work : nullptr};
@@ -2249,7 +2256,7 @@ extern "C" int lig_raster_fwd_l2_u8_batch(int dtype, int n_img, const int32_t *h
     BatchGeo geo;
     if (!batch_geo(n_img, heights, widths, counts, B, geo)) return LIG_ERR_INVALID;
     const int n = geo.total_points();
-    if (!bins || !d_total || !target || !ws || !tile_partials || !diff || !fin || !loss ||
+    if (!bins || !d_total || !target || !ws || !tile_partials || !diff || !loss ||
         (persistent && !work) || (n > 0 && (!xys || !con || !col || !cum)))
         return LIG_ERR_INVALID;
     TileWalk walk{n > 0 ? cum : nullptr, persistent ? work : nullptr};
@@ -2276,7 +2283,7 @@ extern "C" int lig_raster_bwd_diff_batch(int dtype, int n_img, const int32_t *he
     BatchGeo geo;
     if (!batch_geo(n_img, heights, widths, counts, B, geo)) return LIG_ERR_INVALID;
     const int n = geo.total_points();
-    if (!bins || !d_total || !fin || !diff || !grad_loss || !ws || (persistent && !work) ||
+    if (!bins || !d_total || (!fin && op) || !diff || !grad_loss || !ws || (persistent && !work) ||
         (n > 0 && (!xys || !con || !col || !cum || !v_xy || !v_abs || !v_con || !v_rgb)))
         return LIG_ERR_INVALID;
     if (n == 0) return LIG_OK;

@@ -27,8 +27,10 @@ class _RenderL2(Function):
         target = target.reshape(H, W, 3)
 
         def enqueue(b):
+            # the backward reads final indices only with opacities
             return ops.raster_fwd_l2(H, W, block, b.gaussian_ids_sorted, b.tile_bins, b.total,
-                                     xys, con, colors, opacities, target)
+                                     xys, con, colors, opacities, target,
+                                     want_final_idx=opacities is not None)
 
         binning, (diff, fin, loss) = ops.bin_gaussians(xys, ext, cnt, H, W, block,
                                                        after_enqueue=enqueue)

@@ -422,12 +422,14 @@ def raster_bwd_l2(img_h, img_w, block, gaussian_ids_sorted, tile_bins, total, xy
 
 
 def raster_fwd_l2(img_h, img_w, block, gaussian_ids_sorted, tile_bins, total, xys, conics,
-                  colors, opacities, target):
+                  colors, opacities, target, want_final_idx: bool = True):
     """Fit-loop forward with the clamped-L2 loss fused in.  Returns
     (diff [H,W,3], final_idx [H,W], loss 0-d): diff = (0 <= x <= 1) ?
     clamp(x) - target : 0 for the render x, loss = mean((clamp(x) - target)^2).
     A uint8 target (an RGB image as stored) is read as byte / 255, the value
-    torchvision's ToTensor gives."""
+    torchvision's ToTensor gives.  want_final_idx=False (the backward without
+    opacities never reads it): final_idx is None and the kernel neither
+    tracks nor writes it."""
     _check_cuda(xys, conics, colors, opacities, tile_bins, total, target)
     xys = _c(xys)
     dt = xys.dtype
@@ -442,7 +444,7 @@ def raster_fwd_l2(img_h, img_w, block, gaussian_ids_sorted, tile_bins, total, xy
     part = torch.empty((_lib.lib.lig_l2_tile_partials_bytes(tbx * tby) // 8,), dtype=torch.float64,
                        device=dev)
     diff = torch.empty((img_h, img_w, 3), dtype=dt, device=dev)
-    fin = torch.empty((img_h, img_w), dtype=torch.int32, device=dev)
+    fin = torch.empty((img_h, img_w), dtype=torch.int32, device=dev) if want_final_idx else None
     loss = torch.empty((), dtype=dt, device=dev)
     call("lig_raster_fwd_l2_u8" if u8 else "lig_raster_fwd_l2", code, int(img_h), int(img_w),
          int(block), n,

@@ -319,6 +319,30 @@ def test_fused_l2_forward_diff_and_loss(H, W, B, n):
         assert rel_err(np_(gb[i]), np_(full[i])) <= 1e-5
 
 
+@pytest.mark.parametrize("H,W,B,n", [(150, 170, 16, 3000),
+                                     (1040, 1100, 16, 20000)])  # >= 4096 tiles
+def test_fused_l2_without_final_indices(H, W, B, n):
+    """final_idx = NULL (the fit loop without opacities): the fused forward
+    gives the same masked difference and loss bit for bit without tracking or
+    writing the per-pixel last index, and the backward from the difference,
+    which then reads no final indices, gives the same gradients."""
+    means, L, colors, _ = scene(n, H, W, diag=(0.5, 5.0), seed=41)
+    g = torch.Generator().manual_seed(42)
+    target = torch.rand(H, W, 3, generator=g).cuda()
+    xys, ext, con, cnt = ops.project_fwd(L, means, None, H, W, B, True)
+    b = ops.bin_gaussians(xys, ext, cnt, H, W, B)
+    args = (H, W, B, b.gaussian_ids_sorted, b.tile_bins, b.total, xys, con, colors, None)
+    diff, fin, loss = ops.raster_fwd_l2(*args, target)
+    diff0, fin0, loss0 = ops.raster_fwd_l2(*args, target, want_final_idx=False)
+    assert fin0 is None and fin is not None
+    assert torch.equal(diff0, diff) and torch.equal(loss0, loss)
+    one = torch.ones((), device="cuda")
+    ga = ops.raster_bwd_diff(*args, fin, diff, one)
+    gb = ops.raster_bwd_diff(*args, None, diff0, one)
+    for x, y in zip(ga[:4], gb[:4]):   # float atomics: the order of additions differs
+        assert rel_err(np_(x), np_(y)) <= 1e-5
+
+
 @pytest.mark.parametrize("seed,diag,offdiag", [(21, (0.3, 8.0), 4.0),    # thin, tilted
                                               (22, (0.2, 1.0), 0.05),   # small, axis-aligned
                                               (23, (2.0, 20.0), 8.0)])  # large, tilted
