@@ -775,7 +775,7 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
 #define LIG_RASTER_BWD_SPLIT 1  // split a short list's Gaussians across lanes (measured faster)
 #endif
 #ifndef LIG_RASTER_BWD_SPLIT1
-#define LIG_RASTER_BWD_SPLIT1 20  // with up to this many Gaussians left, 2 lanes take one
+#define LIG_RASTER_BWD_SPLIT1 24  // with up to this many Gaussians left, 2 lanes take one
 #endif
 #ifndef LIG_RASTER_BWD_LANE_ELLIPSE
 #define LIG_RASTER_BWD_LANE_ELLIPSE 1  // ellipse culling by the warp's lanes (measured faster)
