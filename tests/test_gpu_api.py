@@ -281,6 +281,8 @@ def test_fused_l2_forward_nonfinite_colours():
 
 @pytest.mark.parametrize("H,W,B,n", [(150, 170, 16, 3000),
                                      (1040, 1100, 16, 20000),  # >= 4096 tiles: four pixels per lane
+                                     (600, 560, 8, 8000),      # >= 4096 tiles, 8x8 tiles
+                                     (2048, 2080, 32, 60000),  # >= 4096 tiles, 32x32 tiles
                                      (97, 203, 12, 2500),
                                      (130, 90, 32, 2000)])
 def test_fused_l2_forward_diff_and_loss(H, W, B, n):

@@ -173,15 +173,29 @@ def _train_py_run(arm, png, tmp, n, iters):
 
 
 def test_train_py_two_level_psnr_matches_reference(tmp_path):
+    """train.py's free-running two-level fit, three runs per arm, medians
+    compared.  The fit is chaotic for both implementations: any two runs,
+    the reference against itself included, part by more than 1e-3 dB within
+    about 30 of the 300 iterations (the backward's float atomics add in a
+    run-dependent order), and the final PSNR has a heavy tail because level 2
+    fits a residual min-max-normalised by level 1's extreme pixels, so one
+    run in several can land far from the rest (+1.4 dB was seen).  The
+    median of three is robust to one such run on either side."""
     from PIL import Image
     gt = _target(256, 256, seed=6)
     arr = (gt[0].permute(1, 2, 0).cpu().numpy() * 255).round().astype(np.uint8)
     png = tmp_path / "synthetic_0001.png"
     Image.fromarray(arr).save(png)
-    mine = _train_py_run("lig", png, tmp_path, 12000, 300)
-    ref = _train_py_run("ref", png, tmp_path, 12000, 300)
-    assert "lig_b200" in mine["origin"] and "_ref" in ref["origin"]
-    assert abs(mine["psnr"] - ref["psnr"]) <= 0.05, (mine["psnr"], ref["psnr"])
+    runs = {"lig": [], "ref": []}
+    for rep in range(3):
+        for arm in ("lig", "ref"):
+            runs[arm].append(_train_py_run(arm, png, tmp_path / f"{arm}{rep}", 12000, 300))
+    mine = sorted(runs["lig"], key=lambda r: r["psnr"])[1]
+    ref = sorted(runs["ref"], key=lambda r: r["psnr"])[1]
+    assert all("lig_b200" in r["origin"] for r in runs["lig"])
+    assert all("_ref" in r["origin"] for r in runs["ref"])
+    assert abs(mine["psnr"] - ref["psnr"]) <= 0.05, (
+        [r["psnr"] for r in runs["lig"]], [r["psnr"] for r in runs["ref"]])
     # a fit that learns: far above the all-black start, and level 2 adds to level 1
     assert mine["psnr"] > mine["start"] + 10.0
     assert mine["psnr"] > mine["level1"] + 0.5
@@ -190,7 +204,7 @@ def test_train_py_two_level_psnr_matches_reference(tmp_path):
     for sa, sb in zip(mine["ckpt"]["state_dict"], ref["ckpt"]["state_dict"]):
         assert set(sa) == set(sb)
     np.testing.assert_allclose([float(v) for v in mine["ckpt"]["store_min"]],
-                               [float(v) for v in ref["ckpt"]["store_min"]], atol=1e-3)
+                               [float(v) for v in ref["ckpt"]["store_min"]], atol=1e-2)
 
 
 # ------------------------------------------------------- minimal_trainer_upscale.py
