@@ -58,7 +58,7 @@ template <typename T> struct alignas(16) Rec {
 //   pass  <=>  bits(sigma) < cut.
 // The cut is found on the device by the same expression: between 5.5
 // (__expf(-5.5) = 0.00409, 4% above 1/255 — far beyond __expf's error) and 5.6
-// (6% below) a warp narrows the bracket 32 ways per round (five rounds).
+// (6% below) a warp narrows the bracket 32 ways per round (four rounds).
 // lig_alpha_cut scans every non-negative float to show the decision is that
 // step and that the search finds its edge (a GPU test).
 __device__ __forceinline__ bool alpha_passes(float s) {
@@ -251,8 +251,8 @@ struct Regions {
 
 // Minimum of sigma(d) = 0.5 (a dx^2 + c dy^2) + b dx dy over the rectangle
 // [dx0, dx1] x [dy0, dy1] (positive-definite conic): zero if the rectangle
-// holds the origin, else the least of the four edge minima (each a clamped
-// 1-D quadratic minimum).
+// holds the origin, else the least of the edge minima (each a clamped 1-D
+// quadratic minimum).
 // With the centre outside the rectangle the minimum lies on an edge that
 // faces the centre (at the minimiser every active bound's inward move must
 // not decrease sigma, while the direction to the centre does; that direction
