@@ -771,6 +771,21 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
 #ifndef LIG_RASTER_BWD_LARGE_MIN_TILES
 #define LIG_RASTER_BWD_LARGE_MIN_TILES 4096
 #endif
+#ifndef LIG_RASTER_BWD_RROWS
+#define LIG_RASTER_BWD_RROWS 8  // float lean walks of large images: region rows (4, 8 or 16)
+#endif
+#ifndef LIG_RASTER_BWD_RROWS_MINB
+#define LIG_RASTER_BWD_RROWS_MINB 8  // resident CTAs per SM of the 8x8 walk (128 threads)
+#endif
+#ifndef LIG_RASTER_BWD_R16_MINB
+#define LIG_RASTER_BWD_R16_MINB 16  // resident CTAs per SM of the 8x16 walk (64 threads)
+#endif
+#ifndef LIG_RASTER_BWD_SPLIT2
+#define LIG_RASTER_BWD_SPLIT2 8  // with up to this many Gaussians left, 4 lanes take one
+#endif
+#ifndef LIG_RASTER_BWD_SPLIT3
+#define LIG_RASTER_BWD_SPLIT3 4  // with up to this many Gaussians left, 8 lanes take one
+#endif
 #ifndef LIG_RASTER_BWD_SPLIT
 #define LIG_RASTER_BWD_SPLIT 1  // split a short list's Gaussians across lanes (measured faster)
 #endif
@@ -1030,16 +1045,18 @@ struct alignas(16) PixPair {
 
 // lean_region in f32x2 form (float): the lane takes NCP column pairs
 // c0, c0 + CSTEP, ... (columns cp and cp + 4 of each) in NR rows r0.. of the
-// 8x4 region, and evaluates the two pixels of a pair with one packed
+// 8-column region, and evaluates the two pixels of a pair with one packed
 // operation where lean_region uses two.  Per pixel the operations and their
 // roundings are lean_region's — sigma = fma(b dx, dy, fma((a/2) dx, dx,
 // ((c/2) dy) dy)), alpha = min(clamp, exp(-sigma)) and the same alpha test —
 // so the alpha decisions are bit-identical; only the order in which the
-// moment and colour sums are added differs.  Same outputs in acc[].
+// moment and colour sums are added differs.  Same quantities as lean_region,
+// added to acc[] (zeroed by the caller), so that an 8x8 region can be walked
+// as two 8x4 halves (pp then holds 8 rows of 4 pair entries).
 // ABS: also the per-pixel absolute values of the mean gradient summed over
 // the pixels (the reference's v_xy_abs, csrc/backward.cu:146-150), in acc[2],
 // acc[3]: per pixel v_sigma (a dx + b dy) and v_sigma (b dx + c dy).
-template <int NCP, int CSTEP, int NR, bool ABS = false>
+template <int NCP, int CSTEP, int NR, bool ABS = false, int NH = 1>
 __device__ __forceinline__ void lean_region_f2(const Rec<float> &g, float clamp,
                                                const PixPair *__restrict__ pp, int c0, int r0,
                                                float px0, float py0, float (&acc)[11]) {
@@ -1052,15 +1069,20 @@ __device__ __forceinline__ void lean_region_f2(const Rec<float> &g, float clamp,
         CC = f2_dup(g.c);
     }
     const f2 CR = f2_dup(g.r), CG = f2_dup(g.g), CB = f2_dup(g.bl);
+    f2 sx = f2_zero(), sy = f2_zero(), sxx = f2_zero(), sxy = f2_zero(), syy = f2_zero();
+    f2 sr = f2_zero(), sg = f2_zero(), sb = f2_zero();
+    // NH blocks of NR rows, one after the other (not interleaved: the sums
+    // carry over, the row and column products are rebuilt per block)
+#pragma unroll 1
+    for (int hh = 0; hh < NH; ++hh) {
+    const int rb = r0 + hh * NR;
     f2 DY[NR], CDD[NR];
 #pragma unroll
     for (int r = 0; r < NR; ++r) {
-        const float dy = g.y - (py0 + (float)(r0 + r));
+        const float dy = g.y - (py0 + (float)(rb + r));
         DY[r] = f2_dup(dy);
         CDD[r] = f2_dup(__fmul_rn(__fmul_rn(hc, dy), dy));
     }
-    f2 sx = f2_zero(), sy = f2_zero(), sxx = f2_zero(), sxy = f2_zero(), syy = f2_zero();
-    f2 sr = f2_zero(), sg = f2_zero(), sb = f2_zero();
 #pragma unroll
     for (int k = 0; k < NCP; ++k) {
         const int cp = c0 + k * CSTEP;
@@ -1071,7 +1093,7 @@ __device__ __forceinline__ void lean_region_f2(const Rec<float> &g, float clamp,
         f2 wc = f2_zero(), yc = f2_zero();
 #pragma unroll
         for (int r = 0; r < NR; ++r) {
-            const PixPair *e = pp + (r0 + r) * 4 + cp;
+            const PixPair *e = pp + (rb + r) * 4 + cp;
             const ulonglong2 v01 = *reinterpret_cast<const ulonglong2 *>(e->v);
             const f2 V0{v01.x}, V1{v01.y};
             const f2 V2{*reinterpret_cast<const unsigned long long *>(e->v + 4)};
@@ -1105,12 +1127,13 @@ __device__ __forceinline__ void lean_region_f2(const Rec<float> &g, float clamp,
         sy = f2_add(sy, yc);
         sxy = f2_fma(yc, DX, sxy);
     }
-    acc[0] = -f2_sum(sx); acc[1] = -f2_sum(sy);
-    acc[4] = -f2_sum(sxx); acc[5] = -f2_sum(sxy); acc[6] = -f2_sum(syy);
-    acc[7] = f2_sum(sr); acc[8] = f2_sum(sg); acc[9] = f2_sum(sb);
+    }
+    acc[0] -= f2_sum(sx); acc[1] -= f2_sum(sy);
+    acc[4] -= f2_sum(sxx); acc[5] -= f2_sum(sxy); acc[6] -= f2_sum(syy);
+    acc[7] += f2_sum(sr); acc[8] += f2_sum(sg); acc[9] += f2_sum(sb);
     if constexpr (ABS) {
-        acc[2] = ax;
-        acc[3] = ay;
+        acc[2] += ax;
+        acc[3] += ay;
     }
 }
 
@@ -1171,7 +1194,14 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
 // cotangent): only the gradients the fit needs — v_xy, v_conic, v_rgb — are
 // accumulated (no |v_xy| sums, no opacity gradient) and each (Gaussian,
 // region) pair adds them with two 16-byte atomics into an [N][8] buffer.
-template <typename T, bool GA, bool LEAN, bool ABS = false>
+// RR (float pair walk only): region rows, 4 (8x4 regions, eight warps per
+// 16x16 tile), 8 (8x8, four warps, each thread staging two pixels) or 16
+// (8x16, two warps, four pixels a thread); a lane group walks a taller region
+// in blocks of four rows.
+// Against 8x4 regions a Gaussian meets fewer regions, so the per-pair costs —
+// the warps' region tests, the per-round set-up, the lane-group reduction and
+// the atomics — are paid fewer times, for more pixel evaluations per pair.
+template <typename T, bool GA, bool LEAN, bool ABS = false, int RR = 4>
 __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
                                          const int32_t *__restrict__ ids,
                                          const int2 *__restrict__ tile_bins,
@@ -1188,10 +1218,14 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
     // records staged by bulk async copies (no register prefetch, no region
     // masks: the warps test the box and ellipse themselves)
     constexpr bool kBulk = kPairs && LIG_RASTER_BWD_BULK;
+    static_assert(RR == 4 || kPairs, "taller regions are walked by the pair form only");
+    static_assert(RR == 4 || RR == 8 || RR == 16, "region rows");
+    constexpr int kRows = RR;  // pair entries per region: kRows * 4
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nt = blockDim.x;  // = 32 * regions: region-major pixel slots
     PixRec<T, GA> *s_pix = reinterpret_cast<PixRec<T, GA> *>(smem_raw);
-    Rec<T> *s_rec = reinterpret_cast<Rec<T> *>(s_pix + nt);
+    // (8x16 regions: two pixel slots a thread hold the pair entries)
+    Rec<T> *s_rec = reinterpret_cast<Rec<T> *>(s_pix + nt * (RR == 16 ? 2 : 1));
     uint32_t *s_bits = reinterpret_cast<uint32_t *>(s_rec + nt);
     int32_t *s_ids = reinterpret_cast<int32_t *>(s_bits + nt);
     uint16_t *s_list = reinterpret_cast<uint16_t *>(s_ids + nt);
@@ -1201,7 +1235,7 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
     const int B = tc.B, H = tc.H, W = tc.W, tx0 = tc.tx0, ty0 = tc.ty0;
     // fused L2: mean over this image's 3HW values (a batch sums per-image means)
     if (!cot.v_img) cot.scale = (T)(2.0 / (3.0 * (double)H * (double)W));
-    const Regions R = Regions::make(GA ? 2 : 0, B);
+    const Regions R = Regions::make(GA ? 2 : (RR == 8 ? 1 : RR == 16 ? 3 : 0), B);
     T rx0 = 0, rx1 = 0, ry0 = 0, ry1 = 0;  // this warp's region (tile-local centres)
     if (LIG_RASTER_BWD_LANE_ELLIPSE) R.rect<T>(w, rx0, rx1, ry0, ry1);
     uint16_t *my_list = s_list + w * nt;
@@ -1228,7 +1262,25 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
     }
     // stage this thread's pixel (region w, slot lane)
     if (!LEAN && tid == 0) s_end = -1;
-    {
+    if constexpr (RR > 4) {
+        // pixels (x, y + 4 p2) of region w; pair entries as below with RR rows
+        // per region
+#pragma unroll
+        for (int p2 = 0; p2 < RR / 4; ++p2) {
+            int lx, ly;
+            R.pixel(w, lane, p2, lx, ly);
+            const int gx = tx0 + lx, gy = ty0 + ly;
+            const bool inside = lx < B && ly < B && gx < W && gy < H;
+            T v0 = (T)0, v1 = (T)0, v2 = (T)0, vw;
+            if (inside) cot.get(tc.poff + gy * W + gx, v0, v1, v2, vw);
+            PixPair *e = reinterpret_cast<PixPair *>(smem_raw) + w * RR * 4 +
+                         ((lane >> 3) + 4 * p2) * 4 + (lane & 3);
+            const int h = (lane >> 2) & 1;
+            e->v[h] = v0;
+            e->v[2 + h] = v1;
+            e->v[4 + h] = v2;
+        }
+    } else {
         int lx, ly;
         R.pixel(w, lane, 0, lx, ly);
         const int gx = tx0 + lx, gy = ty0 + ly;
@@ -1330,15 +1382,17 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
         }
         __syncwarp();
         for (int g0 = 0, lsplit = 0; g0 < nmine; g0 += 32 >> lsplit) {
-            // lanes per Gaussian: with at most 4 / 8 / LIG_RASTER_BWD_SPLIT1
-            // Gaussians left, 8 / 4 / 2 lanes share one Gaussian (a round
+            // lanes per Gaussian: with at most LIG_RASTER_BWD_SPLIT3 / SPLIT2 /
+            // SPLIT1 Gaussians left, 8 / 4 / 2 lanes share one Gaussian (a round
             // then takes 4 / 8 / 16 of them), lane part p taking pixels
             // p, p + 2^lsplit, ... of the region (interleaved, so the group's
             // pixel records sit in different shared-memory banks); their
             // sums are combined below
             const int left = min(32, nmine - g0);
-            lsplit = !LIG_RASTER_BWD_SPLIT ? 0 : left <= 4 ? 3 : left <= 8 ? 2
-                                                 : left <= LIG_RASTER_BWD_SPLIT1 ? 1 : 0;
+            lsplit = !LIG_RASTER_BWD_SPLIT            ? 0
+                     : left <= LIG_RASTER_BWD_SPLIT3 ? 3
+                     : left <= LIG_RASTER_BWD_SPLIT2 ? 2
+                     : left <= LIG_RASTER_BWD_SPLIT1 ? 1 : 0;
             const int gi = lane >> lsplit, part = lane & ((1 << lsplit) - 1);
             const int jstep = 1 << lsplit;
             const int slot = gi < left ? (int)my_list[g0 + gi] : -1;
@@ -1355,9 +1409,28 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
                 // halves (8 lanes)
                 touched = act;
                 const float px0 = (float)(tx0 + (w % R.nbx) * 8) + 0.5f;
-                const float py0 = (float)(ty0 + (w / R.nbx) * 4) + 0.5f;
-                const PixPair *pp = reinterpret_cast<const PixPair *>(smem_raw) + w * 16;
-                if (act) {
+                const float py0 = (float)(ty0 + (w / R.nbx) * kRows) + 0.5f;
+                const PixPair *pp = reinterpret_cast<const PixPair *>(smem_raw) + w * kRows * 4;
+                if (act && RR > 4) {
+                    // the region in blocks of four rows (8 lanes: one half each)
+                    constexpr int NB = RR / 4;
+                    switch (lsplit) {
+                    case 0:
+                        lean_region_f2<4, 1, 4, ABS, NB>(g, clamp, pp, 0, 0, px0, py0, acc);
+                        break;
+                    case 1:
+                        lean_region_f2<2, 2, 4, ABS, NB>(g, clamp, pp, part, 0, px0, py0, acc);
+                        break;
+                    case 2:
+                        lean_region_f2<1, 1, 4, ABS, NB>(g, clamp, pp, part, 0, px0, py0, acc);
+                        break;
+                    default:
+                        lean_region_f2<1, 1, 4, ABS, NB / 2>(g, clamp, pp, part & 3,
+                                                             (RR / 2) * (part >> 2), px0, py0,
+                                                             acc);
+                        break;
+                    }
+                } else if (act) {
                     switch (lsplit) {
                     case 0:
                         lean_region_f2<4, 1, 4, ABS>(g, clamp, pp, 0, 0, px0, py0, acc);
@@ -1535,7 +1608,7 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
     }
 }
 
-template <typename T, bool GA, bool LEAN, int MAXT, int MINB, bool ABS = false>
+template <typename T, bool GA, bool LEAN, int MAXT, int MINB, bool ABS = false, int RR = 4>
 __global__ void __launch_bounds__(MAXT, MINB)
 raster_bwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work,
                   const int32_t *__restrict__ ids, const int2 *__restrict__ tile_bins,
@@ -1558,7 +1631,7 @@ raster_bwd_kernel(const BatchGeo geo, const int32_t *__restrict__ cum, int *work
     for (int tile = next_tile(work, s_slot, true); tile < n_tiles;
          tile = next_tile(work, s_slot, false)) {
         const TileCtx tc = tile_ctx(geo, cum, d_total, tile);
-        bwd_tile<T, GA, LEAN, ABS>(tc, tile, ids, tile_bins, recs, final_idx, cot, v_dx, v_dy,
+        bwd_tile<T, GA, LEAN, ABS, RR>(tc, tile, ids, tile_bins, recs, final_idx, cot, v_dx, v_dy,
                                    v_dxy, clamp, packed, s_end, bar, phase);
     }
 }
@@ -1772,9 +1845,15 @@ int raster_bwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
     int rc = pack<T>(n, xys, con, col, op, ws, goff, s, false, packed, stride);
     if (rc) return rc;
     const T cl = (T)(clamp > 0 ? clamp : (ga ? 0.999 : 0.99));
-    const int nt = 32 * Regions::make(ga ? 2 : 0, geo.B).count;
+    const bool large = geo.total_tiles() >= LIG_RASTER_BWD_LARGE_MIN_TILES;
+    // the float lean walks of large images: 8x8 regions (tiles up to 16x16)
+    const int rr = (LIG_RASTER_BWD_RROWS > 4 && sizeof(T) == 4 && LIG_RASTER_BWD_F2 &&
+                    (lean || lean_abs) && large && geo.B <= 16)
+                       ? LIG_RASTER_BWD_RROWS
+                       : 4;
+    const int nt = 32 * Regions::make(ga ? 2 : (rr == 8 ? 1 : rr == 16 ? 3 : 0), geo.B).count;
     const int nw = nt / 32;
-    const size_t pix = ga ? sizeof(PixRec<T, true>) : sizeof(PixRec<T, false>);
+    const size_t pix = ga ? sizeof(PixRec<T, true>) : sizeof(PixRec<T, false>) * (rr == 16 ? 2 : 1);
     const size_t sm = (size_t)nt * pix + (size_t)nt * (sizeof(Rec<T>) + 2 * sizeof(uint32_t)) +
                       (size_t)nw * nt * sizeof(uint16_t);
     using K = void (*)(const BatchGeo, const int32_t *, int *, const int32_t *, const int2 *,
@@ -1782,7 +1861,6 @@ int raster_bwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
                        const T *, const T *, T, T *);
     const bool small = nt <= 256;
     constexpr bool kAbs = sizeof(T) == 4 && LIG_RASTER_BWD_F2;
-    const bool large = geo.total_tiles() >= LIG_RASTER_BWD_LARGE_MIN_TILES;
     K fn = ga ? (small ? raster_bwd_kernel<T, true, false, 256, LIG_RASTER_BWD_MINB>
                        : raster_bwd_kernel<T, true, false, 1024, 1>)
          : lean_abs ? (small ? (large ? raster_bwd_kernel<T, false, true, 256,
@@ -1798,6 +1876,16 @@ int raster_bwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
                               : raster_bwd_kernel<T, false, true, 1024, 1>)
                      : (small ? raster_bwd_kernel<T, false, false, 256, LIG_RASTER_BWD_MINB>
                               : raster_bwd_kernel<T, false, false, 1024, 1>);
+    if constexpr (kAbs) {
+        if (rr == 8)
+            fn = lean_abs ? raster_bwd_kernel<T, false, true, 128, LIG_RASTER_BWD_RROWS_MINB, true, 8>
+                          : raster_bwd_kernel<T, false, true, 128, LIG_RASTER_BWD_RROWS_MINB, false,
+                                              8>;
+        else if (rr == 16)
+            fn = lean_abs ? raster_bwd_kernel<T, false, true, 64, LIG_RASTER_BWD_R16_MINB, true, 16>
+                          : raster_bwd_kernel<T, false, true, 64, LIG_RASTER_BWD_R16_MINB, false,
+                                              16>;
+    }
     if (!set_dyn_smem((const void *)fn, sm)) return LIG_ERR_LAUNCH;
     int grid = geo.total_tiles();
     if (walk.work) {
