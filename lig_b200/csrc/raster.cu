@@ -772,16 +772,22 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
 #define LIG_RASTER_BWD_LARGE_MIN_TILES 4096
 #endif
 #ifndef LIG_RASTER_BWD_RROWS
-#define LIG_RASTER_BWD_RROWS 8  // float lean walks of large images: region rows (4, 8 or 16)
+#define LIG_RASTER_BWD_RROWS 16  // float lean walks of large images: region rows (4, 8 or 16)
 #endif
 #ifndef LIG_RASTER_BWD_RROWS_MINB
 #define LIG_RASTER_BWD_RROWS_MINB 8  // resident CTAs per SM of the 8x8 walk (128 threads)
 #endif
 #ifndef LIG_RASTER_BWD_R16_MINB
-#define LIG_RASTER_BWD_R16_MINB 16  // resident CTAs per SM of the 8x16 walk (64 threads)
+#define LIG_RASTER_BWD_R16_MINB 14  // resident CTAs per SM of the 8x16 walk (64 threads, 72 registers)
 #endif
 #ifndef LIG_RASTER_BWD_SPLIT2
 #define LIG_RASTER_BWD_SPLIT2 8  // with up to this many Gaussians left, 4 lanes take one
+#endif
+#ifndef LIG_RASTER_BWD_R16_SPLIT1
+#define LIG_RASTER_BWD_R16_SPLIT1 32  // the 8x16 walk: 2 lanes per Gaussian at least
+#endif
+#ifndef LIG_RASTER_BWD_R16_SPLIT3
+#define LIG_RASTER_BWD_R16_SPLIT3 8  // the 8x16 walk: 8 lanes per Gaussian from this many left
 #endif
 #ifndef LIG_RASTER_BWD_SPLIT3
 #define LIG_RASTER_BWD_SPLIT3 4  // with up to this many Gaussians left, 8 lanes take one
@@ -1389,10 +1395,14 @@ __device__ __forceinline__ void bwd_tile(const TileCtx &tc, int tile,
             // pixel records sit in different shared-memory banks); their
             // sums are combined below
             const int left = min(32, nmine - g0);
-            lsplit = !LIG_RASTER_BWD_SPLIT            ? 0
-                     : left <= LIG_RASTER_BWD_SPLIT3 ? 3
-                     : left <= LIG_RASTER_BWD_SPLIT2 ? 2
-                     : left <= LIG_RASTER_BWD_SPLIT1 ? 1 : 0;
+            // (the 8x16 walk: its own first and last thresholds, 64-pixel
+            // regions favour more lanes per Gaussian)
+            constexpr int kS1 = RR == 16 ? LIG_RASTER_BWD_R16_SPLIT1 : LIG_RASTER_BWD_SPLIT1;
+            constexpr int kS3 = RR == 16 ? LIG_RASTER_BWD_R16_SPLIT3 : LIG_RASTER_BWD_SPLIT3;
+            lsplit = !LIG_RASTER_BWD_SPLIT             ? 0
+                     : left <= kS3                     ? 3
+                     : left <= LIG_RASTER_BWD_SPLIT2   ? 2
+                     : left <= kS1                     ? 1 : 0;
             const int gi = lane >> lsplit, part = lane & ((1 << lsplit) - 1);
             const int jstep = 1 << lsplit;
             const int slot = gi < left ? (int)my_list[g0 + gi] : -1;
