@@ -60,7 +60,7 @@ FLOP_PER_EVAL = {"lig_raster_fwd": 20.0, "lig_raster_bwd": 40.0, "lig_raster_bwd
 # kernels on the 2048^2 / 125k-Gaussian step (same density); traffic grows
 # with pixels and Gaussians, so a size-S launch is scaled by (S / 2048)^2.
 DRAM_BYTES_2048 = {"lig_raster_fwd_l2_u8_batch": 21.7e6 + 15.3e6,
-                   "lig_raster_bwd_diff_batch": 63.9e6 + 2.0e6}
+                   "lig_raster_bwd_diff_batch": 63.4e6 + 1.0e6}
 CLOCK_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
