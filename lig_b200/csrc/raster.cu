@@ -772,7 +772,16 @@ __device__ __forceinline__ void fwd_tile(const TileCtx &tc, int tile, const int3
 #define LIG_RASTER_BWD_LARGE_MIN_TILES 4096
 #endif
 #ifndef LIG_RASTER_BWD_RROWS
-#define LIG_RASTER_BWD_RROWS 16  // float lean walks of large images: region rows (4, 8 or 16)
+#define LIG_RASTER_BWD_RROWS 0  // float lean walks of large images: region rows (4, 8, 16; 0: by density)
+#endif
+// Region rows by density (Gaussians per pixel): taller regions save per-pair
+// work, but evaluate more pixels a pair cannot reach, which costs more when
+// the tile lists are long.  Measured (lean backward, 16x16 tiles): at 0.03
+// Gaussians per pixel (8192^2, 2M) 8x16 2.05 ms, 8x8 2.18, 8x4 2.79; at 0.06
+// (4096^2, 1M) 8x16 0.99, 8x8 0.89; at 0.12 (4096^2, 2M) 1.86 / 1.63 / 1.67;
+// at 0.24 (2048^2, 1M) 0.94 / 0.79 / 0.81.  The crossover is near 0.04.
+#ifndef LIG_RASTER_BWD_R16_MAX_DENSITY
+#define LIG_RASTER_BWD_R16_MAX_DENSITY 0.04
 #endif
 #ifndef LIG_RASTER_BWD_RROWS_MINB
 #define LIG_RASTER_BWD_RROWS_MINB 8  // resident CTAs per SM of the 8x8 walk (128 threads)
@@ -1857,9 +1866,11 @@ int raster_bwd(const BatchGeo &geo, TileWalk walk, const int32_t *ids, const int
     const T cl = (T)(clamp > 0 ? clamp : (ga ? 0.999 : 0.99));
     const bool large = geo.total_tiles() >= LIG_RASTER_BWD_LARGE_MIN_TILES;
     // the float lean walks of large images: 8x8 regions (tiles up to 16x16)
-    const int rr = (LIG_RASTER_BWD_RROWS > 4 && sizeof(T) == 4 && LIG_RASTER_BWD_F2 &&
+    const double density = (double)n / (double)geo.total_pixels();
+    const int rr_auto = density <= LIG_RASTER_BWD_R16_MAX_DENSITY ? 16 : 8;
+    const int rr = (LIG_RASTER_BWD_RROWS != 4 && sizeof(T) == 4 && LIG_RASTER_BWD_F2 &&
                     (lean || lean_abs) && large && geo.B <= 16)
-                       ? LIG_RASTER_BWD_RROWS
+                       ? (LIG_RASTER_BWD_RROWS ? LIG_RASTER_BWD_RROWS : rr_auto)
                        : 4;
     const int nt = 32 * Regions::make(ga ? 2 : (rr == 8 ? 1 : rr == 16 ? 3 : 0), geo.B).count;
     const int nw = nt / 32;
