@@ -1066,8 +1066,8 @@ struct alignas(16) PixPair {
 // ((c/2) dy) dy)), alpha = min(clamp, exp(-sigma)) and the same alpha test —
 // so the alpha decisions are bit-identical; only the order in which the
 // moment and colour sums are added differs.  Same quantities as lean_region,
-// added to acc[] (zeroed by the caller), so that an 8x8 region can be walked
-// as two 8x4 halves (pp then holds 8 rows of 4 pair entries).
+// added to acc[] (zeroed by the caller).  NH > 1 walks NH blocks of NR rows
+// (rows r0 .. r0 + NH NR - 1 of a taller region, 4 pair entries a row in pp).
 // ABS: also the per-pixel absolute values of the mean gradient summed over
 // the pixels (the reference's v_xy_abs, csrc/backward.cu:146-150), in acc[2],
 // acc[3]: per pixel v_sigma (a dx + b dy) and v_sigma (b dx + c dy).
@@ -1090,58 +1090,58 @@ __device__ __forceinline__ void lean_region_f2(const Rec<float> &g, float clamp,
     // carry over, the row and column products are rebuilt per block)
 #pragma unroll 1
     for (int hh = 0; hh < NH; ++hh) {
-    const int rb = r0 + hh * NR;
-    f2 DY[NR], CDD[NR];
-#pragma unroll
-    for (int r = 0; r < NR; ++r) {
-        const float dy = g.y - (py0 + (float)(rb + r));
-        DY[r] = f2_dup(dy);
-        CDD[r] = f2_dup(__fmul_rn(__fmul_rn(hc, dy), dy));
-    }
-#pragma unroll
-    for (int k = 0; k < NCP; ++k) {
-        const int cp = c0 + k * CSTEP;
-        const f2 DX = f2_pack(g.x - (px0 + (float)cp), g.x - (px0 + (float)(cp + 4)));
-        const f2 HADX = f2_mul(HA, DX), BDX = f2_mul(BB, DX);
-        f2 AX;
-        if constexpr (ABS) AX = f2_mul(AA, DX);
-        f2 wc = f2_zero(), yc = f2_zero();
+        const int rb = r0 + hh * NR;
+        f2 DY[NR], CDD[NR];
 #pragma unroll
         for (int r = 0; r < NR; ++r) {
-            const PixPair *e = pp + (rb + r) * 4 + cp;
-            const ulonglong2 v01 = *reinterpret_cast<const ulonglong2 *>(e->v);
-            const f2 V0{v01.x}, V1{v01.y};
-            const f2 V2{*reinterpret_cast<const unsigned long long *>(e->v + 4)};
-            const f2 S = f2_fma(BDX, DY[r], f2_fma(HADX, DX, CDD[r]));
-            float s0, s1;
-            f2_unpack(S, s0, s1);
-            const float al0 = fminf(clamp, __expf(-s0)), al1 = fminf(clamp, __expf(-s1));
-            const float a0 = (s0 < 0.f || al0 < 1.f / 255.f) ? 0.f : al0;
-            const float a1 = (s1 < 0.f || al1 < 1.f / 255.f) ? 0.f : al1;
-            const f2 A = f2_pack(a0, a1);
-            sr = f2_fma(A, V0, sr);
-            sg = f2_fma(A, V1, sg);
-            sb = f2_fma(A, V2, sb);
-            // -v_sigma per pixel
-            const f2 WV = f2_mul(A, f2_fma(CB, V2, f2_fma(CG, V1, f2_mul(CR, V0))));
-            wc = f2_add(wc, WV);
-            const f2 TY = f2_mul(WV, DY[r]);
-            yc = f2_add(yc, TY);
-            syy = f2_fma(TY, DY[r], syy);
-            if constexpr (ABS) {
-                float gx0, gx1, gy0, gy1;
-                f2_unpack(f2_mul(WV, f2_fma(BB, DY[r], AX)), gx0, gx1);
-                f2_unpack(f2_mul(WV, f2_fma(CC, DY[r], BDX)), gy0, gy1);
-                ax += fabsf(gx0) + fabsf(gx1);
-                ay += fabsf(gy0) + fabsf(gy1);
-            }
+            const float dy = g.y - (py0 + (float)(rb + r));
+            DY[r] = f2_dup(dy);
+            CDD[r] = f2_dup(__fmul_rn(__fmul_rn(hc, dy), dy));
         }
-        const f2 TX = f2_mul(wc, DX);
-        sx = f2_add(sx, TX);
-        sxx = f2_fma(TX, DX, sxx);
-        sy = f2_add(sy, yc);
-        sxy = f2_fma(yc, DX, sxy);
-    }
+#pragma unroll
+        for (int k = 0; k < NCP; ++k) {
+            const int cp = c0 + k * CSTEP;
+            const f2 DX = f2_pack(g.x - (px0 + (float)cp), g.x - (px0 + (float)(cp + 4)));
+            const f2 HADX = f2_mul(HA, DX), BDX = f2_mul(BB, DX);
+            f2 AX;
+            if constexpr (ABS) AX = f2_mul(AA, DX);
+            f2 wc = f2_zero(), yc = f2_zero();
+#pragma unroll
+            for (int r = 0; r < NR; ++r) {
+                const PixPair *e = pp + (rb + r) * 4 + cp;
+                const ulonglong2 v01 = *reinterpret_cast<const ulonglong2 *>(e->v);
+                const f2 V0{v01.x}, V1{v01.y};
+                const f2 V2{*reinterpret_cast<const unsigned long long *>(e->v + 4)};
+                const f2 S = f2_fma(BDX, DY[r], f2_fma(HADX, DX, CDD[r]));
+                float s0, s1;
+                f2_unpack(S, s0, s1);
+                const float al0 = fminf(clamp, __expf(-s0)), al1 = fminf(clamp, __expf(-s1));
+                const float a0 = (s0 < 0.f || al0 < 1.f / 255.f) ? 0.f : al0;
+                const float a1 = (s1 < 0.f || al1 < 1.f / 255.f) ? 0.f : al1;
+                const f2 A = f2_pack(a0, a1);
+                sr = f2_fma(A, V0, sr);
+                sg = f2_fma(A, V1, sg);
+                sb = f2_fma(A, V2, sb);
+                // -v_sigma per pixel
+                const f2 WV = f2_mul(A, f2_fma(CB, V2, f2_fma(CG, V1, f2_mul(CR, V0))));
+                wc = f2_add(wc, WV);
+                const f2 TY = f2_mul(WV, DY[r]);
+                yc = f2_add(yc, TY);
+                syy = f2_fma(TY, DY[r], syy);
+                if constexpr (ABS) {
+                    float gx0, gx1, gy0, gy1;
+                    f2_unpack(f2_mul(WV, f2_fma(BB, DY[r], AX)), gx0, gx1);
+                    f2_unpack(f2_mul(WV, f2_fma(CC, DY[r], BDX)), gy0, gy1);
+                    ax += fabsf(gx0) + fabsf(gx1);
+                    ay += fabsf(gy0) + fabsf(gy1);
+                }
+            }
+            const f2 TX = f2_mul(wc, DX);
+            sx = f2_add(sx, TX);
+            sxx = f2_fma(TX, DX, sxx);
+            sy = f2_add(sy, yc);
+            sxy = f2_fma(yc, DX, sxy);
+        }
     }
     acc[0] -= f2_sum(sx); acc[1] -= f2_sum(sy);
     acc[4] -= f2_sum(sxx); acc[5] -= f2_sum(sxy); acc[6] -= f2_sum(syy);
