@@ -168,7 +168,10 @@ def test_single_channel_upscaler_is_one_channel_of_the_rgb_form(dtype):
 
 
 @pytest.mark.parametrize("H,W,B,n", [(150, 170, 16, 3000),
-                                     (1040, 1100, 16, 20000),  # >= 4096 tiles
+                                     # >= 4096 tiles: 0.017 Gaussians per pixel, 8x16 regions
+                                     (1040, 1100, 16, 20000),
+                                     # >= 4096 tiles: 0.052 Gaussians per pixel, 8x8 regions
+                                     (1040, 1100, 16, 60000),
                                      (97, 203, 12, 2500)])
 def test_dropin_backward_image_loss_matches_reference(H, W, B, n):
     """The drop-in backward for an image-only loss without opacities (LIG's
@@ -230,11 +233,14 @@ def test_lig_training_step_decreases_loss():
     assert losses[-1] < 0.7 * losses[0]
 
 
-def test_fused_render_l2_matches_unfused_chain():
+@pytest.mark.parametrize("H,W,B,n", [(150, 170, 16, 3000),
+                                     # >= 4096 tiles: the 8x16 and the 8x8 backward walks
+                                     (1040, 1100, 16, 20000),
+                                     (1040, 1100, 16, 60000)])
+def test_fused_render_l2_matches_unfused_chain(H, W, B, n):
     """lig_b200.fused.render_l2_loss == project + rasterize + clamp + mse_loss,
     value and gradients (the fused backward forms dL/dimg in-kernel)."""
     from lig_b200.fused import render_l2_loss
-    H, W, B, n = 150, 170, 16, 3000
     means, L, colors, _ = scene(n, H, W, diag=(0.5, 5.0), seed=4)
     g = torch.Generator().manual_seed(9)
     target = torch.rand(H, W, 3, generator=g).cuda()
