@@ -588,6 +588,12 @@ __global__ void flag_overflow_kernel(const int32_t *d_total, int capacity, int32
 #ifndef LIG_BIN_SCATTER
 #define LIG_BIN_SCATTER 1
 #endif
+#ifndef LIG_SORT_LONG_CTAS_PER_SM
+#define LIG_SORT_LONG_CTAS_PER_SM 8  // CTAs per SM of the long-tile sort (one tile per CTA at a time)
+#endif
+#ifndef LIG_SORT_REG512
+#define LIG_SORT_REG512 1  // tiles of 257..512 entries sorted by a warp in registers
+#endif
 constexpr int kSegSmem = 4096;     // sorted in shared memory up to this length (long tiles)
 #ifndef LIG_BIN_SORT_WARPS
 #define LIG_BIN_SORT_WARPS 8  // measured: 8 warps per CTA 0.258 ms, 4: 0.260, 2: 0.266 (bin, 8192^2)
@@ -708,9 +714,12 @@ __device__ __forceinline__ void sort_segment_regs(uint32_t *seg, int L, int32_t 
 // 4. one warp per tile: sort its entries (from `vals`, written to `ids` as
 // Gaussian ids), write tile_bins ((0, 0) for an empty tile, as the
 // reference's zero-initialised edges) and, when asked, the sorted 64-bit
-// keys.  Tiles of up to 256 entries are sorted in registers; longer ones are
-// queued for tile_sort_long_kernel (no shared memory here, so that the
-// common short tiles run at full occupancy).
+// keys.  Tiles of up to 512 entries are sorted in registers (16 a lane at
+// most: 48 registers, no block barriers); longer ones are queued for
+// tile_sort_long_kernel (no shared memory here, so that the common short
+// tiles run at high occupancy).  At config 1's level-1 density (2048^2, 1M
+// Gaussians, about 360 entries a tile) sorting 257..512-entry tiles here
+// instead of one CTA per tile took the binning from 0.41 to 0.17 ms.
 __global__ void __launch_bounds__(32 * kSegWarps)
 tile_sort_kernel(BatchGeo geo, const uint32_t *__restrict__ tcount,
                  const uint32_t *__restrict__ tend, int capacity, uint32_t *__restrict__ vals,
@@ -735,11 +744,16 @@ tile_sort_kernel(BatchGeo geo, const uint32_t *__restrict__ tcount,
         else if (L <= 64) sort_segment_regs<2>(seg, L, dst, geo);
         else if (L <= 128) sort_segment_regs<4>(seg, L, dst, geo);
         else if (L <= 256) sort_segment_regs<8>(seg, L, dst, geo);
+#if LIG_SORT_REG512
+        else if (L <= 512) sort_segment_regs<16>(seg, L, dst, geo);
+#endif
         else if (lane == 0) long_list[1 + atomicAdd(long_list, 1)] = t;
     }
 }
 
-// Tiles with more than 256 entries: one CTA per tile.  Up to kSegSmem
+// Tiles with more than 512 entries: one CTA per tile, 8 CTAs per SM (0.58 ->
+// 0.41 ms binning at 2048^2 / 1M against 2, when this kernel also took the
+// 257..512-entry tiles).  Up to kSegSmem
 // entries are sorted in shared memory (bitonic, padded to a power of two
 // with the largest key); longer segments in place in global memory with the
 // bitonic sort written with ascending comparators only (each merge starts by
@@ -888,8 +902,8 @@ int run_bin_scatter(const BatchGeo &geo, const void *xys, const void *ext, const
     tile_sort_kernel<<<sort_blocks, 32 * kSegWarps, 0, s>>>(geo, tcount, cursor, capacity, vals,
                                                           gid_sorted, (int2 *)tile_bins,
                                                           isect_sorted, long_list);
-    tile_sort_long_kernel<<<148 * 2, kLongThreads, 0, s>>>(geo, tcount, cursor, capacity, vals,
-                                                           gid_sorted, long_list);
+    tile_sort_long_kernel<<<148 * LIG_SORT_LONG_CTAS_PER_SM, kLongThreads, 0, s>>>(
+        geo, tcount, cursor, capacity, vals, gid_sorted, long_list);
     note_launches(3);
     LIG_LAUNCH_CHECK();
     return LIG_OK;
